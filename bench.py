@@ -1,0 +1,381 @@
+"""Benchmark: batched DDM with the angle boundary on B200.
+
+Workload (one "step"): 4096 parameter vectors drawn uniformly from
+v in [-3,3], a in [0.3,3], z in [0.1,0.9], t in [0.001,2], theta in [-0.1,1.3],
+each with its own n_samples ~ U{1000..20000} (about 43M trajectories),
+delta_t = 1e-3, max_t = 20, float32 -- simulated in ONE persistent launch
+replayed from a CUDA graph.  Metric: trajectories/s (whole job, all ranks).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+`--impl reference` times the reference's own CPU simulator (compiled from its
+sources into oracle/_ref; the C restatement in oracle/ if that build is absent)
+on every host core with a process pool, on a bounded sample of the same
+workload, and prints the same JSON line with "impl": "reference".
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+for _p in (ROOT / "ssm-simulators_b200", ROOT / "oracle"):
+    if str(_p) not in sys.path:
+        sys.path.insert(0, str(_p))
+
+N_THETA = 4096
+SEED = 20241203
+METRIC = "trajectories/s"
+WORKLOAD = ("ddm_flexbound angle boundary, 4096 theta ~ U(v[-3,3], a[0.3,3], z[0.1,0.9], "
+            "t[0.001,2], theta[-0.1,1.3]), n_samples ~ U{1000..20000} per theta, dt=1e-3, max_t=20, "
+            "one persistent graph-captured launch")
+# Issue-slot roofline of the Euler step: the minimum warp-instruction count per
+# accumulator-step of the algorithm (Philox4x32-10 = 60 instructions per 4
+# normals -> 15; Box-Muller ~6.5 per normal incl. 2 SFU ops; update, boundary
+# and exit test ~6.5) -> 28 lane-instructions per accumulator-step.
+INSTR_PER_STEP = 28.0
+N_SM = 148
+LANES_PER_SM_CLK = 128
+
+
+def workload(seed: int = SEED, n_theta: int = N_THETA):
+    rng = np.random.default_rng(seed)
+    f = lambda lo, hi: rng.uniform(lo, hi, n_theta).astype(np.float32)  # noqa: E731
+    theta = {"v": f(-3, 3), "a": f(0.3, 3), "z": f(0.1, 0.9), "t": f(0.001, 2), "theta": f(-0.1, 1.3)}
+    n_samples = rng.integers(1000, 20001, n_theta).astype(np.int64)
+    return theta, n_samples
+
+
+# ------------------------------------------------------------------ CPU side
+def _cores() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:  # pragma: no cover
+        return os.cpu_count() or 1
+
+
+def _angle_host(t, a, theta):
+    return a + np.multiply(t, (-np.sin(theta) / np.cos(theta)))
+
+
+def _cpu_worker(job):
+    """Simulate a list of theta rows with the reference's sequential simulator
+    (or the oracle's C restatement if the reference build is absent)."""
+    kind, rows = job
+    root = Path(__file__).resolve().parent
+    n_done = 0
+    if kind == "reference":
+        sys.path.insert(0, str(root / "oracle" / "_ref"))
+        from cssm.ddm_models import ddm_flexbound  # type: ignore
+
+        for (v, a, z, t, th, n, seed) in rows:
+            f = lambda x: np.array([x], dtype=np.float32)  # noqa: E731
+            ddm_flexbound(f(v), f(a), f(z), f(t), f(999.0), f(1.0), max_t=20.0, delta_t=0.001,
+                          n_samples=int(n), n_trials=1, boundary_fun=_angle_host,
+                          boundary_params={"a": f(a), "theta": f(th)}, random_state=int(seed),
+                          return_option="minimal", smooth_unif=True)
+            n_done += int(n)
+    else:
+        sys.path.insert(0, str(root / "oracle"))
+        import ssm_oracle  # type: ignore
+
+        for (v, a, z, t, th, n, seed) in rows:
+            f = lambda x: np.array([x], dtype=np.float32)  # noqa: E731
+            ssm_oracle.flex("ddm_flexbound", f(v), f(z), f(t), f(999.0), f(1.0), max_t=20.0,
+                            delta_t=0.001, n_samples=int(n), n_trials=1, boundary_fun=_angle_host,
+                            boundary_params={"a": f(a), "theta": f(th)}, smooth_unif=True,
+                            random_state=int(seed))
+            n_done += int(n)
+    return n_done
+
+
+def _cpu_kind() -> str:
+    ref = ROOT / "oracle" / "_ref" / "cssm"
+    return "reference" if any(ref.glob("ddm_models*.so")) else "port"
+
+
+class CpuPool:
+    """All-core CPU baseline: one spawned worker per host core, each running
+    the sequential reference path on a contiguous shard of theta rows (the
+    reference's own per-CPU pool pattern, ssms/dataset_generators/lan_mlp.py:489-498)."""
+
+    def __init__(self, cores: int | None = None):
+        import multiprocessing as mp
+
+        self.cores = cores or _cores()
+        self.kind = _cpu_kind()
+        self.pool = mp.get_context("spawn").Pool(self.cores)
+        # warm the workers (imports, library loads)
+        self.pool.map(_cpu_worker, [(self.kind, [(0.5, 1.0, 0.5, 0.1, 0.2, 10, 1)])] * self.cores)
+
+    def sample_rows(self, theta, n_samples, per_core: int = 24):
+        m = min(len(n_samples), per_core * self.cores)
+        return [(float(theta["v"][i]), float(theta["a"][i]), float(theta["z"][i]),
+                 float(theta["t"][i]), float(theta["theta"][i]), int(n_samples[i]), 1000 + i)
+                for i in range(m)]
+
+    def run(self, rows) -> tuple[int, float]:
+        shards = [rows[i::self.cores] for i in range(self.cores)]
+        t0 = time.perf_counter()
+        done = sum(self.pool.map(_cpu_worker, [(self.kind, s) for s in shards]))
+        return done, time.perf_counter() - t0
+
+    def close(self):
+        self.pool.close()
+        self.pool.join()
+
+
+def cpu_baseline_record(theta, n_samples) -> dict:
+    pool = CpuPool()
+    rows = pool.sample_rows(theta, n_samples)
+    done, sec = pool.run(rows)
+    pool.close()
+    return {"value": done / sec, "unit": METRIC, "cores": pool.cores, "kind": pool.kind,
+            "sample": f"first {len(rows)} of the {N_THETA} theta rows ({done} trajectories), "
+                      f"sequential reference simulator per row, {pool.cores} spawned processes, "
+                      f"wall {sec:.2f} s"}
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = ROOT / "gpurun_out" / f"clocks_{index}_{os.getpid()}.csv"
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.path.parent.mkdir(exist_ok=True)
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.index), "-lms", "200"],
+                                         stdout=self.fh, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.fh.close()
+
+    def summary(self) -> dict:
+        if self.proc is None or not self.path.exists():
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.path.read_text().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": smax, "reasons": ["unsampled"]}
+        busy = [x for x in sm if smax and x > 0.5 * smax] or sm
+        return {"sm_mhz": statistics.median(busy), "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ GPU side
+def _traffic_record():
+    p = ROOT / "profiles" / "ddm_angle_batched_traffic.json"
+    try:
+        return json.loads(p.read_text())
+    except (OSError, ValueError):
+        return None
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+
+    from ssms_b200.batch import BatchedSimulator
+
+    torch.cuda.set_device(local_rank)
+    theta, n_samples = workload(SEED)
+    sim = BatchedSimulator("angle", theta, n_samples, max_t=20.0, delta_t=0.001,
+                           seed=SEED + 7919 * rank, smooth_unif=True)
+    total = sim.total
+    # one untimed run with step counts: the algorithmic work of every replay
+    out = sim.run(want_steps=True)
+    steps_per_launch = int(out.steps.to(torch.int64).sum().item())
+    sim.capture()
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > L2
+    stream = torch.cuda.current_stream()
+
+    def dist_barrier():
+        if world > 1:
+            torch.distributed.barrier()
+
+    for _ in range(args.warmup):
+        sim.replay()
+    torch.cuda.synchronize()
+    dist_barrier()
+    ms = []
+    with ClockSampler(local_rank) as clk:
+        for _ in range(args.steps):
+            flush.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            sim.replay()
+            e1.record(stream)
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+    torch.cuda.synchronize()
+    dist_barrier()
+    t_sum = sum(ms)
+    if world > 1:
+        tt = torch.tensor([t_sum], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+        t_sum = float(tt.item())
+    ms_per_step = t_sum / args.steps
+    value = world * total * args.steps / (t_sum / 1e3)
+
+    # end to end: pinned host theta -> device, graph replay, rts+choices -> pinned host
+    host_theta = {k: torch.from_numpy(np.ascontiguousarray(theta[k])).pin_memory()
+                  for k in ("v", "a", "z", "t")}
+    slope_h = torch.from_numpy(np.ascontiguousarray(sim.spec["p1"])).pin_memory()
+    rts_h = torch.empty(total, dtype=torch.float32).pin_memory()
+    chs_h = torch.empty(total, dtype=torch.int32).pin_memory()
+    h2d = sum(x.numel() * 4 for x in host_theta.values()) + slope_h.numel() * 4
+    d2h = total * 8
+    e2e_ms = []
+    for i in range(args.warmup + args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        sim.v.copy_(host_theta["v"], non_blocking=True)
+        sim.a.copy_(host_theta["a"], non_blocking=True)
+        sim.z.copy_(host_theta["z"], non_blocking=True)
+        sim.t.copy_(host_theta["t"], non_blocking=True)
+        sim.p1.copy_(slope_h, non_blocking=True)
+        sim.replay()
+        rts_h.copy_(sim.rts, non_blocking=True)
+        chs_h.copy_(sim.choices, non_blocking=True)
+        torch.cuda.synchronize()
+        if i >= args.warmup:
+            e2e_ms.append((time.perf_counter() - t0) * 1e3)
+    e2e_t = sum(e2e_ms)
+    if world > 1:
+        tt = torch.tensor([e2e_t], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+        e2e_t = float(tt.item())
+    e2e_value = world * total * args.steps / (e2e_t / 1e3)
+
+    clocks = clk.summary()
+    f_max = (clocks.get("sm_max_mhz") or 1965.0) * 1e6
+    peak_steps = N_SM * LANES_PER_SM_CLK * f_max / INSTR_PER_STEP
+    achieved_steps = steps_per_launch / (ms_per_step / 1e3)
+    traffic = _traffic_record()
+    line = {
+        "metric": METRIC, "value": value, "unit": "trajectories/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded uniform parameter draws; no dataset)",
+        "config": {"workload": WORKLOAD, "n_theta": N_THETA, "trajectories_per_step": total,
+                   "accumulator_steps_per_step": steps_per_launch, "seed": SEED,
+                   "l2": "flushed (256 MB write) between timed steps", "parallelism": f"replicas x{world}"},
+        "roofline": {"bound": "issue", "achieved": achieved_steps / 1e9, "peak": peak_steps / 1e9,
+                     "unit": "G accumulator-steps/s", "frac": achieved_steps / peak_steps,
+                     "traffic": None if traffic is None else traffic.get("bytes_per_launch"),
+                     "peak_basis": f"{N_SM} SMs x {LANES_PER_SM_CLK} lanes/clk x {f_max/1e6:.0f} MHz / "
+                                   f"{INSTR_PER_STEP:.0f} lane-instructions per accumulator-step",
+                     "output_hbm_gbs": total * 8 / (ms_per_step / 1e3) / 1e9},
+        "e2e": {"value": e2e_value, "unit": "trajectories/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+        "gpu_launches": 2 * args.steps,
+        "clocks": clocks,
+    }
+    return line, theta, n_samples
+
+
+def run_reference(args):
+    theta, n_samples = workload(SEED)
+    pool = CpuPool()
+    rows = pool.sample_rows(theta, n_samples, per_core=8)
+    for _ in range(args.warmup):
+        pool.run(rows)
+    done_total, sec_total = 0, 0.0
+    for _ in range(args.steps):
+        done, sec = pool.run(rows)
+        done_total += done
+        sec_total += sec
+    pool.close()
+    value = done_total / sec_total
+    return {
+        "metric": METRIC, "value": value, "unit": "trajectories/s", "n_gpus": 0,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sec_total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded uniform parameter draws; no dataset)",
+        "config": {"workload": WORKLOAD, "n_theta": N_THETA,
+                   "sample_theta_per_step": len(rows), "seed": SEED},
+        "impl": "reference",
+        "cpu_baseline": {"value": value, "unit": METRIC, "cores": pool.cores, "kind": pool.kind,
+                         "sample": f"first {len(rows)} theta rows per step ({done_total // max(args.steps, 1)} "
+                                   f"trajectories), {pool.cores} spawned processes"},
+        "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(run_reference(args)), flush=True)
+        return
+
+    if world > 1:
+        import datetime
+
+        import torch
+
+        torch.cuda.set_device(local_rank)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    line, theta, n_samples = run_ours(args, rank, world, local_rank)
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_record(theta, n_samples)
+    if world > 1:
+        import torch
+
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

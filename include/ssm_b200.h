@@ -1,0 +1,133 @@
+/*
+ * ssm_b200.h -- C ABI of the sm_100a sequential-sampling-model simulators.
+ *
+ * Every entry point takes plain device pointers, sizes and a cudaStream_t
+ * (passed as void*), launches asynchronously on that stream and returns an
+ * int status (SSM_OK on success).  Nothing here allocates device memory: the
+ * caller owns outputs and provides the scratch workspace whose size the
+ * matching *_workspace_bytes() query reports.  Outputs follow the reference
+ * package's layout: rts float32 and choices int32, indexed by
+ * (sample n, trial k) as  n * n_trials + k  ([n_samples, n_trials, 1] in the
+ * reference), or -- for the ragged batched form -- sample_offsets[k] + n.
+ *
+ * Each entry point cites the reference interface it replaces (paths relative
+ * to the ssm-simulators source tree).
+ */
+#ifndef SSM_B200_H
+#define SSM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define SSM_OK 0
+#define SSM_ERR_ARG 1          /* invalid argument (null pointer, bad size, bad enum) */
+#define SSM_ERR_CUDA 2         /* a CUDA runtime call failed; see ssm_last_error() */
+#define SSM_ERR_WORKSPACE 3    /* workspace missing or smaller than *_workspace_bytes() */
+#define SSM_ERR_NOISE_RANGE 4  /* a trajectory needed more injected increments than its row holds */
+#define SSM_ERR_DEVICE 5       /* the device reported an error flag (read by ssm_check_status) */
+
+/* ---- boundary kinds for the single-accumulator simulators -------------- */
+/* The reference evaluates boundary_fun(t_s, **boundary_params) on the host
+ * into a float32 table (src/cssm/_utils.pyx:655-666).  Here the common
+ * families are evaluated in registers; any other function uses TABLE. */
+#define SSM_BOUND_TABLE 0    /* b(ix) = table[k * table_stride + min(ix, table_len-1)] */
+#define SSM_BOUND_CONSTANT 1 /* b(t) = a                                               */
+#define SSM_BOUND_LINEAR 2   /* b(t) = a + t * p1   (angle: p1 = -sin(theta)/cos(theta)) */
+#define SSM_BOUND_WEIBULL 3  /* b(t) = a * exp(-(t / p2)^p1)  (p1 = alpha, p2 = beta)   */
+
+/* ---- noise sources ------------------------------------------------------ */
+/* Device RNG: counter-based Philox4x32-10 keyed by (seed, trial k, sample n),
+ * so a trajectory's stream does not depend on the launch configuration.
+ * Noise injection: the caller passes pre-drawn standard increments, one row
+ * of noise_row_len float32 per trajectory (row index = output index), plus
+ * one uniform per trajectory for the rt jitter; results are then bit-exact
+ * with a sequential CPU restatement consuming the same rows. */
+
+/* Per-call launch options shared by the simulators. */
+typedef struct ssm_launch {
+    int block_threads;     /* 0 = library default (autotuned value if set) */
+    int blocks_per_sm;     /* 0 = as many as fit                            */
+    int chunk;             /* trajectories a warp claims per queue access; 0 = default */
+} ssm_launch;
+
+/* Version / diagnostics -------------------------------------------------- */
+int ssm_version(void);
+/* Last error message of the calling thread (static storage, never NULL). */
+const char *ssm_last_error(void);
+/* Copy the device error word written by the last launch that used `workspace`
+ * back to the host (synchronises `stream`); returns SSM_OK or the stored code. */
+int ssm_check_status(const void *workspace, void *stream);
+
+/* ---- single-accumulator Euler-Maruyama DDM family ----------------------- */
+
+/* Bytes of scratch the DDM-family entry points need for n_trials trials. */
+size_t ssm_ddm_workspace_bytes(int64_t n_trials);
+
+/*
+ * ssm_ddm_flexbound -- replaces cssm.ddm_flexbound
+ * (src/cssm/ddm_models.pyx:589-878, sequential loop :696-744).
+ * Per trial k: start y = -b(0) + 2 z b(0); while -b(ix) <= y <= b(ix) and
+ * t <= min(max_t, deadline - t_nd): y += v dt + sqrt(dt) s g.  rt = t + t_nd +
+ * jitter, choice = sign(y), rt = -999 when rt >= deadline or deadline <= 0.
+ *
+ * v, a, z, t, deadline, s : float32[n_trials]
+ * bound_p1, bound_p2      : float32[n_trials] or NULL (see SSM_BOUND_*)
+ * bound_table             : float32[n_trials * table_stride] (TABLE only)
+ * sample_offsets          : NULL for n_samples per trial in the reference
+ *                           layout, else int64[n_trials+1] ragged prefix sums
+ *                           (output index sample_offsets[k] + n)
+ * max_t_per_trial         : NULL (use max_t) or float32[n_trials]
+ * noise_rows / noise_row_len / noise_unif : NULL for the device RNG
+ * traj                    : NULL or float32[traj_len]; receives trial 0 /
+ *                           sample 0's path (-999 padded) as in the reference
+ * steps                   : NULL or int32 per output; Euler steps taken
+ */
+int ssm_ddm_flexbound(const float *v, const float *a, const float *z, const float *t,
+                      const float *deadline, const float *s, int64_t n_trials, int64_t n_samples,
+                      const int64_t *sample_offsets, float max_t, const float *max_t_per_trial,
+                      float delta_t, int bound_kind, const float *bound_p1, const float *bound_p2,
+                      const float *bound_table, int64_t table_stride, int64_t table_len,
+                      uint64_t seed, int smooth_unif, const float *noise_rows,
+                      int64_t noise_row_len, const float *noise_unif, float *rts,
+                      int32_t *choices, int32_t *steps, float *traj, int64_t traj_len,
+                      const ssm_launch *launch, void *workspace, size_t workspace_bytes,
+                      void *stream);
+
+/*
+ * ssm_ddm -- replaces cssm.ddm (src/cssm/ddm_models.pyx:349-582): the legacy
+ * DDM on [0, a] with start z a and exit when y > a or y < 0.
+ */
+int ssm_ddm(const float *v, const float *a, const float *z, const float *t, const float *deadline,
+            const float *s, int64_t n_trials, int64_t n_samples, float max_t, float delta_t,
+            uint64_t seed, int smooth_unif, const float *noise_rows, int64_t noise_row_len,
+            const float *noise_unif, float *rts, int32_t *choices, int32_t *steps, float *traj,
+            int64_t traj_len, const ssm_launch *launch, void *workspace, size_t workspace_bytes,
+            void *stream);
+
+/*
+ * ssm_levy_flexbound -- replaces cssm.levy_flexbound
+ * (src/cssm/levy_models.pyx:47-348): y += v dt + s dt^(1/alpha) X, X symmetric
+ * alpha-stable drawn in-kernel by Chambers-Mallows-Stuck (reference sampler:
+ * src/cssm/_utils.pyx:369-472).  Same boundary/offset/noise conventions as
+ * ssm_ddm_flexbound; injected rows hold alpha-stable draws.
+ */
+int ssm_levy_flexbound(const float *v, const float *a, const float *z, const float *alpha,
+                       const float *t, const float *deadline, const float *s, int64_t n_trials,
+                       int64_t n_samples, const int64_t *sample_offsets, float max_t,
+                       float delta_t, int bound_kind, const float *bound_p1, const float *bound_p2,
+                       const float *bound_table, int64_t table_stride, int64_t table_len,
+                       uint64_t seed, int smooth_unif, const float *noise_rows,
+                       int64_t noise_row_len, const float *noise_unif, float *rts,
+                       int32_t *choices, int32_t *steps, float *traj, int64_t traj_len,
+                       const ssm_launch *launch, void *workspace, size_t workspace_bytes,
+                       void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SSM_B200_H */

@@ -1,0 +1,110 @@
+// Shared device/host helpers for the sm_100a simulators: status handling,
+// the counter-based Philox4x32-10 generator and normal/uniform transforms.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "ssm_b200.h"
+
+namespace ssm {
+
+// ---------------------------------------------------------------- host side
+void set_error(const char *fmt, ...);
+int cuda_fail(cudaError_t e, const char *where);
+int sm_count();
+
+#define SSM_CUDA(call)                                         \
+    do {                                                       \
+        cudaError_t e_ = (call);                               \
+        if (e_ != cudaSuccess) return ::ssm::cuda_fail(e_, #call); \
+    } while (0)
+
+#define SSM_REQUIRE(cond, ...)          \
+    do {                                \
+        if (!(cond)) {                  \
+            ::ssm::set_error(__VA_ARGS__); \
+            return SSM_ERR_ARG;         \
+        }                               \
+    } while (0)
+
+// Workspace header shared by every persistent kernel: a work counter and an
+// error word.  It sits at the start of the caller's workspace and is cleared
+// by the launching entry point (cudaMemsetAsync) before each launch.
+struct alignas(256) WorkspaceHeader {
+    unsigned long long counter;  // next unclaimed trajectory index
+    int err;                     // first error code raised on the device (0 = none)
+    int err_detail;              // e.g. the trajectory that overran its noise row
+    unsigned long long aux[4];
+};
+static_assert(sizeof(WorkspaceHeader) == 256, "header must stay 256 B");
+
+// Philox4x32-10 round keys.  The key schedule depends only on the seed, so it
+// is expanded once on the host and travels in the kernel parameter block
+// (constant bank): each round's key XOR is then a free constant operand.
+struct PhiloxKeys {
+    uint32_t k0[10];
+    uint32_t k1[10];
+};
+
+inline PhiloxKeys philox_keys(uint64_t seed) {
+    PhiloxKeys k;
+    uint32_t a = (uint32_t)seed, b = (uint32_t)(seed >> 32);
+    for (int r = 0; r < 10; ++r) {
+        k.k0[r] = a;
+        k.k1[r] = b;
+        a += 0x9E3779B9u;  // Weyl increments of the Philox key schedule
+        b += 0xBB67AE85u;
+    }
+    return k;
+}
+
+// ---------------------------------------------------------------- device side
+// Philox4x32 with 10 rounds (Salmon, Moraes, Dror & Shaw, "Parallel Random
+// Numbers: As Easy as 1, 2, 3", SC'11).  One call maps a 128-bit counter to
+// 128 random bits; we key it by the seed and count over (step block, sample,
+// trial, stream) so every trajectory owns an independent stream.
+__device__ __forceinline__ uint4 philox10(uint4 c, const PhiloxKeys &key) {
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        const uint32_t lo0 = 0xD2511F53u * c.x;
+        const uint32_t hi0 = __umulhi(0xD2511F53u, c.x);
+        const uint32_t lo1 = 0xCD9E8D57u * c.z;
+        const uint32_t hi1 = __umulhi(0xCD9E8D57u, c.z);
+        c = make_uint4(hi1 ^ c.y ^ key.k0[r], lo1, hi0 ^ c.w ^ key.k1[r], lo0);
+    }
+    return c;
+}
+
+// 23 random bits -> float in [1, 2) by exponent stuffing (two integer ops, no
+// int->float conversion, which runs at quarter rate).
+__device__ __forceinline__ float bits_to_1_2(uint32_t x) {
+    return __uint_as_float(0x3f800000u | (x >> 9));
+}
+// Uniform on the open interval (0, 1): values j*2^-23 + 2^-24, j = 0..2^23-1.
+__device__ __forceinline__ float uniform_open(uint32_t x) {
+    return bits_to_1_2(x) - 0.99999994f;  // 1 - 2^-24; exact in float32
+}
+// Uniform on [0, 1) with 24-bit resolution (used once per trajectory).
+__device__ __forceinline__ float uniform_co(uint32_t x) {
+    return (float)(x >> 8) * 5.9604645e-08f;  // 2^-24
+}
+
+// Box-Muller transform of two 32-bit words into two N(0,1) variates
+// (r = sqrt(-2 ln u1), phase 2 pi u2).  Uses the SFU approximations of log2,
+// rsqrt, sin and cos: 4 MUFU operations per pair.
+__device__ __forceinline__ float2 box_muller(uint32_t a, uint32_t b) {
+    const float u1 = uniform_open(a);
+    const float u2 = bits_to_1_2(b) - 1.0f;
+    const float e = -1.3862944f * __log2f(u1);  // -2 ln u1 > 0
+    const float r = e * rsqrtf(e);
+    float s, c;
+    __sincosf(6.2831853f * u2, &s, &c);
+    return make_float2(r * c, r * s);
+}
+
+__device__ __forceinline__ void raise_error(WorkspaceHeader *h, int code, int detail) {
+    if (atomicCAS(&h->err, 0, code) == 0) h->err_detail = detail;
+}
+
+}  // namespace ssm

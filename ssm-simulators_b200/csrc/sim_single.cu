@@ -1,0 +1,561 @@
+// Single-accumulator Euler-Maruyama simulators for sm_100a: the flexible-bound
+// DDM (cssm.ddm_flexbound), the legacy [0, a] DDM (cssm.ddm) and the Levy
+// flight DDM (cssm.levy_flexbound).
+//
+// Design (one thread per trajectory, persistent grid):
+//  * A per-trial prologue (k_prep) turns the reference's per-trial arrays into
+//    a 64-byte TrialRow with every derived float computed once, in the same
+//    IEEE operation order the reference uses (src/cssm/ddm_models.pyx:700-744).
+//  * The main kernel runs one grid of resident CTAs.  Each warp claims
+//    trajectories from a global work counter in chunks; whenever lanes finish
+//    (ballot), the warp hands them the next trajectories of its chunk
+//    (popc rank), so lanes never idle while work remains and divergence
+//    between fast and slow trajectories costs at most one 4-step block.
+//  * Steps run in blocks of four: one Philox4x32-10 call yields four 32-bit
+//    words = two Box-Muller pairs = the four N(0,1) increments of the block.
+//  * Boundaries are evaluated in registers (constant / linear collapse /
+//    Weibull) or read from a caller-evaluated table for arbitrary shapes.
+//  * Noise injection replaces the generator by caller rows and switches every
+//    float operation to explicit round-to-nearest intrinsics, giving results
+//    bit-identical to the sequential CPU restatement.
+#include "common.cuh"
+
+namespace ssm {
+
+enum Model { M_FLEX = 0, M_LEGACY = 1, M_LEVY = 2 };
+
+struct alignas(16) TrialRow {
+    float drift;     // v * dt
+    float scale;     // sqrt(dt) * s ;  Levy: s * dt^(1/alpha)
+    float y0;        // start point
+    float dl_tmp;    // min(max_t, deadline - t): the walk runs while t <= dl_tmp
+    float t;         // non-decision time
+    float deadline;  // rt >= deadline (or deadline <= 0) -> omission
+    float a;         // boundary height (legacy DDM: upper bound)
+    float p1;        // LINEAR: slope ; WEIBULL: shape alpha
+    float p2;        // WEIBULL: scale beta
+    float dtp1;      // dt * p1 (linear boundary per step, fast path)
+    float inv_beta;  // 1 / beta
+    float alpha;     // Levy stability index
+    float inv_alpha; // 1 / alpha
+    float expo;      // (1 - alpha) / alpha
+    float pad[2];
+};
+static_assert(sizeof(TrialRow) == 64, "TrialRow is one 64-byte line");
+
+struct SingleParams {
+    PhiloxKeys key;
+    const TrialRow *rows;
+    const int64_t *offsets;  // ragged prefix sums (n_trials + 1) or nullptr
+    int64_t n_trials;
+    int64_t total;           // number of trajectories; -1 = read offsets[n_trials]
+    float dt;
+    int smooth;
+    int chunk;
+    const float *table;
+    int64_t tstride, tlen;
+    const float *noise;      // injected increments: row w holds nlen floats
+    int64_t nlen;
+    const float *nunif;      // injected jitter uniforms, one per trajectory
+    float *rts;
+    int32_t *choices;
+    int32_t *steps;
+    WorkspaceHeader *hdr;
+    float *traj;             // trajectory recorder (record kernel only)
+    int64_t traj_len;
+};
+
+struct PrepArgs {
+    const float *v, *a, *z, *t, *deadline, *s, *alpha, *p1, *p2, *maxt_k, *table;
+    int64_t n_trials, tstride;
+    float dt, sqrt_dt, max_t;
+    int model, bound;
+    TrialRow *rows;
+};
+
+// ------------------------------------------------------------------ prologue
+__global__ void k_prep(const PrepArgs A) {
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= A.n_trials) return;
+    TrialRow r;
+    const float dt = A.dt;
+    r.drift = __fmul_rn(A.v[k], dt);
+    r.t = A.t[k];
+    r.deadline = A.deadline[k];
+    const float maxt = A.maxt_k ? A.maxt_k[k] : A.max_t;
+    const float dl = __fsub_rn(r.deadline, r.t);
+    r.dl_tmp = (dl < maxt) ? dl : maxt;  // src/cssm/_utils.pyx:712-718
+    r.a = A.a ? A.a[k] : 0.f;
+    r.p1 = A.p1 ? A.p1[k] : 0.f;
+    r.p2 = A.p2 ? A.p2[k] : 1.f;
+    r.dtp1 = dt * r.p1;
+    r.inv_beta = 1.0f / r.p2;
+    r.alpha = A.alpha ? A.alpha[k] : 2.f;
+    r.inv_alpha = (float)(1.0 / (double)r.alpha);
+    r.expo = (float)((1.0 - (double)r.alpha) / (double)r.alpha);
+    r.pad[0] = r.pad[1] = 0.f;
+    if (A.model == M_LEVY) {
+        // delta_t_alpha = s * pow(delta_t, 1.0 / alpha) in double (levy_models.pyx:166)
+        r.scale = __double2float_rn((double)A.s[k] * pow((double)dt, 1.0 / (double)r.alpha));
+    } else {
+        r.scale = __fmul_rn(A.sqrt_dt, A.s[k]);  // ddm_models.pyx:705
+    }
+    if (A.model == M_LEGACY) {
+        r.y0 = __fmul_rn(A.z[k], r.a);  // ddm_models.pyx:451
+    } else {
+        const float b0 = (A.bound == SSM_BOUND_TABLE) ? A.table[k * A.tstride] : r.a;
+        // -b0 + z*2*b0, evaluated in double as the generated C does (ddm_models.pyx:709)
+        const double bd = (double)b0;
+        r.y0 = __double2float_rn(__dadd_rn(-bd, __dmul_rn(__dmul_rn((double)A.z[k], 2.0), bd)));
+    }
+    reinterpret_cast<TrialRow *>(A.rows)[k] = r;
+}
+
+// ------------------------------------------------------------------ helpers
+__device__ __forceinline__ int64_t ragged_find(const int64_t *off, int64_t K, int64_t w,
+                                               int64_t hint) {
+    int64_t k = hint;
+    if (k < 0 || k >= K || __ldg(off + k) > w) k = 0;
+    int64_t step = 1;
+    while (k + step < K && __ldg(off + k + step) <= w) {
+        k += step;
+        step <<= 1;
+    }
+    int64_t hi = (k + step < K) ? k + step : K;
+    while (hi - k > 1) {
+        const int64_t mid = (k + hi) >> 1;
+        if (__ldg(off + mid) <= w) k = mid; else hi = mid;
+    }
+    return k;
+}
+
+template <int BOUND, bool EXACT>
+__device__ __forceinline__ float bound_at(const TrialRow &r, float ixf, int ix,
+                                          const SingleParams &p, int64_t k) {
+    if (BOUND == SSM_BOUND_CONSTANT) {
+        return r.a;
+    } else if (BOUND == SSM_BOUND_LINEAR) {
+        // table value a + f32(ix*dt) * p1 (boundary_functions.py:57-72 on t_s)
+        if (EXACT) return __fadd_rn(r.a, __fmul_rn(__fmul_rn(ixf, p.dt), r.p1));
+        return fmaf(ixf, r.dtp1, r.a);
+    } else if (BOUND == SSM_BOUND_WEIBULL) {
+        // a * exp(-(t/beta)^alpha) (boundary_functions.py:103-122)
+        const float x = ixf * p.dt * r.inv_beta;
+        const float pw = (x > 0.f) ? exp2f(r.p1 * __log2f(x)) : 0.f;
+        return r.a * __expf(-pw);
+    } else {
+        const int64_t i = (ix < p.tlen) ? ix : p.tlen - 1;
+        return __ldg(p.table + k * p.tstride + i);
+    }
+}
+
+// Symmetric alpha-stable variate by Chambers-Mallows-Stuck (Chambers, Mallows
+// & Stuck, JASA 71, 1976) with the reference's guards (_utils.pyx:426-472):
+// U ~ U(-pi/2 + 1e-7, pi/2 - 1e-7), W ~ Exp(1) floored at 1e-10, cosines
+// floored at 1e-10 in magnitude, output clipped to +-1e10 and NaN -> 0.
+__device__ __forceinline__ float cms_stable(uint32_t bu, uint32_t bw, const TrialRow &r) {
+    const float u01 = bits_to_1_2(bu) - 1.0f;
+    const float U = fmaf(u01, 3.1415925f, -1.5707962f);
+    const float W = fmaxf(-__logf(uniform_open(bw)), 1e-10f);
+    float X;
+    if (r.alpha == 1.0f) {
+        X = tanf(U);
+    } else {
+        const float cu = fmaxf(fabsf(cosf(U)), 1e-10f);
+        const float cua = fmaxf(fabsf(cosf(U * (1.0f - r.alpha))), 1e-10f);
+        X = (sinf(r.alpha * U) / __powf(cu, r.inv_alpha)) * __powf(cua / W, r.expo);
+    }
+    if (X != X) X = 0.f;
+    return fminf(fmaxf(X, -1e10f), 1e10f);
+}
+
+struct Lane {
+    int64_t w;
+    uint32_t k, n, blk;
+    int ix;
+    float y, tp, ixf;
+};
+
+// Four increments for the lane's current step block.
+template <int MODEL, bool NOISE>
+__device__ __forceinline__ void draw4(const SingleParams &p, const Lane &L, const TrialRow &r,
+                                      float g[4]) {
+    if (NOISE) {
+        const float *row = p.noise + L.w * p.nlen;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) g[q] = (L.ix + q < p.nlen) ? __ldg(row + L.ix + q) : 0.f;
+    } else if (MODEL == M_LEVY) {
+        const uint4 b0 = philox10(make_uint4(L.blk, L.n, L.k, 0u), p.key);
+        const uint4 b1 = philox10(make_uint4(L.blk, L.n, L.k, 2u), p.key);
+        g[0] = cms_stable(b0.x, b0.y, r);
+        g[1] = cms_stable(b0.z, b0.w, r);
+        g[2] = cms_stable(b1.x, b1.y, r);
+        g[3] = cms_stable(b1.z, b1.w, r);
+    } else {
+        const uint4 b = philox10(make_uint4(L.blk, L.n, L.k, 0u), p.key);
+        const float2 n0 = box_muller(b.x, b.y);
+        const float2 n1 = box_muller(b.z, b.w);
+        g[0] = n0.x;
+        g[1] = n0.y;
+        g[2] = n1.x;
+        g[3] = n1.y;
+    }
+}
+
+// Advance one lane by up to four Euler steps; returns false once the walk has
+// stopped (the reference's `while` condition failed before a step).
+template <int MODEL, int BOUND, bool NOISE, bool RECORD>
+__device__ __forceinline__ bool step_block(const SingleParams &p, Lane &L, const TrialRow &r,
+                                           const float g[4]) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        bool inside;
+        if (MODEL == M_LEGACY) {
+            inside = (L.y <= r.a) && (L.y >= 0.f) && (L.tp <= r.dl_tmp);  // ddm_models.pyx:451
+        } else {
+            const float b = bound_at<BOUND, NOISE>(r, L.ixf, L.ix, p, L.k);
+            inside = (fabsf(L.y) <= b) && (L.tp <= r.dl_tmp);  // ddm_models.pyx:719
+        }
+        if (!inside) return false;
+        if (NOISE && L.ix >= p.nlen) {
+            raise_error(p.hdr, SSM_ERR_NOISE_RANGE, (int)L.w);
+            return false;
+        }
+        // (y + v*dt) + scale*g: the association the reference build uses
+        if (NOISE) {
+            L.y = __fadd_rn(__fadd_rn(L.y, r.drift), __fmul_rn(r.scale, g[q]));
+            L.tp = __fadd_rn(L.tp, p.dt);
+        } else {
+            L.y = fmaf(r.scale, g[q], L.y + r.drift);
+            L.tp += p.dt;
+        }
+        L.ixf += 1.0f;
+        L.ix += 1;
+        if (RECORD && L.ix < p.traj_len) p.traj[L.ix] = L.y;
+    }
+    return true;
+}
+
+template <bool NOISE>
+__device__ __forceinline__ void finalize(const SingleParams &p, const Lane &L, const TrialRow &r) {
+    float u;
+    if (NOISE) u = __ldg(p.nunif + L.w);
+    else u = uniform_co(philox10(make_uint4(0u, L.n, L.k, 1u), p.key).x);
+    // compute_smooth_unif (_utils.pyx:668-695): double arithmetic, float result
+    float sm = 0.f;
+    if (p.smooth) {
+        if (L.tp == 0.f) sm = __double2float_rn(((double)u * 0.5) * (double)p.dt);
+        else if (L.tp < r.dl_tmp) sm = __double2float_rn((0.5 - (double)u) * (double)p.dt);
+    }
+    float rt = __fadd_rn(__fadd_rn(L.tp, r.t), sm);
+    if (rt >= r.deadline || r.deadline <= 0.f) rt = -999.f;  // enforce_deadline
+    const int choice = (L.y > 0.f) - (L.y < 0.f);             // sign(y)
+    p.rts[L.w] = rt;
+    p.choices[L.w] = choice;
+    if (p.steps) p.steps[L.w] = L.ix;
+}
+
+__device__ __forceinline__ void lane_init(const SingleParams &p, Lane &L, TrialRow &r, int64_t w,
+                                          int64_t &hint) {
+    int64_t k, n;
+    if (p.offsets == nullptr) {
+        k = w % p.n_trials;
+        n = w / p.n_trials;
+    } else {
+        k = ragged_find(p.offsets, p.n_trials, w, hint);
+        n = w - __ldg(p.offsets + k);
+        hint = k;
+    }
+    const float4 *src = reinterpret_cast<const float4 *>(p.rows + k);
+    float4 *dst = reinterpret_cast<float4 *>(&r);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) dst[i] = __ldg(src + i);
+    L.w = w;
+    L.k = (uint32_t)k;
+    L.n = (uint32_t)n;
+    L.blk = 0;
+    L.ix = 0;
+    L.ixf = 0.f;
+    L.tp = 0.f;
+    L.y = r.y0;
+}
+
+// ------------------------------------------------------------------ main kernel
+template <int MODEL, int BOUND, bool NOISE>
+__global__ void __launch_bounds__(256) k_single(const __grid_constant__ SingleParams p) {
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const unsigned lt_mask = (1u << lane) - 1u;
+    const int64_t total = (p.total >= 0) ? p.total : __ldg(p.offsets + p.n_trials);
+
+    Lane L;
+    TrialRow r;
+    L.w = 0; L.k = L.n = L.blk = 0; L.ix = 0; L.y = L.tp = L.ixf = 0.f;
+    bool active = false;
+    bool exhausted = false;
+    int64_t q_next = 0, q_end = 0, hint = 0;
+
+    for (;;) {
+        const unsigned need = __ballot_sync(FULL, !active);
+        if (need != 0u && !exhausted) {
+            const int cnt = __popc(need);
+            const int64_t avail = q_end - q_next;
+            int64_t base = 0;
+            if (avail < cnt) {
+                unsigned long long b = 0ull;
+                if (lane == 0) b = atomicAdd(&p.hdr->counter, (unsigned long long)p.chunk);
+                base = (int64_t)__shfl_sync(FULL, b, 0);
+                if (base >= total) exhausted = true;
+            }
+            if (!active) {
+                const int rank = __popc(need & lt_mask);
+                const int64_t w = (rank < avail) ? q_next + rank : base + (rank - avail);
+                if (w < total) {
+                    lane_init(p, L, r, w, hint);
+                    active = true;
+                }
+            }
+            if (avail >= cnt) {
+                q_next += cnt;
+            } else {
+                q_next = base + (cnt - avail);
+                q_end = base + p.chunk;
+            }
+        }
+        if (__ballot_sync(FULL, active) == 0u) break;
+        if (active) {
+            float g[4];
+            draw4<MODEL, NOISE>(p, L, r, g);
+            const bool live = step_block<MODEL, BOUND, NOISE, false>(p, L, r, g);
+            L.blk += 1;
+            if (!live) {
+                finalize<NOISE>(p, L, r);
+                active = false;
+            }
+        }
+    }
+}
+
+// Re-simulates trial 0 / sample 0 with the same stream and writes its path
+// (metadata['trajectory'], -999 padded: ddm_models.pyx:714-728).
+template <int MODEL, int BOUND, bool NOISE>
+__global__ void k_record(const __grid_constant__ SingleParams p) {
+    for (int64_t i = threadIdx.x; i < p.traj_len; i += blockDim.x) p.traj[i] = -999.f;
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    Lane L;
+    TrialRow r;
+    int64_t hint = 0;
+    lane_init(p, L, r, 0, hint);
+    if (p.traj_len > 0) p.traj[0] = L.y;
+    for (;;) {
+        float g[4];
+        draw4<MODEL, NOISE>(p, L, r, g);
+        const bool live = step_block<MODEL, BOUND, NOISE, true>(p, L, r, g);
+        L.blk += 1;
+        if (!live) break;
+    }
+}
+
+// ------------------------------------------------------------------ host side
+struct Launcher {
+    template <int MODEL, int BOUND, bool NOISE>
+    static int run(const SingleParams &p, const ssm_launch *opt, cudaStream_t st) {
+        auto kern = k_single<MODEL, BOUND, NOISE>;
+        int threads = (opt && opt->block_threads > 0) ? opt->block_threads : 256;
+        if (threads > 256 || threads % 32) {
+            set_error("block_threads must be a multiple of 32 and at most 256");
+            return SSM_ERR_ARG;
+        }
+        int per_sm = 0;
+        SSM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, 0));
+        if (opt && opt->blocks_per_sm > 0 && opt->blocks_per_sm < per_sm) per_sm = opt->blocks_per_sm;
+        if (per_sm < 1) per_sm = 1;
+        const int grid = sm_count() * per_sm;
+        kern<<<grid, threads, 0, st>>>(p);
+        SSM_CUDA(cudaGetLastError());
+        if (p.traj && p.traj_len > 0) {
+            k_record<MODEL, BOUND, NOISE><<<1, 128, 0, st>>>(p);
+            SSM_CUDA(cudaGetLastError());
+        }
+        return SSM_OK;
+    }
+
+    template <int MODEL>
+    static int dispatch(int bound, bool noise, const SingleParams &p, const ssm_launch *opt,
+                        cudaStream_t st) {
+        if (MODEL == M_LEGACY) {
+            return noise ? run<MODEL, SSM_BOUND_CONSTANT, true>(p, opt, st)
+                         : run<MODEL, SSM_BOUND_CONSTANT, false>(p, opt, st);
+        }
+        switch (bound) {
+            case SSM_BOUND_TABLE:
+                return noise ? run<MODEL, SSM_BOUND_TABLE, true>(p, opt, st)
+                             : run<MODEL, SSM_BOUND_TABLE, false>(p, opt, st);
+            case SSM_BOUND_CONSTANT:
+                return noise ? run<MODEL, SSM_BOUND_CONSTANT, true>(p, opt, st)
+                             : run<MODEL, SSM_BOUND_CONSTANT, false>(p, opt, st);
+            case SSM_BOUND_LINEAR:
+                return noise ? run<MODEL, SSM_BOUND_LINEAR, true>(p, opt, st)
+                             : run<MODEL, SSM_BOUND_LINEAR, false>(p, opt, st);
+            case SSM_BOUND_WEIBULL:
+                return noise ? run<MODEL, SSM_BOUND_WEIBULL, true>(p, opt, st)
+                             : run<MODEL, SSM_BOUND_WEIBULL, false>(p, opt, st);
+            default:
+                set_error("unknown boundary kind %d", bound);
+                return SSM_ERR_ARG;
+        }
+    }
+};
+
+static size_t single_ws_bytes(int64_t n_trials) {
+    size_t b = sizeof(WorkspaceHeader) + (size_t)(n_trials > 0 ? n_trials : 0) * sizeof(TrialRow);
+    return (b + 255) & ~(size_t)255;
+}
+
+struct SingleCall {
+    int model;
+    const float *v, *a, *z, *alpha, *t, *deadline, *s;
+    int64_t n_trials, n_samples;
+    const int64_t *offsets;
+    float max_t;
+    const float *maxt_k;
+    float dt;
+    int bound;
+    const float *p1, *p2, *table;
+    int64_t tstride, tlen;
+    uint64_t seed;
+    int smooth;
+    const float *noise;
+    int64_t nlen;
+    const float *nunif;
+    float *rts;
+    int32_t *choices, *steps;
+    float *traj;
+    int64_t traj_len;
+    const ssm_launch *launch;
+    void *ws;
+    size_t ws_bytes;
+    void *stream;
+};
+
+static int run_single(const SingleCall &c) {
+    SSM_REQUIRE(c.n_trials >= 0 && c.n_samples >= 0, "n_trials and n_samples must be >= 0");
+    SSM_REQUIRE(c.dt > 0.f, "delta_t must be > 0");
+    SSM_REQUIRE(c.v && c.z && c.t && c.deadline && c.s && c.a, "v, a, z, t, deadline, s are required");
+    SSM_REQUIRE(c.rts && c.choices, "rts and choices outputs are required");
+    SSM_REQUIRE(c.model != M_LEVY || c.alpha, "alpha is required for the Levy model");
+    if (c.model != M_LEGACY) {
+        SSM_REQUIRE(c.bound >= SSM_BOUND_TABLE && c.bound <= SSM_BOUND_WEIBULL, "unknown boundary kind %d", c.bound);
+        SSM_REQUIRE(c.bound != SSM_BOUND_LINEAR || c.p1, "linear boundary needs bound_p1");
+        SSM_REQUIRE(c.bound != SSM_BOUND_WEIBULL || (c.p1 && c.p2), "weibull boundary needs bound_p1 and bound_p2");
+        SSM_REQUIRE(c.bound != SSM_BOUND_TABLE || (c.table && c.tlen >= 1 && c.tstride >= c.tlen),
+                    "table boundary needs bound_table with table_stride >= table_len >= 1");
+    }
+    SSM_REQUIRE(!c.noise || (c.nlen > 0 && c.nunif), "noise_rows needs noise_row_len > 0 and noise_unif");
+    SSM_REQUIRE(!c.traj || c.traj_len >= 1, "traj needs traj_len >= 1");
+    const size_t need = single_ws_bytes(c.n_trials);
+    if (!c.ws || c.ws_bytes < need || ((uintptr_t)c.ws & 255u)) {
+        set_error("workspace must be 256-byte aligned and hold %zu bytes", need);
+        return SSM_ERR_WORKSPACE;
+    }
+    cudaStream_t st = (cudaStream_t)c.stream;
+    WorkspaceHeader *hdr = (WorkspaceHeader *)c.ws;
+    TrialRow *rows = (TrialRow *)((char *)c.ws + sizeof(WorkspaceHeader));
+    SSM_CUDA(cudaMemsetAsync(hdr, 0, sizeof(WorkspaceHeader), st));
+    if (c.n_trials == 0) return SSM_OK;
+
+    PrepArgs A;
+    A.v = c.v; A.a = c.a; A.z = c.z; A.t = c.t; A.deadline = c.deadline; A.s = c.s;
+    A.alpha = c.alpha; A.p1 = c.p1; A.p2 = c.p2; A.maxt_k = c.maxt_k; A.table = c.table;
+    A.n_trials = c.n_trials; A.tstride = c.tstride; A.dt = c.dt;
+    A.sqrt_dt = (float)sqrt((double)c.dt);  // setup_simulation: sqrt(delta_t) -> float
+    A.max_t = c.max_t; A.model = c.model; A.bound = c.bound; A.rows = rows;
+    k_prep<<<(unsigned)((c.n_trials + 127) / 128), 128, 0, st>>>(A);
+    SSM_CUDA(cudaGetLastError());
+
+    SingleParams p;
+    p.key = philox_keys(c.seed);
+    p.rows = rows;
+    p.offsets = c.offsets;
+    p.n_trials = c.n_trials;
+    p.total = c.offsets ? -1 : c.n_trials * c.n_samples;
+    p.dt = c.dt;
+    p.smooth = c.smooth ? 1 : 0;
+    p.chunk = (c.launch && c.launch->chunk >= 32) ? c.launch->chunk : 64;
+    p.table = c.table; p.tstride = c.tstride; p.tlen = c.tlen;
+    p.noise = c.noise; p.nlen = c.nlen; p.nunif = c.nunif;
+    p.rts = c.rts; p.choices = c.choices; p.steps = c.steps;
+    p.hdr = hdr;
+    p.traj = c.traj; p.traj_len = c.traj_len;
+    if (p.total == 0) {
+        if (c.traj) {  // nothing simulated: trajectory metadata is all padding
+            p.traj_len = c.traj_len;
+        }
+        return SSM_OK;
+    }
+    const bool noise = c.noise != nullptr;
+    switch (c.model) {
+        case M_FLEX: return Launcher::dispatch<M_FLEX>(c.bound, noise, p, c.launch, st);
+        case M_LEGACY: return Launcher::dispatch<M_LEGACY>(c.bound, noise, p, c.launch, st);
+        default: return Launcher::dispatch<M_LEVY>(c.bound, noise, p, c.launch, st);
+    }
+}
+
+}  // namespace ssm
+
+extern "C" {
+
+size_t ssm_ddm_workspace_bytes(int64_t n_trials) { return ssm::single_ws_bytes(n_trials); }
+
+int ssm_ddm_flexbound(const float *v, const float *a, const float *z, const float *t,
+                      const float *deadline, const float *s, int64_t n_trials, int64_t n_samples,
+                      const int64_t *sample_offsets, float max_t, const float *max_t_per_trial,
+                      float delta_t, int bound_kind, const float *bound_p1, const float *bound_p2,
+                      const float *bound_table, int64_t table_stride, int64_t table_len,
+                      uint64_t seed, int smooth_unif, const float *noise_rows,
+                      int64_t noise_row_len, const float *noise_unif, float *rts,
+                      int32_t *choices, int32_t *steps, float *traj, int64_t traj_len,
+                      const ssm_launch *launch, void *workspace, size_t workspace_bytes,
+                      void *stream) {
+    ssm::SingleCall c{ssm::M_FLEX, v, a, z, nullptr, t, deadline, s, n_trials, n_samples,
+                      sample_offsets, max_t, max_t_per_trial, delta_t, bound_kind, bound_p1,
+                      bound_p2, bound_table, table_stride, table_len, seed, smooth_unif,
+                      noise_rows, noise_row_len, noise_unif, rts, choices, steps, traj,
+                      traj_len, launch, workspace, workspace_bytes, stream};
+    return ssm::run_single(c);
+}
+
+int ssm_ddm(const float *v, const float *a, const float *z, const float *t, const float *deadline,
+            const float *s, int64_t n_trials, int64_t n_samples, float max_t, float delta_t,
+            uint64_t seed, int smooth_unif, const float *noise_rows, int64_t noise_row_len,
+            const float *noise_unif, float *rts, int32_t *choices, int32_t *steps, float *traj,
+            int64_t traj_len, const ssm_launch *launch, void *workspace, size_t workspace_bytes,
+            void *stream) {
+    ssm::SingleCall c{ssm::M_LEGACY, v, a, z, nullptr, t, deadline, s, n_trials, n_samples,
+                      nullptr, max_t, nullptr, delta_t, SSM_BOUND_CONSTANT, nullptr, nullptr,
+                      nullptr, 0, 0, seed, smooth_unif, noise_rows, noise_row_len, noise_unif,
+                      rts, choices, steps, traj, traj_len, launch, workspace, workspace_bytes,
+                      stream};
+    return ssm::run_single(c);
+}
+
+int ssm_levy_flexbound(const float *v, const float *a, const float *z, const float *alpha,
+                       const float *t, const float *deadline, const float *s, int64_t n_trials,
+                       int64_t n_samples, const int64_t *sample_offsets, float max_t,
+                       float delta_t, int bound_kind, const float *bound_p1, const float *bound_p2,
+                       const float *bound_table, int64_t table_stride, int64_t table_len,
+                       uint64_t seed, int smooth_unif, const float *noise_rows,
+                       int64_t noise_row_len, const float *noise_unif, float *rts,
+                       int32_t *choices, int32_t *steps, float *traj, int64_t traj_len,
+                       const ssm_launch *launch, void *workspace, size_t workspace_bytes,
+                       void *stream) {
+    ssm::SingleCall c{ssm::M_LEVY, v, a, z, alpha, t, deadline, s, n_trials, n_samples,
+                      sample_offsets, max_t, nullptr, delta_t, bound_kind, bound_p1, bound_p2,
+                      bound_table, table_stride, table_len, seed, smooth_unif, noise_rows,
+                      noise_row_len, noise_unif, rts, choices, steps, traj, traj_len, launch,
+                      workspace, workspace_bytes, stream};
+    return ssm::run_single(c);
+}
+
+}  // extern "C"

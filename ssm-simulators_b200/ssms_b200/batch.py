@@ -1,0 +1,129 @@
+"""Batched simulation: thousands of parameter vectors with uneven n_samples
+(and optionally uneven max_t) in ONE persistent launch, optionally captured
+in a CUDA graph.
+
+The reference simulates one scalar n_samples for all trials and loops over
+parameter sets in Python/processes (ssms/dataset_generators/lan_mlp.py:489-498).
+Here the trials are laid out ragged -- trial k owns outputs
+[offsets[k], offsets[k+1]) -- and a single persistent grid drains the whole
+set from a work counter.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from . import _device as D
+from . import _lib
+from . import boundary_functions as bf
+from . import device as dev
+
+# model name -> (simulator family, boundary name, boundary parameter names)
+BATCH_MODELS = {
+    "ddm": ("ddm_flexbound", "constant", ["a"]),
+    "angle": ("ddm_flexbound", "angle", ["a", "theta"]),
+    "weibull": ("ddm_flexbound", "weibull_cdf", ["a", "alpha", "beta"]),
+    "ddm_legacy": ("ddm", None, []),
+    "levy": ("levy_flexbound", "constant", ["a"]),
+    "levy_angle": ("levy_flexbound", "angle", ["a", "theta"]),
+}
+
+
+class BatchedSimulator:
+    """Device-resident batch of trials for the single-accumulator models.
+
+    theta: dict of per-trial float32 arrays (model parameter names, e.g.
+    v, a, z, t, theta for "angle"); n_samples: int array [n_trials].
+    """
+
+    def __init__(self, model: str, theta: dict, n_samples, *, max_t: float = 20.0,
+                 max_t_per_trial=None, delta_t: float = 0.001, seed: int = 0,
+                 smooth_unif: bool = True, s=None, deadline=None, launch=None):
+        if model not in BATCH_MODELS:
+            raise ValueError(f"unsupported batched model {model!r}; choose from {sorted(BATCH_MODELS)}")
+        family, bname, bkeys = BATCH_MODELS[model]
+        D.require_cuda()
+        self.model, self.family = model, family
+        ns = np.asarray(n_samples, dtype=np.int64).reshape(-1)
+        K = ns.shape[0]
+        if np.any(ns < 0):
+            raise ValueError("n_samples must be >= 0")
+        self.n_trials = K
+        self.offsets_host = np.concatenate([[0], np.cumsum(ns)]).astype(np.int64)
+        self.total = int(self.offsets_host[-1])
+        f = lambda x: np.asarray(x, dtype=np.float32).reshape(-1)  # noqa: E731
+        th = {k: f(v) for k, v in theta.items()}
+        self.v, self.z, self.t = (D.to_dev_f32(th[k], K, k) for k in ("v", "z", "t"))
+        self.a = D.to_dev_f32(th.get("a", np.ones(K, np.float32)), K, "a")
+        self.s = D.to_dev_f32(np.ones(K, np.float32) if s is None else f(s), K, "s")
+        self.deadline = D.to_dev_f32(np.full(K, 999.0, np.float32) if deadline is None else f(deadline), K, "deadline")
+        self.alpha = D.to_dev_f32(th["alpha"], K, "alpha") if family == "levy_flexbound" else None
+        self.max_t = float(max_t)
+        self.max_t_k = None if max_t_per_trial is None else D.to_dev_f32(f(max_t_per_trial), K, "max_t_per_trial")
+        self.delta_t = float(delta_t)
+        self.seed = int(seed)
+        self.smooth = bool(smooth_unif)
+        self.launch = launch
+        if family == "ddm":
+            self.spec = {"kind": _lib.BOUND_CONSTANT, "p1": None, "p2": None, "table": None}
+        else:
+            fun = bf.BOUNDARIES[bname][0]
+            bp = {k: th[k] for k in bkeys}
+            self.spec = bf.kernel_spec(fun, bp, K, bf.make_t_s(max(max_t, float(np.max(max_t_per_trial)) if max_t_per_trial is not None else max_t), delta_t))
+        self.table = None
+        if self.spec["table"] is not None:
+            self.table = torch.from_numpy(np.ascontiguousarray(self.spec["table"])).cuda()
+        self.p1 = None if self.spec["p1"] is None else D.to_dev_f32(self.spec["p1"], K, "p1")
+        self.p2 = None if self.spec["p2"] is None else D.to_dev_f32(self.spec["p2"], K, "p2")
+        self.offsets = torch.from_numpy(self.offsets_host).cuda()
+        self.rts = torch.empty(self.total, dtype=torch.float32, device="cuda")
+        self.choices = torch.empty(self.total, dtype=torch.int32, device="cuda")
+        self.graph: torch.cuda.CUDAGraph | None = None
+        self.last = None
+
+    def run(self, want_steps: bool = False, launch=None) -> dev.SimOutput:
+        """Launch the batch on the current stream (asynchronous)."""
+        if self.family == "ddm" and self.max_t_k is not None:
+            raise ValueError("per-trial max_t is supported by the flexible-bound families")
+        self.last = dev.simulate_single(
+            self.family, v=self.v, z=self.z, t=self.t, deadline=self.deadline, s=self.s, a=self.a,
+            alpha=self.alpha, n_trials=self.n_trials, sample_offsets=self.offsets,
+            max_t=self.max_t, max_t_per_trial=self.max_t_k, delta_t=self.delta_t,
+            bound_kind=self.spec["kind"], bound_p1=self.p1, bound_p2=self.p2,
+            bound_table=self.table, seed=self.seed, smooth_unif=self.smooth,
+            want_steps=want_steps, out_rts=self.rts, out_choices=self.choices,
+            launch=launch if launch is not None else self.launch)
+        return self.last
+
+    def capture(self) -> torch.cuda.CUDAGraph:
+        """Capture one launch of the whole batch in a CUDA graph (replay() reruns it)."""
+        torch.cuda.synchronize()
+        self.run()  # warm-up outside capture (allocates the cached workspace)
+        torch.cuda.synchronize()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            self.run()
+        self.graph = g
+        return g
+
+    def replay(self) -> None:
+        if self.graph is None:
+            self.capture()
+        self.graph.replay()
+
+    def to_host(self) -> tuple[np.ndarray, np.ndarray]:
+        return self.rts.cpu().numpy(), self.choices.cpu().numpy()
+
+    def split(self, rts: np.ndarray, choices: np.ndarray, k: int):
+        lo, hi = self.offsets_host[k], self.offsets_host[k + 1]
+        return rts[lo:hi], choices[lo:hi]
+
+
+def simulate_batch(model: str, theta: dict, n_samples, **kw) -> dict:
+    """One-call batched simulation returning host arrays in the ragged layout:
+    {"rts": f32[total], "choices": i32[total], "offsets": i64[n_trials+1]}."""
+    sim = BatchedSimulator(model, theta, n_samples, **kw)
+    sim.run()
+    rts, chs = sim.to_host()
+    return {"rts": rts, "choices": chs, "offsets": sim.offsets_host}

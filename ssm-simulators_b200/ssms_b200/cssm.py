@@ -1,0 +1,152 @@
+"""Drop-in replacements for the reference's ``cssm`` simulator entry points.
+
+Same names, arguments, defaults, return dicts and errors as the reference's
+Cython functions; the simulation itself runs in ``libssm_b200.so`` on the GPU.
+Inputs are float32 numpy arrays as in the reference; outputs are numpy arrays
+in the reference layout ``[n_samples, n_trials, 1]``.  ``n_threads`` is
+accepted and ignored (there is no thread-count gate on the device) and is
+reported as 1, which is what the reference reports on hosts without GSL.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+
+from . import _lib
+from . import boundary_functions as bf
+from . import device as dev
+
+DTYPE = np.float32
+
+
+def _f32(x, name):
+    arr = np.asarray(x)
+    if arr.dtype != np.float32:
+        arr = arr.astype(np.float32)
+    return np.ascontiguousarray(arr)
+
+
+def _seed(random_state):
+    if random_state is None:
+        return int(np.random.randint(0, 2**31))
+    return int(random_state)
+
+
+def _num_draws(max_t, delta_t) -> int:
+    # int(float32(max_t) / float32(delta_t) + 1) in float32 arithmetic (_utils.pyx:616)
+    return int(np.float32(np.float32(max_t) / np.float32(delta_t)) + np.float32(1))
+
+
+def _check_return_option(return_option):
+    if return_option not in ("full", "minimal"):
+        raise ValueError('return_option must be either "full" or "minimal"')
+
+
+def _minimal_meta(name, choices, n_samples, n_trials, boundary_name=None):
+    meta = {"simulator": name, "possible_choices": choices, "n_samples": n_samples,
+            "n_trials": n_trials}
+    if boundary_name is not None:
+        meta["boundary_fun_type"] = boundary_name
+    return meta
+
+
+def _traj_host(traj_t, n):
+    traj = np.full((n, 1), -999, dtype=DTYPE)
+    if traj_t is not None:
+        traj[:, 0] = traj_t.cpu().numpy()[:n]
+    return traj
+
+
+def _run_flex(model, v, a, z, t, deadline, s, alpha, max_t, delta_t, n_samples, n_trials,
+              boundary_fun, boundary_params, random_state, return_option, smooth_unif,
+              **kwargs):
+    _check_return_option(return_option)
+    n_trials = int(n_trials)
+    n_samples = int(n_samples)
+    if boundary_fun is None:
+        raise TypeError("boundary_fun is required")
+    v, a, z, t, deadline, s = (_f32(x, nm) for x, nm in
+                               ((v, "v"), (a, "a"), (z, "z"), (t, "t"), (deadline, "deadline"), (s, "s")))
+    t_s = bf.make_t_s(max_t, delta_t)
+    spec = bf.kernel_spec(boundary_fun, boundary_params, n_trials, t_s,
+                          force_table=bool(kwargs.get("_force_table", False)))
+    full = return_option == "full"
+    nd = _num_draws(max_t, delta_t)
+    out = dev.simulate_single(
+        model, v=v, z=z, t=t, deadline=deadline, s=s, a=spec["a"],
+        alpha=None if alpha is None else _f32(alpha, "alpha"), n_trials=n_trials,
+        n_samples=n_samples, max_t=max_t, delta_t=delta_t, bound_kind=spec["kind"],
+        bound_p1=spec["p1"], bound_p2=spec["p2"], bound_table=spec["table"],
+        seed=_seed(random_state), smooth_unif=smooth_unif,
+        traj_len=nd if (full and n_trials > 0 and n_samples > 0) else 0)
+    rts = out.rts.cpu().numpy().reshape(n_samples, n_trials, 1)
+    choices = out.choices.cpu().numpy().reshape(n_samples, n_trials, 1)
+    minimal = _minimal_meta(model, [-1, 1], n_samples, n_trials, boundary_fun.__name__)
+    if not full:
+        return {"rts": rts, "choices": choices, "metadata": minimal}
+    meta = dict(minimal)
+    if model == "levy_flexbound":
+        meta.update({"v": v, "z": z, "t": t, "alpha": alpha, "s": s})
+    else:
+        meta.update({"v": v, "a": a, "z": z, "t": t, "s": s, "deadline": deadline})
+    meta.update({"delta_t": float(np.float32(delta_t)), "max_t": float(np.float32(max_t)),
+                 "n_threads": 1})
+    meta["boundary_fun_type"] = boundary_fun.__name__
+    boundary = np.zeros(t_s.shape, dtype=DTYPE)
+    if n_trials > 0:
+        bp0 = {key: np.asarray(val)[0] for key, val in boundary_params.items()}
+        boundary[:] = np.asarray(boundary_fun(t=t_s, **bp0)).astype(DTYPE)
+    meta["boundary"] = boundary
+    meta["trajectory"] = _traj_host(out.traj, nd)
+    if boundary_params:
+        meta.update(boundary_params)
+    return {"rts": rts, "choices": choices, "metadata": meta}
+
+
+def ddm_flexbound(v, a, z, t, deadline, s, max_t=20, delta_t=0.001, n_samples=20000,
+                  n_trials=1, boundary_fun=None, boundary_params={}, random_state=None,  # noqa: B006
+                  return_option="full", smooth_unif=False, n_threads=1, **kwargs):
+    """DDM with flexible symmetric bounds +-b(t) (src/cssm/ddm_models.pyx:589-878)."""
+    return _run_flex("ddm_flexbound", v, a, z, t, deadline, s, None, max_t, delta_t, n_samples,
+                     n_trials, boundary_fun, boundary_params, random_state, return_option,
+                     smooth_unif, **kwargs)
+
+
+def levy_flexbound(v, z, alpha, t, deadline, s, delta_t=0.001, max_t=20, n_samples=20000,
+                   n_trials=1, boundary_fun=None, boundary_params={}, random_state=None,  # noqa: B006
+                   return_option="full", smooth_unif=False, n_threads=1, **kwargs):
+    """Levy-flight DDM with alpha-stable increments (src/cssm/levy_models.pyx:47-348)."""
+    a = np.asarray(boundary_params.get("a", np.ones(int(n_trials))), dtype=np.float32)
+    return _run_flex("levy_flexbound", v, a, z, t, deadline, s, alpha, max_t, delta_t, n_samples,
+                     n_trials, boundary_fun, boundary_params, random_state, return_option,
+                     smooth_unif, **kwargs)
+
+
+def ddm(v, a, z, t, deadline, s, max_t=20, delta_t=0.001, n_samples=20000, n_trials=10,
+        random_state=None, return_option="full", smooth_unif=False, n_threads=1, **kwargs):
+    """Legacy DDM on [0, a] (src/cssm/ddm_models.pyx:349-582)."""
+    _check_return_option(return_option)
+    n_trials = int(n_trials)
+    n_samples = int(n_samples)
+    v, a, z, t, deadline, s = (_f32(x, nm) for x, nm in
+                               ((v, "v"), (a, "a"), (z, "z"), (t, "t"), (deadline, "deadline"), (s, "s")))
+    full = return_option == "full"
+    nd = _num_draws(max_t, delta_t)
+    out = dev.simulate_single(
+        "ddm", v=v, z=z, t=t, deadline=deadline, s=s, a=a, n_trials=n_trials,
+        n_samples=n_samples, max_t=max_t, delta_t=delta_t, seed=_seed(random_state),
+        smooth_unif=smooth_unif, traj_len=nd if (full and n_trials > 0 and n_samples > 0) else 0)
+    rts = out.rts.cpu().numpy().reshape(n_samples, n_trials, 1)
+    choices = out.choices.cpu().numpy().reshape(n_samples, n_trials, 1)
+    minimal = _minimal_meta("ddm", [-1, 1], n_samples, n_trials, "constant")
+    if not full:
+        return {"rts": rts, "choices": choices, "metadata": minimal}
+    meta = dict(minimal)
+    meta.update({"v": v, "a": a, "z": z, "t": t, "deadline": deadline, "s": s})
+    meta.update({"delta_t": float(np.float32(delta_t)), "max_t": max_t, "n_threads": 1})
+    meta["trajectory"] = _traj_host(out.traj, nd)
+    return {"rts": rts, "choices": choices, "metadata": meta}
+
+
+__all__ = ["ddm", "ddm_flexbound", "levy_flexbound"]
+_ = _lib  # the C ABI is loaded lazily on the first call

@@ -1,0 +1,129 @@
+"""Tensor-level API: run the sm_100a simulators on CUDA tensors.
+
+These functions are the thin layer over the C ABI.  Inputs may be numpy
+arrays or tensors; outputs stay on the device (no host copy), which is what
+batched pipelines (KDE training data, surrogate training) consume.  The
+numpy/dict API of the reference package lives in ``ssms_b200.cssm``.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from . import _device as D
+from . import _lib
+from .tuning import launch_for
+
+MODEL_FLEX = "ddm_flexbound"
+MODEL_LEGACY = "ddm"
+MODEL_LEVY = "levy_flexbound"
+
+
+@dataclass
+class SimOutput:
+    rts: torch.Tensor             # float32 [total]
+    choices: torch.Tensor         # int32 [total]
+    steps: torch.Tensor | None    # int32 [total] (Euler steps per trajectory)
+    traj: torch.Tensor | None     # float32 [traj_len] trial-0/sample-0 path
+    workspace: torch.Tensor       # scratch used by the launch (holds the device status word)
+
+
+def _opt_f32(x, n, name):
+    return None if x is None else D.to_dev_f32(x, n, name)
+
+
+def simulate_single(model: str, *, v, z, t, deadline, s, a=None, alpha=None,
+                    n_trials: int, n_samples: int = 0, sample_offsets=None,
+                    max_t: float = 20.0, max_t_per_trial=None, delta_t: float = 0.001,
+                    bound_kind: int = _lib.BOUND_CONSTANT, bound_p1=None, bound_p2=None,
+                    bound_table=None, seed: int = 0, smooth_unif: bool = False,
+                    noise_rows=None, noise_unif=None, want_steps: bool = False,
+                    traj_len: int = 0, out_rts: torch.Tensor | None = None,
+                    out_choices: torch.Tensor | None = None, launch=None,
+                    stream: torch.cuda.Stream | None = None) -> SimOutput:
+    """Simulate the single-accumulator family on the current CUDA device.
+
+    ``sample_offsets`` (int64 [n_trials+1]) switches to the ragged layout where
+    trial k owns outputs [offsets[k], offsets[k+1]); otherwise the output index
+    of (sample n, trial k) is n * n_trials + k as in the reference.
+    """
+    dev = D.require_cuda()
+    K = int(n_trials)
+    vt = D.to_dev_f32(v, K, "v")
+    zt = D.to_dev_f32(z, K, "z")
+    tt = D.to_dev_f32(t, K, "t")
+    dlt = D.to_dev_f32(deadline, K, "deadline")
+    st = D.to_dev_f32(s, K, "s")
+    at = D.to_dev_f32(a if a is not None else np.ones(K, np.float32), K, "a")
+    alt = _opt_f32(alpha, K, "alpha")
+    p1t = _opt_f32(bound_p1, K, "bound_p1")
+    p2t = _opt_f32(bound_p2, K, "bound_p2")
+    mtk = _opt_f32(max_t_per_trial, K, "max_t_per_trial")
+    tab = None
+    tstride = tlen = 0
+    if bound_table is not None:
+        tab = D.to_dev_f32(bound_table).reshape(-1)
+        tlen = int(np.shape(bound_table)[-1]) if not isinstance(bound_table, torch.Tensor) else int(bound_table.shape[-1])
+        tstride = tlen
+    if sample_offsets is not None:
+        offs = sample_offsets
+        if not isinstance(offs, torch.Tensor):
+            offs = torch.as_tensor(np.asarray(offs, dtype=np.int64))
+        offs = offs.to(device=dev, dtype=torch.int64).contiguous()
+        if offs.numel() != K + 1:
+            raise ValueError("sample_offsets must have n_trials + 1 entries")
+        total = int(offs[-1].item()) if out_rts is None else out_rts.numel()
+    else:
+        offs = None
+        total = K * int(n_samples)
+    rts = out_rts if out_rts is not None else torch.empty(total, dtype=torch.float32, device=dev)
+    chs = out_choices if out_choices is not None else torch.empty(total, dtype=torch.int32, device=dev)
+    steps = torch.empty(total, dtype=torch.int32, device=dev) if want_steps else None
+    traj = torch.empty(int(traj_len), dtype=torch.float32, device=dev) if traj_len > 0 else None
+    nrows = nunif = None
+    nlen = 0
+    if noise_rows is not None:
+        nrows = D.to_dev_f32(noise_rows)
+        nlen = int(np.shape(noise_rows)[-1]) if not isinstance(noise_rows, torch.Tensor) else int(noise_rows.shape[-1])
+        nunif = D.to_dev_f32(noise_unif, total, "noise_unif")
+        if nrows.numel() < total * nlen:
+            raise ValueError("noise_rows must hold one row per trajectory")
+    L = _lib.lib()
+    ws = D.workspace(L.ssm_ddm_workspace_bytes(K), tag=0, stream=stream)
+    lopt = launch if launch is not None else launch_for(model)
+    sp = D.stream_ptr(stream)
+    common_tail = (
+        _lib.U64_cast(seed), int(bool(smooth_unif)), D.ptr(nrows), nlen, D.ptr(nunif),
+        D.ptr(rts), D.ptr(chs), D.ptr(steps), D.ptr(traj), int(traj_len),
+    )
+    if model == MODEL_FLEX:
+        status = L.ssm_ddm_flexbound(
+            D.ptr(vt), D.ptr(at), D.ptr(zt), D.ptr(tt), D.ptr(dlt), D.ptr(st), K, int(n_samples),
+            D.ptr(offs), float(np.float32(max_t)), D.ptr(mtk), float(np.float32(delta_t)),
+            int(bound_kind), D.ptr(p1t), D.ptr(p2t), D.ptr(tab), tstride, tlen, *common_tail,
+            ctypes.addressof(lopt), D.ptr(ws), ws.numel(), sp)
+    elif model == MODEL_LEGACY:
+        status = L.ssm_ddm(
+            D.ptr(vt), D.ptr(at), D.ptr(zt), D.ptr(tt), D.ptr(dlt), D.ptr(st), K, int(n_samples),
+            float(np.float32(max_t)), float(np.float32(delta_t)), *common_tail,
+            ctypes.addressof(lopt), D.ptr(ws), ws.numel(), sp)
+    elif model == MODEL_LEVY:
+        if alt is None:
+            raise ValueError("levy_flexbound needs alpha")
+        status = L.ssm_levy_flexbound(
+            D.ptr(vt), D.ptr(at), D.ptr(zt), D.ptr(alt), D.ptr(tt), D.ptr(dlt), D.ptr(st), K,
+            int(n_samples), D.ptr(offs), float(np.float32(max_t)), float(np.float32(delta_t)),
+            int(bound_kind), D.ptr(p1t), D.ptr(p2t), D.ptr(tab), tstride, tlen, *common_tail,
+            ctypes.addressof(lopt), D.ptr(ws), ws.numel(), sp)
+    else:
+        raise ValueError(f"unknown single-accumulator model {model!r}")
+    _lib.check(status)
+    if noise_rows is not None:
+        _lib.check(L.ssm_check_status(D.ptr(ws), sp))
+    return SimOutput(rts=rts, choices=chs, steps=steps, traj=traj, workspace=ws)
+
+
