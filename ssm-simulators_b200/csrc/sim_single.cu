@@ -39,7 +39,8 @@ struct alignas(16) TrialRow {
     float alpha;     // Levy stability index
     float inv_alpha; // 1 / alpha
     float expo;      // (1 - alpha) / alpha
-    float pad[2];
+    int cap;         // hard limit on Euler steps: a walk reaching it raises SSM_ERR_DEVICE
+    int pad;
 };
 static_assert(sizeof(TrialRow) == 64, "TrialRow is one 64-byte line");
 
@@ -93,7 +94,14 @@ __global__ void k_prep(const PrepArgs A) {
     r.alpha = A.alpha ? A.alpha[k] : 2.f;
     r.inv_alpha = (float)(1.0 / (double)r.alpha);
     r.expo = (float)((1.0 - (double)r.alpha) / (double)r.alpha);
-    r.pad[0] = r.pad[1] = 0.f;
+    r.pad = 0;
+    // The walk stops once the float32 time passes dl_tmp, i.e. after about
+    // dl_tmp/dt steps; twice that plus slack bounds every legal walk.  A stalled
+    // accumulator (dt below half an ulp of t) or an infinite horizon hits the cap.
+    const double nsteps = (double)r.dl_tmp / (double)dt;
+    if (!(nsteps > 0.0)) r.cap = 64;                      // NaN or <= 0: at most one step
+    else if (nsteps <= 8388608.0) r.cap = (int)(2.0 * nsteps) + 64;
+    else r.cap = 0;                                       // unsupported horizon: flagged
     if (A.model == M_LEVY) {
         // delta_t_alpha = s * pow(delta_t, 1.0 / alpha) in double (levy_models.pyx:166)
         r.scale = __double2float_rn((double)A.s[k] * pow((double)dt, 1.0 / (double)r.alpha));
@@ -207,6 +215,10 @@ __device__ __forceinline__ void draw4(const SingleParams &p, const Lane &L, cons
 template <int MODEL, int BOUND, bool NOISE, bool RECORD>
 __device__ __forceinline__ bool step_block(const SingleParams &p, Lane &L, const TrialRow &r,
                                            const float g[4]) {
+    if (L.ix >= r.cap) {
+        raise_error(p.hdr, SSM_ERR_DEVICE, (int)L.w);
+        return false;
+    }
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
         bool inside;
@@ -441,7 +453,9 @@ struct SingleCall {
 
 static int run_single(const SingleCall &c) {
     SSM_REQUIRE(c.n_trials >= 0 && c.n_samples >= 0, "n_trials and n_samples must be >= 0");
-    SSM_REQUIRE(c.dt > 0.f, "delta_t must be > 0");
+    SSM_REQUIRE(c.dt > 0.f && isfinite(c.dt), "delta_t must be finite and > 0");
+    SSM_REQUIRE(c.maxt_k || (isfinite(c.max_t) && (double)c.max_t / (double)c.dt <= 8388608.0),
+                "max_t must be finite with max_t / delta_t <= 2^23");
     SSM_REQUIRE(c.v && c.z && c.t && c.deadline && c.s && c.a, "v, a, z, t, deadline, s are required");
     SSM_REQUIRE(c.rts && c.choices, "rts and choices outputs are required");
     SSM_REQUIRE(c.model != M_LEVY || c.alpha, "alpha is required for the Levy model");

@@ -69,6 +69,8 @@ def simulate_single(model: str, *, v, z, t, deadline, s, a=None, alpha=None,
         tab = D.to_dev_f32(bound_table).reshape(-1)
         tlen = int(np.shape(bound_table)[-1]) if not isinstance(bound_table, torch.Tensor) else int(bound_table.shape[-1])
         tstride = tlen
+        if tlen < 1 or tab.numel() < K * tstride:
+            raise ValueError("bound_table must be float32 [n_trials, table_len]")
     if sample_offsets is not None:
         offs = sample_offsets
         if not isinstance(offs, torch.Tensor):
