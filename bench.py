@@ -214,7 +214,7 @@ def run_ours(args, rank, world, local_rank):
     from ssms_b200.batch import BatchedSimulator
 
     torch.cuda.set_device(local_rank)
-    theta, n_samples = workload(SEED)
+    theta, n_samples = workload(SEED, args.n_theta)
     sim = BatchedSimulator("angle", theta, n_samples, max_t=20.0, delta_t=0.001,
                            seed=SEED + 7919 * rank, smooth_unif=True)
     total = sim.total
@@ -294,7 +294,7 @@ def run_ours(args, rank, world, local_rank):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded uniform parameter draws; no dataset)",
-        "config": {"workload": WORKLOAD, "n_theta": N_THETA, "trajectories_per_step": total,
+        "config": {"workload": WORKLOAD, "n_theta": args.n_theta, "trajectories_per_step": total,
                    "accumulator_steps_per_step": steps_per_launch, "seed": SEED,
                    "l2": "flushed (256 MB write) between timed steps", "parallelism": f"replicas x{world}"},
         "roofline": {"bound": "issue", "achieved": achieved_steps / 1e9, "peak": peak_steps / 1e9,
@@ -346,6 +346,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--n-theta", type=int, default=N_THETA,
+                    help="parameter vectors per step (smaller values only for profiling captures)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

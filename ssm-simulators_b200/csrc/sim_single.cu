@@ -11,14 +11,22 @@
 //    (ballot), the warp hands them the next trajectories of its chunk
 //    (popc rank), so lanes never idle while work remains and divergence
 //    between fast and slow trajectories costs at most one 4-step block.
-//  * Steps run in blocks of four: one Philox4x32-10 call yields four 32-bit
-//    words = two Box-Muller pairs = the four N(0,1) increments of the block.
+//  * Steps run in blocks of eight: two independent Philox4x32-10 calls yield
+//    eight 32-bit words = four Box-Muller pairs = the block's increments,
+//    already scaled to drift + s sqrt(dt) N(0,1); the steps themselves are
+//    predicated (no per-step branch).
 //  * Boundaries are evaluated in registers (constant / linear collapse /
 //    Weibull) or read from a caller-evaluated table for arbitrary shapes.
 //  * Noise injection replaces the generator by caller rows and switches every
 //    float operation to explicit round-to-nearest intrinsics, giving results
 //    bit-identical to the sequential CPU restatement.
 #include "common.cuh"
+
+
+// Resident CTAs per SM the compiler must fit (register cap 65536 / (256 * n)).
+#ifndef SSM_MIN_CTAS
+#define SSM_MIN_CTAS 4
+#endif
 
 namespace ssm {
 
@@ -39,8 +47,8 @@ struct alignas(16) TrialRow {
     float alpha;     // Levy stability index
     float inv_alpha; // 1 / alpha
     float expo;      // (1 - alpha) / alpha
-    int cap;         // hard limit on Euler steps: a walk reaching it raises SSM_ERR_DEVICE
-    int pad;
+    float capf;      // hard limit on Euler steps: a walk reaching it raises SSM_ERR_DEVICE
+    float c2;        // -2 ln(2) * scale^2: folds the noise scale into Box-Muller's radius
 };
 static_assert(sizeof(TrialRow) == 64, "TrialRow is one 64-byte line");
 
@@ -94,20 +102,20 @@ __global__ void k_prep(const PrepArgs A) {
     r.alpha = A.alpha ? A.alpha[k] : 2.f;
     r.inv_alpha = (float)(1.0 / (double)r.alpha);
     r.expo = (float)((1.0 - (double)r.alpha) / (double)r.alpha);
-    r.pad = 0;
     // The walk stops once the float32 time passes dl_tmp, i.e. after about
     // dl_tmp/dt steps; twice that plus slack bounds every legal walk.  A stalled
     // accumulator (dt below half an ulp of t) or an infinite horizon hits the cap.
     const double nsteps = (double)r.dl_tmp / (double)dt;
-    if (!(nsteps > 0.0)) r.cap = 64;                      // NaN or <= 0: at most one step
-    else if (nsteps <= 8388608.0) r.cap = (int)(2.0 * nsteps) + 64;
-    else r.cap = 0;                                       // unsupported horizon: flagged
+    if (!(nsteps > 0.0)) r.capf = 64.f;                   // NaN or <= 0: at most one step
+    else if (nsteps <= 8388608.0) r.capf = (float)(int)(2.0 * nsteps + 64.0);
+    else r.capf = 0.f;                                    // unsupported horizon: flagged
     if (A.model == M_LEVY) {
         // delta_t_alpha = s * pow(delta_t, 1.0 / alpha) in double (levy_models.pyx:166)
         r.scale = __double2float_rn((double)A.s[k] * pow((double)dt, 1.0 / (double)r.alpha));
     } else {
         r.scale = __fmul_rn(A.sqrt_dt, A.s[k]);  // ddm_models.pyx:705
     }
+    r.c2 = -1.3862944f * r.scale * r.scale;
     if (A.model == M_LEGACY) {
         r.y0 = __fmul_rn(A.z[k], r.a);  // ddm_models.pyx:451
     } else {
@@ -177,79 +185,110 @@ __device__ __forceinline__ float cms_stable(uint32_t bu, uint32_t bw, const Tria
     return fminf(fmaxf(X, -1e10f), 1e10f);
 }
 
+// Euler steps per block: two Philox4x32-10 calls give the eight increments.
+constexpr int BLK = 8;
+
 struct Lane {
     int64_t w;
     uint32_t k, n, blk;
-    int ix;
-    float y, tp, ixf;
+    int ix;           // steps taken (maintained where an integer index is needed)
+    float y, tp, ixf; // position, float32 time accumulator, steps taken as float
 };
 
-// Four increments for the lane's current step block.
+// Box-Muller pair already scaled into Euler increments: drift + scale * N(0,1).
+// c2 = -2 ln(2) scale^2, so r = sqrt(c2 * log2(u1)) = scale * sqrt(-2 ln u1).
+__device__ __forceinline__ void bm_increment(uint32_t a, uint32_t b, float c2, float drift,
+                                             float &g0, float &g1) {
+    const float u1 = __uint_as_float(0x3f800000u | (a & 0x007fffffu)) - 0.99999994f;  // (0, 1)
+    const float ang = fmaf(__uint_as_float(0x3f800000u | (b & 0x007fffffu)), 6.2831853f, -6.2831853f);
+    const float e = c2 * __log2f(u1);
+    float r;
+    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(e));
+    float sn, cs;
+    __sincosf(ang, &sn, &cs);
+    g0 = fmaf(r, cs, drift);
+    g1 = fmaf(r, sn, drift);
+}
+
+// The block's increments.  Noise injection returns the raw caller draws (the
+// step applies drift and scale with explicit rounding); the device RNG returns
+// finished increments drift + scale * X.
 template <int MODEL, bool NOISE>
-__device__ __forceinline__ void draw4(const SingleParams &p, const Lane &L, const TrialRow &r,
-                                      float g[4]) {
+__device__ __forceinline__ void draw_block(const SingleParams &p, const Lane &L, const TrialRow &r,
+                                           float g[BLK]) {
     if (NOISE) {
         const float *row = p.noise + L.w * p.nlen;
 #pragma unroll
-        for (int q = 0; q < 4; ++q) g[q] = (L.ix + q < p.nlen) ? __ldg(row + L.ix + q) : 0.f;
+        for (int q = 0; q < BLK; ++q) g[q] = (L.ix + q < p.nlen) ? __ldg(row + L.ix + q) : 0.f;
     } else if (MODEL == M_LEVY) {
-        const uint4 b0 = philox10(make_uint4(L.blk, L.n, L.k, 0u), p.key);
-        const uint4 b1 = philox10(make_uint4(L.blk, L.n, L.k, 2u), p.key);
-        g[0] = cms_stable(b0.x, b0.y, r);
-        g[1] = cms_stable(b0.z, b0.w, r);
-        g[2] = cms_stable(b1.x, b1.y, r);
-        g[3] = cms_stable(b1.z, b1.w, r);
+#pragma unroll
+        for (int h = 0; h < BLK / 2; h += 2) {
+            const uint4 b = philox10(make_uint4(L.blk, L.n, L.k, 2u + (uint32_t)h), p.key);
+            g[2 * h + 0] = fmaf(r.scale, cms_stable(b.x, b.y, r), r.drift);
+            g[2 * h + 1] = fmaf(r.scale, cms_stable(b.z, b.w, r), r.drift);
+            const uint4 c = philox10(make_uint4(L.blk, L.n, L.k, 3u + (uint32_t)h), p.key);
+            g[2 * h + 2] = fmaf(r.scale, cms_stable(c.x, c.y, r), r.drift);
+            g[2 * h + 3] = fmaf(r.scale, cms_stable(c.z, c.w, r), r.drift);
+        }
     } else {
-        const uint4 b = philox10(make_uint4(L.blk, L.n, L.k, 0u), p.key);
-        const float2 n0 = box_muller(b.x, b.y);
-        const float2 n1 = box_muller(b.z, b.w);
-        g[0] = n0.x;
-        g[1] = n0.y;
-        g[2] = n1.x;
-        g[3] = n1.y;
+        const uint4 b0 = philox10(make_uint4(2u * L.blk, L.n, L.k, 0u), p.key);
+        const uint4 b1 = philox10(make_uint4(2u * L.blk + 1u, L.n, L.k, 0u), p.key);
+        bm_increment(b0.x, b0.y, r.c2, r.drift, g[0], g[1]);
+        bm_increment(b0.z, b0.w, r.c2, r.drift, g[2], g[3]);
+        bm_increment(b1.x, b1.y, r.c2, r.drift, g[4], g[5]);
+        bm_increment(b1.z, b1.w, r.c2, r.drift, g[6], g[7]);
     }
 }
 
-// Advance one lane by up to four Euler steps; returns false once the walk has
-// stopped (the reference's `while` condition failed before a step).
+// Advance one lane by up to BLK Euler steps.  Every step first tests the
+// reference's `while` condition (ddm_models.pyx:719; legacy DDM :451); once it
+// fails the remaining steps of the block are predicated off.  Returns whether
+// the walk is still running.
 template <int MODEL, int BOUND, bool NOISE, bool RECORD>
 __device__ __forceinline__ bool step_block(const SingleParams &p, Lane &L, const TrialRow &r,
-                                           const float g[4]) {
-    if (L.ix >= r.cap) {
+                                           const float g[BLK]) {
+    if (L.ixf >= r.capf) {
         raise_error(p.hdr, SSM_ERR_DEVICE, (int)L.w);
         return false;
     }
+    constexpr bool INT_IX = NOISE || RECORD || BOUND == SSM_BOUND_TABLE;
+    bool live = true;
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
+    for (int q = 0; q < BLK; ++q) {
         bool inside;
         if (MODEL == M_LEGACY) {
-            inside = (L.y <= r.a) && (L.y >= 0.f) && (L.tp <= r.dl_tmp);  // ddm_models.pyx:451
+            inside = live && (L.y <= r.a) && (L.y >= 0.f) && (L.tp <= r.dl_tmp);
         } else {
             const float b = bound_at<BOUND, NOISE>(r, L.ixf, L.ix, p, L.k);
-            inside = (fabsf(L.y) <= b) && (L.tp <= r.dl_tmp);  // ddm_models.pyx:719
+            inside = live && (fabsf(L.y) <= b) && (L.tp <= r.dl_tmp);
         }
-        if (!inside) return false;
-        if (NOISE && L.ix >= p.nlen) {
+        if (NOISE && inside && L.ix >= p.nlen) {
             raise_error(p.hdr, SSM_ERR_NOISE_RANGE, (int)L.w);
-            return false;
+            inside = false;
         }
-        // (y + v*dt) + scale*g: the association the reference build uses
-        if (NOISE) {
-            L.y = __fadd_rn(__fadd_rn(L.y, r.drift), __fmul_rn(r.scale, g[q]));
-            L.tp = __fadd_rn(L.tp, p.dt);
-        } else {
-            L.y = fmaf(r.scale, g[q], L.y + r.drift);
-            L.tp += p.dt;
+        if (inside) {
+            if (NOISE) {
+                // (y + v*dt) + scale*g: the association the reference build uses
+                L.y = __fadd_rn(__fadd_rn(L.y, r.drift), __fmul_rn(r.scale, g[q]));
+                L.tp = __fadd_rn(L.tp, p.dt);
+            } else {
+                L.y += g[q];
+                L.tp += p.dt;
+            }
+            L.ixf += 1.0f;
+            if (INT_IX) L.ix += 1;
+            if (RECORD && L.ix < p.traj_len) p.traj[L.ix] = L.y;
         }
-        L.ixf += 1.0f;
-        L.ix += 1;
-        if (RECORD && L.ix < p.traj_len) p.traj[L.ix] = L.y;
+        live = inside;
     }
-    return true;
+    return live;
 }
 
 template <bool NOISE>
-__device__ __forceinline__ void finalize(const SingleParams &p, const Lane &L, const TrialRow &r) {
+__device__ __forceinline__ void finalize(const SingleParams &p, const Lane &L) {
+    // fields needed only here are re-read instead of being held across the walk
+    const TrialRow *row = p.rows + L.k;
+    const float t = __ldg(&row->t), deadline = __ldg(&row->deadline), dl = __ldg(&row->dl_tmp);
     float u;
     if (NOISE) u = __ldg(p.nunif + L.w);
     else u = uniform_co(philox10(make_uint4(0u, L.n, L.k, 1u), p.key).x);
@@ -257,14 +296,14 @@ __device__ __forceinline__ void finalize(const SingleParams &p, const Lane &L, c
     float sm = 0.f;
     if (p.smooth) {
         if (L.tp == 0.f) sm = __double2float_rn(((double)u * 0.5) * (double)p.dt);
-        else if (L.tp < r.dl_tmp) sm = __double2float_rn((0.5 - (double)u) * (double)p.dt);
+        else if (L.tp < dl) sm = __double2float_rn((0.5 - (double)u) * (double)p.dt);
     }
-    float rt = __fadd_rn(__fadd_rn(L.tp, r.t), sm);
-    if (rt >= r.deadline || r.deadline <= 0.f) rt = -999.f;  // enforce_deadline
-    const int choice = (L.y > 0.f) - (L.y < 0.f);             // sign(y)
+    float rt = __fadd_rn(__fadd_rn(L.tp, t), sm);
+    if (rt >= deadline || deadline <= 0.f) rt = -999.f;  // enforce_deadline
+    const int choice = (L.y > 0.f) - (L.y < 0.f);         // sign(y)
     p.rts[L.w] = rt;
     p.choices[L.w] = choice;
-    if (p.steps) p.steps[L.w] = L.ix;
+    if (p.steps) p.steps[L.w] = (int)L.ixf;
 }
 
 __device__ __forceinline__ void lane_init(const SingleParams &p, Lane &L, TrialRow &r, int64_t w,
@@ -294,7 +333,7 @@ __device__ __forceinline__ void lane_init(const SingleParams &p, Lane &L, TrialR
 
 // ------------------------------------------------------------------ main kernel
 template <int MODEL, int BOUND, bool NOISE>
-__global__ void __launch_bounds__(256) k_single(const __grid_constant__ SingleParams p) {
+__global__ void __launch_bounds__(256, SSM_MIN_CTAS) k_single(const __grid_constant__ SingleParams p) {
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const unsigned lt_mask = (1u << lane) - 1u;
@@ -336,12 +375,12 @@ __global__ void __launch_bounds__(256) k_single(const __grid_constant__ SinglePa
         }
         if (__ballot_sync(FULL, active) == 0u) break;
         if (active) {
-            float g[4];
-            draw4<MODEL, NOISE>(p, L, r, g);
+            float g[BLK];
+            draw_block<MODEL, NOISE>(p, L, r, g);
             const bool live = step_block<MODEL, BOUND, NOISE, false>(p, L, r, g);
             L.blk += 1;
             if (!live) {
-                finalize<NOISE>(p, L, r);
+                finalize<NOISE>(p, L);
                 active = false;
             }
         }
@@ -361,8 +400,8 @@ __global__ void k_record(const __grid_constant__ SingleParams p) {
     lane_init(p, L, r, 0, hint);
     if (p.traj_len > 0) p.traj[0] = L.y;
     for (;;) {
-        float g[4];
-        draw4<MODEL, NOISE>(p, L, r, g);
+        float g[BLK];
+        draw_block<MODEL, NOISE>(p, L, r, g);
         const bool live = step_block<MODEL, BOUND, NOISE, true>(p, L, r, g);
         L.blk += 1;
         if (!live) break;
@@ -457,7 +496,8 @@ static int run_single(const SingleCall &c) {
     SSM_REQUIRE(c.maxt_k || (isfinite(c.max_t) && (double)c.max_t / (double)c.dt <= 8388608.0),
                 "max_t must be finite with max_t / delta_t <= 2^23");
     SSM_REQUIRE(c.v && c.z && c.t && c.deadline && c.s && c.a, "v, a, z, t, deadline, s are required");
-    SSM_REQUIRE(c.rts && c.choices, "rts and choices outputs are required");
+    SSM_REQUIRE((c.rts && c.choices) || (!c.offsets && c.n_trials * c.n_samples == 0),
+                "rts and choices outputs are required");
     SSM_REQUIRE(c.model != M_LEVY || c.alpha, "alpha is required for the Levy model");
     if (c.model != M_LEGACY) {
         SSM_REQUIRE(c.bound >= SSM_BOUND_TABLE && c.bound <= SSM_BOUND_WEIBULL, "unknown boundary kind %d", c.bound);

@@ -96,6 +96,11 @@ def simulate_single(model: str, *, v, z, t, deadline, s, a=None, alpha=None,
             raise ValueError("noise_rows must hold one row per trajectory")
     L = _lib.lib()
     ws = D.workspace(L.ssm_ddm_workspace_bytes(K), tag=0, stream=stream)
+    if K == 0 or (offs is None and total == 0):
+        # nothing to simulate (zero-length inputs map to null pointers)
+        if traj is not None:
+            traj.fill_(-999.0)
+        return SimOutput(rts=rts, choices=chs, steps=steps, traj=traj, workspace=ws)
     lopt = launch if launch is not None else launch_for(model)
     sp = D.stream_ptr(stream)
     common_tail = (
