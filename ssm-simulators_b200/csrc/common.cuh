@@ -67,11 +67,11 @@ inline PhiloxKeys philox_keys(uint64_t seed) {
 __device__ __forceinline__ uint4 philox10(uint4 c, const PhiloxKeys &key) {
 #pragma unroll
     for (int r = 0; r < 10; ++r) {
-        const uint32_t lo0 = 0xD2511F53u * c.x;
-        const uint32_t hi0 = __umulhi(0xD2511F53u, c.x);
-        const uint32_t lo1 = 0xCD9E8D57u * c.z;
-        const uint32_t hi1 = __umulhi(0xCD9E8D57u, c.z);
-        c = make_uint4(hi1 ^ c.y ^ key.k0[r], lo1, hi0 ^ c.w ^ key.k1[r], lo0);
+        // one 32x32->64 multiply (IMAD.WIDE.U32) per product gives both halves
+        const uint64_t p0 = (uint64_t)0xD2511F53u * c.x;
+        const uint64_t p1 = (uint64_t)0xCD9E8D57u * c.z;
+        c = make_uint4((uint32_t)(p1 >> 32) ^ c.y ^ key.k0[r], (uint32_t)p1,
+                       (uint32_t)(p0 >> 32) ^ c.w ^ key.k1[r], (uint32_t)p0);
     }
     return c;
 }
