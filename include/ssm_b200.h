@@ -127,6 +127,35 @@ int ssm_levy_flexbound(const float *v, const float *a, const float *z, const flo
                        const ssm_launch *launch, void *workspace, size_t workspace_bytes,
                        void *stream);
 
+/*
+ * ssm_ddm_flexbound_static -- no counterpart in the reference.  The same
+ * simulation as ssm_ddm_flexbound for callers that cannot allocate device
+ * memory (for example code running inside an allocator-free host plugin, or a
+ * caller whose memory pool is owned by someone else): it takes no workspace.
+ * Its scratch (work counter, error word and one 64-byte row per trial) lives in
+ * a file-scope __device__ array of SSM_STATIC_WS_BYTES bytes that every GPU
+ * loading this library holds until the process exits; n_trials above
+ * SSM_STATIC_MAX_TRIALS is rejected with SSM_ERR_ARG.  The first call on a
+ * device looks up the array's device address (cudaGetSymbolAddress) with that
+ * device current, so make that first call before any stream capture.  Every
+ * call shares the one array: calls that overlap on the GPU (other streams,
+ * other host threads) race and must be serialised by the caller.  Device-side
+ * error flags of this variant are not reported; use the workspace form when
+ * they are needed.  The caller still owns every input and output buffer.
+ */
+#define SSM_STATIC_MAX_TRIALS 16384
+#define SSM_STATIC_WS_BYTES (256 + 64 * SSM_STATIC_MAX_TRIALS)
+int ssm_ddm_flexbound_static(const float *v, const float *a, const float *z, const float *t,
+                             const float *deadline, const float *s, int64_t n_trials,
+                             int64_t n_samples, const int64_t *sample_offsets, float max_t,
+                             const float *max_t_per_trial, float delta_t, int bound_kind,
+                             const float *bound_p1, const float *bound_p2,
+                             const float *bound_table, int64_t table_stride, int64_t table_len,
+                             uint64_t seed, int smooth_unif, const float *noise_rows,
+                             int64_t noise_row_len, const float *noise_unif, float *rts,
+                             int32_t *choices, int32_t *steps, float *traj, int64_t traj_len,
+                             const ssm_launch *launch, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

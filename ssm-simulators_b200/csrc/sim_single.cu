@@ -20,6 +20,8 @@
 //  * Noise injection replaces the generator by caller rows and switches every
 //    float operation to explicit round-to-nearest intrinsics, giving results
 //    bit-identical to the sequential CPU restatement.
+#include <mutex>
+
 #include "common.cuh"
 
 
@@ -613,3 +615,55 @@ int ssm_levy_flexbound(const float *v, const float *a, const float *z, const flo
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant.  Its scratch is this file-scope device array; host
+// code must not hand the symbol itself to a kernel (in host code it names a
+// host-side stand-in), so the device address is looked up once per device.
+namespace ssm {
+static __device__ __align__(256) unsigned char g_static_ws[SSM_STATIC_WS_BYTES];
+static std::mutex g_static_mu;
+static void *g_static_ptr[64] = {};
+
+static int static_workspace(void **out) {
+    int dev = 0;
+    SSM_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) {
+        set_error("device ordinal %d out of range for the static workspace", dev);
+        return SSM_ERR_ARG;
+    }
+    std::lock_guard<std::mutex> lock(g_static_mu);
+    if (g_static_ptr[dev] == nullptr) {
+        void *p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_static_ws);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_static_ws)");
+        g_static_ptr[dev] = p;
+    }
+    *out = g_static_ptr[dev];
+    return SSM_OK;
+}
+}  // namespace ssm
+
+extern "C" int ssm_ddm_flexbound_static(
+    const float *v, const float *a, const float *z, const float *t, const float *deadline,
+    const float *s, int64_t n_trials, int64_t n_samples, const int64_t *sample_offsets,
+    float max_t, const float *max_t_per_trial, float delta_t, int bound_kind,
+    const float *bound_p1, const float *bound_p2, const float *bound_table, int64_t table_stride,
+    int64_t table_len, uint64_t seed, int smooth_unif, const float *noise_rows,
+    int64_t noise_row_len, const float *noise_unif, float *rts, int32_t *choices, int32_t *steps,
+    float *traj, int64_t traj_len, const ssm_launch *launch, void *stream) {
+    if (n_trials > SSM_STATIC_MAX_TRIALS) {
+        ssm::set_error("ssm_ddm_flexbound_static supports at most %d trials (got %lld); "
+                       "use ssm_ddm_flexbound with a caller workspace",
+                       SSM_STATIC_MAX_TRIALS, (long long)n_trials);
+        return SSM_ERR_ARG;
+    }
+    void *ws = nullptr;
+    const int st = ssm::static_workspace(&ws);
+    if (st != SSM_OK) return st;
+    return ssm_ddm_flexbound(v, a, z, t, deadline, s, n_trials, n_samples, sample_offsets, max_t,
+                             max_t_per_trial, delta_t, bound_kind, bound_p1, bound_p2,
+                             bound_table, table_stride, table_len, seed, smooth_unif, noise_rows,
+                             noise_row_len, noise_unif, rts, choices, steps, traj, traj_len,
+                             launch, ws, SSM_STATIC_WS_BYTES, stream);
+}
