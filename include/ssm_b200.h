@@ -127,6 +127,58 @@ int ssm_levy_flexbound(const float *v, const float *a, const float *z, const flo
                        const ssm_launch *launch, void *workspace, size_t workspace_bytes,
                        void *stream);
 
+/* ---- multi-accumulator race / LCA --------------------------------------- */
+
+/* Bytes of scratch ssm_race_model / ssm_lca need. */
+size_t ssm_race_workspace_bytes(int64_t n_trials, int n_particles);
+
+/*
+ * ssm_race_model -- replaces cssm.race_model (src/cssm/race_models.pyx:141-506,
+ * sequential loop :417-464).  n_particles accumulators start at z_j b(0); while
+ * no accumulator exceeds b(t) and t <= min(max_t, deadline - t_nd), each
+ * does x_j = max(0, x_j + v_j dt + sqrt(dt) s_j g_j).  choice = argmax_j x_j.
+ * v, z, s: float32[n_trials * n_particles] (row-major); t, deadline: [n_trials].
+ * Boundary: a (+ bound_p1 / bound_p2) or a table, as for ssm_ddm_flexbound.
+ * Injected rows hold n_particles increments per step (index step*np + j).
+ */
+int ssm_race_model(const float *v, const float *z, const float *t, const float *s,
+                   const float *deadline, int64_t n_trials, int64_t n_samples, int n_particles,
+                   const int64_t *sample_offsets, float max_t, float delta_t, int bound_kind,
+                   const float *a, const float *bound_p1, const float *bound_p2,
+                   const float *bound_table, int64_t table_stride, int64_t table_len,
+                   uint64_t seed, int smooth_unif, const float *noise_rows, int64_t noise_row_len,
+                   const float *noise_unif, float *rts, int32_t *choices, int32_t *steps,
+                   float *traj, int64_t traj_len, const ssm_launch *launch, void *workspace,
+                   size_t workspace_bytes, void *stream);
+
+/*
+ * ssm_lca -- replaces cssm.lca (src/cssm/race_models.pyx:509-920, sequential
+ * loop :825-879): as the race with leak g and lateral inhibition b,
+ * x_j += ((v_j - g x_j) - b (sum - x_j)) dt + sqrt(dt) s_j g_j, clipped at 0; the
+ * time accumulator is double precision as in the reference.  g, b: [n_trials].
+ */
+int ssm_lca(const float *v, const float *z, const float *g, const float *b, const float *t,
+            const float *s, const float *deadline, int64_t n_trials, int64_t n_samples,
+            int n_particles, const int64_t *sample_offsets, float max_t, float delta_t,
+            int bound_kind, const float *a, const float *bound_p1, const float *bound_p2,
+            const float *bound_table, int64_t table_stride, int64_t table_len, uint64_t seed,
+            int smooth_unif, const float *noise_rows, int64_t noise_row_len,
+            const float *noise_unif, float *rts, int32_t *choices, int32_t *steps, float *traj,
+            int64_t traj_len, const ssm_launch *launch, void *workspace, size_t workspace_bytes,
+            void *stream);
+
+/*
+ * ssm_lba_vanilla -- replaces cssm.lba_vanilla (src/cssm/lba_models.pyx:36-139):
+ * per sample x_j = (a - U(0, z)) / |N(v_j, sd_j)|, choice = argmin_j x_j,
+ * rt = min_j x_j + t, rt = -999 when rt >= deadline.  v, sd: float32[n_trials *
+ * nact]; a, z, t, deadline: [n_trials].  noise_u / noise_g (both or neither):
+ * injected U(0,1) and N(0,1) draws, float32[total * nact].  No workspace.
+ */
+int ssm_lba_vanilla(const float *v, const float *a, const float *z, const float *deadline,
+                    const float *sd, const float *t, int64_t n_trials, int64_t n_samples, int nact,
+                    const int64_t *sample_offsets, uint64_t seed, const float *noise_u,
+                    const float *noise_g, float *rts, int32_t *choices, void *stream);
+
 /*
  * ssm_ddm_flexbound_static -- no counterpart in the reference.  The same
  * simulation as ssm_ddm_flexbound for callers that cannot allocate device

@@ -148,5 +148,104 @@ def ddm(v, a, z, t, deadline, s, max_t=20, delta_t=0.001, n_samples=20000, n_tri
     return {"rts": rts, "choices": choices, "metadata": meta}
 
 
-__all__ = ["ddm", "ddm_flexbound", "levy_flexbound"]
+def _param_dict(arr, prefix, n):
+    # build_param_dict_from_2d_array (src/cssm/_utils.pyx:720-732)
+    return {f"{prefix}{i}": arr[:, i] for i in range(n)}
+
+
+def _run_race(model, v, z, t, s, deadline, g, b, delta_t, max_t, n_samples, n_trials,
+              boundary_fun, boundary_params, random_state, return_option, smooth_unif, **kwargs):
+    _check_return_option(return_option)
+    n_trials, n_samples = int(n_trials), int(n_samples)
+    if boundary_fun is None:
+        raise TypeError("boundary_fun is required")
+    v, z, s = (np.ascontiguousarray(_f32(x, nm)) for x, nm in ((v, "v"), (z, "z"), (s, "s")))
+    t = _f32(t, "t")
+    deadline = _f32(deadline, "deadline")
+    n_part = v.shape[1]
+    t_s = bf.make_t_s(max_t, delta_t)
+    spec = bf.kernel_spec(boundary_fun, boundary_params, n_trials, t_s,
+                          force_table=bool(kwargs.get("_force_table", False)))
+    full = return_option == "full"
+    n_rows = int(np.float32(np.float32(max_t) / np.float32(delta_t))) + 1
+    out = dev.simulate_race(
+        model, v=v, z=z, t=t.reshape(n_trials, -1)[:, 0] if n_trials else t.reshape(-1),
+        s=s, deadline=deadline, n_trials=n_trials, n_samples=n_samples,
+        g=None if g is None else _f32(g, "g").reshape(-1), b=None if b is None else _f32(b, "b").reshape(-1),
+        max_t=max_t, delta_t=delta_t, bound_kind=spec["kind"], a=spec["a"], bound_p1=spec["p1"],
+        bound_p2=spec["p2"], bound_table=spec["table"], seed=_seed(random_state),
+        smooth_unif=smooth_unif, traj_len=n_rows * n_part if (full and n_trials and n_samples) else 0)
+    rts = out.rts.cpu().numpy().reshape(n_samples, n_trials, 1)
+    choices = out.choices.cpu().numpy().reshape(n_samples, n_trials, 1)
+    # the reference reports [-1, 1] in minimal metadata and 0..n-1 in full metadata
+    minimal = _minimal_meta(model, [-1, 1], n_samples, n_trials, boundary_fun.__name__)
+    if not full:
+        return {"rts": rts, "choices": choices, "metadata": minimal}
+    meta = dict(minimal)
+    meta["possible_choices"] = list(np.arange(0, n_part, 1))
+    params = {"v": v, "z": z, "t": t, "deadline": deadline, "s": s}
+    if model == "lca":
+        params = {"v": v, "z": z, "g": g, "b": b, "t": t, "deadline": deadline, "s": s}
+    meta.update(params)
+    meta.update({"delta_t": float(np.float32(delta_t)), "max_t": float(np.float32(max_t)),
+                 "n_threads": 1})
+    meta["boundary_fun_type"] = boundary_fun.__name__
+    boundary = np.zeros(t_s.shape, dtype=DTYPE)
+    if n_trials > 0:
+        bp0 = {key: np.asarray(val)[0] for key, val in boundary_params.items()}
+        boundary[:] = np.asarray(boundary_fun(t=t_s, **bp0)).astype(DTYPE)
+    meta["boundary"] = boundary
+    traj = np.full((n_rows, n_part), -999, dtype=DTYPE)
+    if out.traj is not None:
+        traj.reshape(-1)[:] = out.traj.cpu().numpy()[: n_rows * n_part]
+    meta["trajectory"] = traj
+    if boundary_params:
+        meta.update(boundary_params)
+    meta.update({**_param_dict(v, "v", n_part), **_param_dict(z, "z", n_part)})
+    return {"rts": rts, "choices": choices, "metadata": meta}
+
+
+def race_model(v, z, t, s, deadline, delta_t=0.001, max_t=20, n_samples=2000, n_trials=1,
+               boundary_fun=None, boundary_params={}, random_state=None,  # noqa: B006
+               return_option="full", smooth_unif=False, n_threads=1, **kwargs):
+    """Race of n accumulators clipped at 0 (src/cssm/race_models.pyx:141-506)."""
+    return _run_race("race_model", v, z, t, s, deadline, None, None, delta_t, max_t, n_samples,
+                     n_trials, boundary_fun, boundary_params, random_state, return_option,
+                     smooth_unif, **kwargs)
+
+
+def lca(v, z, g, b, t, s, deadline, delta_t=0.001, max_t=20, n_samples=2000, n_trials=1,
+        boundary_fun=None, boundary_params={}, random_state=None,  # noqa: B006
+        return_option="full", smooth_unif=False, n_threads=1, **kwargs):
+    """Leaky competing accumulators (src/cssm/race_models.pyx:509-920)."""
+    return _run_race("lca", v, z, t, s, deadline, g, b, delta_t, max_t, n_samples, n_trials,
+                     boundary_fun, boundary_params, random_state, return_option, smooth_unif,
+                     **kwargs)
+
+
+def lba_vanilla(v, a, z, deadline, sd, t, nact=3, n_samples=2000, n_trials=1, max_t=20,
+                **kwargs):
+    """Linear ballistic accumulator, closed form (src/cssm/lba_models.pyx:36-139).
+
+    The reference draws from numpy's unseeded global generator; here the device
+    generator is seeded by ``random_state`` when given (else a fresh seed)."""
+    n_trials, n_samples, nact = int(n_trials), int(n_samples), int(nact)
+    v, sd = (np.ascontiguousarray(_f32(x, nm)).reshape(n_trials, -1) for x, nm in ((v, "v"), (sd, "sd")))
+    a, z = (_f32(x, nm).reshape(n_trials, -1) for x, nm in ((a, "a"), (z, "z")))
+    t, deadline = _f32(t, "t").reshape(-1), _f32(deadline, "deadline").reshape(-1)
+    if v.shape[1] != nact:
+        raise ValueError(f"v has {v.shape[1]} columns but nact = {nact}")
+    out = dev.simulate_lba(v=v, a=a[:, 0], z=z[:, 0], deadline=deadline, sd=sd, t=t,
+                           n_trials=n_trials, n_samples=n_samples,
+                           seed=_seed(kwargs.get("random_state")))
+    rts = out.rts.cpu().numpy().reshape(n_samples, n_trials, 1)
+    choices = out.choices.cpu().numpy().reshape(n_samples, n_trials, 1)
+    meta = _minimal_meta("lba_vanilla", list(np.arange(0, nact, 1)), n_samples, n_trials)
+    meta.update({"a": a, "z": z, "deadline": deadline, "sd": sd, "t": t})
+    meta.update({"max_t": max_t, "n_threads": 1})
+    meta.update(_param_dict(v, "v_", nact))
+    return {"rts": rts, "choices": choices, "metadata": meta}
+
+
+__all__ = ["ddm", "ddm_flexbound", "levy_flexbound", "race_model", "lca", "lba_vanilla"]
 _ = _lib  # the C ABI is loaded lazily on the first call

@@ -134,3 +134,118 @@ def simulate_single(model: str, *, v, z, t, deadline, s, a=None, alpha=None,
     return SimOutput(rts=rts, choices=chs, steps=steps, traj=traj, workspace=ws)
 
 
+
+
+def _offsets(sample_offsets, K, dev):
+    if sample_offsets is None:
+        return None
+    offs = sample_offsets
+    if not isinstance(offs, torch.Tensor):
+        offs = torch.as_tensor(np.asarray(offs, dtype=np.int64))
+    offs = offs.to(device=dev, dtype=torch.int64).contiguous()
+    if offs.numel() != K + 1:
+        raise ValueError("sample_offsets must have n_trials + 1 entries")
+    return offs
+
+
+def simulate_race(model: str, *, v, z, t, s, deadline, n_trials: int, n_samples: int = 0,
+                  g=None, b=None, sample_offsets=None, max_t: float = 20.0, delta_t: float = 0.001,
+                  bound_kind: int = _lib.BOUND_CONSTANT, a=None, bound_p1=None, bound_p2=None,
+                  bound_table=None, seed: int = 0, smooth_unif: bool = False, noise_rows=None,
+                  noise_unif=None, want_steps: bool = False, traj_len: int = 0, total=None,
+                  launch=None, stream: torch.cuda.Stream | None = None) -> SimOutput:
+    """race_model / lca on the GPU.  v, z, s: [n_trials, n_particles]; t: [n_trials]
+    (or [n_trials, 1]); g, b: [n_trials] for lca."""
+    dev = D.require_cuda()
+    K = int(n_trials)
+    v_np = v if isinstance(v, torch.Tensor) else np.asarray(v, np.float32)
+    n_part = int(v_np.shape[1]) if K > 0 else int(np.shape(v_np)[-1]) if np.ndim(v_np) == 2 else 1
+    vt = D.to_dev_f32(v, K * n_part, "v")
+    zt = D.to_dev_f32(z, K * n_part, "z")
+    st = D.to_dev_f32(s, K * n_part, "s")
+    tt = D.to_dev_f32(t, K, "t")
+    dlt = D.to_dev_f32(deadline, K, "deadline")
+    gt = _opt_f32(g, K, "g")
+    bt = _opt_f32(b, K, "b")
+    at = _opt_f32(a, K, "a")
+    p1t = _opt_f32(bound_p1, K, "bound_p1")
+    p2t = _opt_f32(bound_p2, K, "bound_p2")
+    tab, tstride, tlen = None, 0, 0
+    if bound_table is not None:
+        tab = D.to_dev_f32(bound_table)
+        tlen = int(bound_table.shape[-1])
+        tstride = tlen
+        if tab.numel() < K * tstride:
+            raise ValueError("bound_table must be float32 [n_trials, table_len]")
+    offs = _offsets(sample_offsets, K, dev)
+    if total is None:
+        total = int(offs[-1].item()) if offs is not None else K * int(n_samples)
+    rts = torch.empty(total, dtype=torch.float32, device=dev)
+    chs = torch.empty(total, dtype=torch.int32, device=dev)
+    steps = torch.empty(total, dtype=torch.int32, device=dev) if want_steps else None
+    traj = torch.empty(int(traj_len), dtype=torch.float32, device=dev) if traj_len > 0 else None
+    nrows = nunif = None
+    nlen = 0
+    if noise_rows is not None:
+        nrows = D.to_dev_f32(noise_rows)
+        nlen = int(noise_rows.shape[-1])
+        nunif = D.to_dev_f32(noise_unif, total, "noise_unif")
+        if nrows.numel() < total * nlen:
+            raise ValueError("noise_rows must hold one row per trajectory")
+    L = _lib.lib()
+    ws = D.workspace(L.ssm_race_workspace_bytes(K, n_part), tag=0, stream=stream)
+    if K == 0 or (offs is None and total == 0):
+        if traj is not None:
+            traj.fill_(-999.0)
+        return SimOutput(rts=rts, choices=chs, steps=steps, traj=traj, workspace=ws)
+    lopt = launch if launch is not None else launch_for(model)
+    sp = D.stream_ptr(stream)
+    tail = (int(bound_kind), D.ptr(at), D.ptr(p1t), D.ptr(p2t), D.ptr(tab), tstride, tlen,
+            _lib.U64_cast(seed), int(bool(smooth_unif)), D.ptr(nrows), nlen, D.ptr(nunif),
+            D.ptr(rts), D.ptr(chs), D.ptr(steps), D.ptr(traj), int(traj_len),
+            ctypes.addressof(lopt), D.ptr(ws), ws.numel(), sp)
+    head_dims = (K, int(n_samples), n_part, D.ptr(offs), float(np.float32(max_t)),
+                 float(np.float32(delta_t)))
+    if model == "race_model":
+        status = L.ssm_race_model(D.ptr(vt), D.ptr(zt), D.ptr(tt), D.ptr(st), D.ptr(dlt),
+                                  *head_dims, *tail)
+    elif model == "lca":
+        if gt is None or bt is None:
+            raise ValueError("lca needs g and b")
+        status = L.ssm_lca(D.ptr(vt), D.ptr(zt), D.ptr(gt), D.ptr(bt), D.ptr(tt), D.ptr(st),
+                           D.ptr(dlt), *head_dims, *tail)
+    else:
+        raise ValueError(f"unknown race model {model!r}")
+    _lib.check(status)
+    if noise_rows is not None:
+        _lib.check(L.ssm_check_status(D.ptr(ws), sp))
+    return SimOutput(rts=rts, choices=chs, steps=steps, traj=traj, workspace=ws)
+
+
+def simulate_lba(*, v, a, z, deadline, sd, t, n_trials: int, n_samples: int = 0,
+                 sample_offsets=None, seed: int = 0, noise_u=None, noise_g=None, total=None,
+                 stream: torch.cuda.Stream | None = None) -> SimOutput:
+    """lba_vanilla on the GPU.  v, sd: [n_trials, nact]; a, z (start-point range A),
+    t, deadline: [n_trials]."""
+    dev = D.require_cuda()
+    K = int(n_trials)
+    nact = int(np.shape(v)[-1]) if not isinstance(v, torch.Tensor) else int(v.shape[-1])
+    vt = D.to_dev_f32(v, K * nact, "v")
+    sdt = D.to_dev_f32(sd, K * nact, "sd")
+    at, zt, tt, dlt = (D.to_dev_f32(x, K, nm) for x, nm in ((a, "a"), (z, "z"), (t, "t"), (deadline, "deadline")))
+    offs = _offsets(sample_offsets, K, dev)
+    if total is None:
+        total = int(offs[-1].item()) if offs is not None else K * int(n_samples)
+    rts = torch.empty(total, dtype=torch.float32, device=dev)
+    chs = torch.empty(total, dtype=torch.int32, device=dev)
+    nu = ng = None
+    if noise_u is not None:
+        nu = D.to_dev_f32(noise_u, total * nact, "noise_u")
+        ng = D.to_dev_f32(noise_g, total * nact, "noise_g")
+    if K == 0 or total == 0:
+        return SimOutput(rts=rts, choices=chs, steps=None, traj=None, workspace=rts)
+    L = _lib.lib()
+    _lib.check(L.ssm_lba_vanilla(D.ptr(vt), D.ptr(at), D.ptr(zt), D.ptr(dlt), D.ptr(sdt), D.ptr(tt),
+                                 K, int(n_samples), nact, D.ptr(offs), _lib.U64_cast(seed),
+                                 D.ptr(nu), D.ptr(ng), D.ptr(rts), D.ptr(chs), D.stream_ptr(stream)))
+    return SimOutput(rts=rts, choices=chs, steps=None, traj=None, workspace=rts)
