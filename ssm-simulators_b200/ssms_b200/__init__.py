@@ -10,6 +10,7 @@ called through a C ABI (include/ssm_b200.h) with ctypes.
 """
 
 from . import boundary_functions, cssm  # noqa: F401
+from .config import ModelConfigBuilder, model_config  # noqa: F401
+from .simulator import OMISSION_SENTINEL, Simulator, simulator  # noqa: F401
 
 __version__ = "0.1.0"
-OMISSION_SENTINEL: float = -999.0

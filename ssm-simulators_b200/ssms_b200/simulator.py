@@ -1,0 +1,328 @@
+"""``Simulator(model).simulate(theta, n_samples)`` and ``simulator(theta, model)``.
+
+Mirrors the reference's public simulation API
+(ssms/basic_simulators/simulator_class.py:35-721 and simulator.py:624-864):
+theta normalisation (dict / list / array / DataFrame), the deadline default of
+999, the noise vector, the per-model parameter transforms, the boundary dict,
+parameter validation, the simulator call, the n_trials == 1 squeeze and
+``metadata["model"]``.  ``simulator()`` adds choice / omission / go-nogo
+probabilities and the 128- and 256-bin rt histograms.  The simulators called
+are the GPU implementations in ``ssms_b200.cssm``.
+"""
+
+from __future__ import annotations
+
+import inspect
+import numbers
+import warnings
+from copy import deepcopy
+from threading import Lock
+
+import numpy as np
+
+from .config import ModelConfigBuilder, get_boundary_registry
+from .transforms import apply_all
+
+OMISSION_SENTINEL: float = -999.0
+
+_seed_rng = np.random.default_rng()
+_seed_lock = Lock()
+_SEED_MIN, _SEED_MAX = -(2**31), 2**31 - 1
+
+
+def _get_unique_seed() -> int:
+    with _seed_lock:
+        return int(_seed_rng.integers(0, 2**31))
+
+
+def _validate_random_state_for_c_rng(random_state) -> None:
+    if random_state is None or not isinstance(random_state, numbers.Integral):
+        return
+    rs = int(random_state)
+    if rs < _SEED_MIN or rs > _SEED_MAX:
+        raise ValueError(f"random_state={rs} is outside [{_SEED_MIN}, {_SEED_MAX}], the range the "
+                         "C-level simulator can use on all platforms. Use a smaller integer seed.")
+
+
+def _make_valid_dict(dict_in: dict) -> dict:
+    lengths = []
+    for key, value in dict_in.items():
+        if isinstance(value, list):
+            dict_in[key] = np.array(value).astype(np.float32)
+        elif isinstance(value, int | float):
+            dict_in[key] = np.array([value]).astype(np.float32)
+        dict_in[key] = np.squeeze(dict_in[key]).astype(np.float32)
+        if dict_in[key].ndim > 1:
+            raise ValueError(f"Dimension of {key} is greater than 1")
+        if dict_in[key].ndim > 0:
+            lengths.append(dict_in[key].shape[0])
+    if len(set(lengths)) > 1:
+        raise ValueError("thetas have to be either scalars or same length for all thetas which are not scalars")
+    for key, value in dict_in.items():
+        if value.ndim == 0:
+            dict_in[key] = np.tile(value, lengths[0]) if lengths else np.expand_dims(value, axis=0)
+    return dict_in
+
+
+def _theta_dict_to_array(theta: dict, model_param_list: list[str]) -> np.ndarray:
+    return np.stack([theta[p] for p in model_param_list], axis=1).astype(np.float32)
+
+
+def _theta_array_to_dict(theta: np.ndarray, model_param_list: list[str]) -> dict:
+    if theta.ndim == 1 and len(model_param_list) != theta.shape[0]:
+        raise ValueError("model_param_list and theta array do not imply the same number of parameters")
+    if theta.ndim == 2 and len(model_param_list) != theta.shape[1]:
+        raise ValueError("model_param_list and theta array do not imply the same number of parameters")
+    if theta.ndim == 1:
+        theta = np.expand_dims(theta, axis=0).astype(np.float32)
+    return {p: theta[:, i] for i, p in enumerate(model_param_list)}
+
+
+def _preprocess_theta_generic(theta):
+    import pandas as pd
+
+    if isinstance(theta, list):
+        return np.asarray(theta).astype(np.float32)
+    if isinstance(theta, np.ndarray):
+        return theta.astype(np.float32)
+    if isinstance(theta, dict):
+        return _make_valid_dict(deepcopy(theta))
+    if isinstance(theta, pd.DataFrame):
+        d = theta.to_dict(orient="list")
+        return {k: np.array(v).astype(np.float32) for k, v in d.items()}
+    raise ValueError("theta is not supplied as list, numpy array, dictionary, or pandas DataFrame!")
+
+
+def _preprocess_theta_deadline(theta, deadline: bool, config: dict):
+    if not isinstance(theta, dict):
+        theta = _theta_array_to_dict(theta, config["params"])
+    n_trials = theta[config["params"][0]].shape[0]
+    if not deadline:
+        theta["deadline"] = np.tile(np.array([999], dtype=np.float32), n_trials)
+    return n_trials, theta
+
+
+def make_noise_vec(sigma_noise, n_trials: int, n_particles: int) -> np.ndarray:
+    shape = n_trials if (n_particles == 1 or n_particles is None) else (n_trials, 1)
+    base = [sigma_noise[0]] * n_particles if isinstance(sigma_noise, np.ndarray) else [sigma_noise] * n_particles
+    return np.tile(np.array(base, dtype=np.float32), shape)
+
+
+def make_boundary_dict(config: dict, theta: dict) -> dict:
+    if callable(config.get("boundary")) and config.get("boundary_params"):
+        names = config["boundary_params"]
+        fun = config["boundary"]
+    else:
+        info = get_boundary_registry().get(config["boundary_name"])
+        names, fun = info["params"], info["fun"]
+    return {"boundary_params": {p: v for p, v in theta.items() if p in names}, "boundary_fun": fun}
+
+
+def validate_ssm_parameters(model: str, theta: dict) -> None:
+    """The reference's parameter checks (simulator.py:500-581) for the models here."""
+    if model == "lba_3_vs_constraint":
+        v_sum = np.sum(np.array(theta["v"]), axis=1)
+        if np.any(v_sum <= 0.99) or np.any(v_sum >= 1.01):
+            raise ValueError("Drift rates do not sum to 1 for each trial")
+    if model in ("lba_3_vs_constraint", "lba3", "lba2"):
+        if np.any(theta["z"] >= theta["a"]):
+            raise ValueError("Starting point z >= a for at least one trial")
+
+
+def bin_simulator_output(out: dict, bin_dt: float = 0.04, nbins: int = 0, max_t: float = -1,
+                         freq_cnt: bool = False) -> np.ndarray:
+    """Histogram of rts per choice (simulator.py:435-497): last bin open to +inf."""
+    if out is None:
+        raise ValueError("out is not supplied")
+    if max_t == -1:
+        max_t = out["metadata"]["max_t"]
+    if nbins == 0:
+        nbins = int(max_t / bin_dt)
+    bins = np.zeros(nbins + 1)
+    bins[:nbins] = np.linspace(0, max_t, nbins)
+    bins[nbins] = np.inf
+    choices = out["metadata"]["possible_choices"]
+    counts = np.zeros((nbins, len(choices)))
+    for i, c in enumerate(choices):
+        counts[:, i] = np.histogram(out["rts"][out["choices"] == c], bins=bins)[0]
+    if freq_cnt is False:
+        counts = counts / out["metadata"]["n_samples"]
+    return counts
+
+
+def _noise(theta, model_name, no_noise, sigma_noise):
+    if "sd" in theta or "s" in theta:
+        if sigma_noise is not None:
+            raise ValueError("sigma_noise parameter should be None if 'sd' or 's' is passed via theta dictionary")
+        if no_noise:
+            return 0.0
+        return theta["sd"] if "sd" in theta else theta["s"]
+    if no_noise:
+        return 0.0
+    if "lba" in model_name and sigma_noise is None:
+        return 0.1
+    return 1.0 if sigma_noise is None else sigma_noise
+
+
+class Simulator:
+    """Class-based simulation interface (simulator_class.py:35-721)."""
+
+    def __init__(self, model=None, boundary=None, drift=None, simulator_function=None,
+                 parameter_adapter=None, parameter_adaptations=None, **config_overrides):
+        if drift is not None:
+            raise ValueError("drift functions belong to the ddm_flex simulator family, which this "
+                             "package does not implement")
+        self._parameter_adapter = parameter_adapter
+        self._custom_adaptations = list(parameter_adaptations or [])
+        if isinstance(model, dict):
+            config = deepcopy(model)
+        elif isinstance(model, str):
+            config = ModelConfigBuilder.from_model(model)
+        elif model is None and simulator_function is not None:
+            config = self._minimal_config(simulator_function, config_overrides)
+        else:
+            raise ValueError("Must provide either a model name, config dict, or simulator_function")
+        config.update(config_overrides)
+        if simulator_function is not None:
+            self._validate_simulator_function(simulator_function, config)
+            config["simulator"] = simulator_function
+        if boundary is not None:
+            self._apply_boundary(config, boundary)
+        for field in ("params", "nchoices", "simulator"):
+            if field not in config:
+                raise ValueError(f"Configuration missing required field: '{field}'")
+        self._config = config
+
+    @staticmethod
+    def _minimal_config(fn, overrides):
+        if "params" not in overrides:
+            raise ValueError("When using a custom simulator_function without a base model, you must provide 'params'")
+        if "nchoices" not in overrides:
+            raise ValueError("When using a custom simulator_function without a base model, you must provide 'nchoices'")
+        cfg = {"name": overrides.get("name", "custom"), "params": overrides["params"],
+               "n_params": len(overrides["params"]), "nchoices": overrides["nchoices"],
+               "choices": overrides.get("choices", list(range(overrides["nchoices"]))),
+               "n_particles": overrides.get("n_particles", 1), "simulator": fn}
+        for k in ("param_bounds", "default_params"):
+            if k in overrides:
+                cfg[k] = overrides[k]
+        return cfg
+
+    @staticmethod
+    def _validate_simulator_function(fn, config):
+        params = inspect.signature(fn).parameters
+        for p in ("max_t", "n_samples", "delta_t", "random_state"):
+            if p not in params:
+                warnings.warn(f"Simulator function '{fn.__name__}' is missing recommended parameter "
+                              f"'{p}'. This may cause issues during simulation.", UserWarning)
+        for p in config.get("params", []):
+            if p not in params:
+                raise ValueError(f"Simulator function '{fn.__name__}' is missing required model parameter '{p}'")
+
+    @staticmethod
+    def _apply_boundary(config, boundary):
+        if isinstance(boundary, str):
+            reg = get_boundary_registry()
+            if not reg.is_registered(boundary):
+                raise ValueError(f"Unknown boundary '{boundary}'. Available boundaries: {reg.list_boundaries()}")
+            info = reg.get(boundary)
+            config["boundary_name"], config["boundary"] = boundary, info["fun"]
+            config.setdefault("boundary_params", info["params"])
+        elif callable(boundary):
+            names = list(inspect.signature(boundary).parameters)
+            if not names or names[0] != "t":
+                raise ValueError(f"Boundary function '{boundary.__name__}' must accept 't' as first positional argument")
+            config["boundary"] = boundary
+            config["boundary_name"] = getattr(boundary, "__name__", "custom")
+            if "boundary_params" not in config:
+                warnings.warn("Custom boundary function provided without 'boundary_params'.", UserWarning)
+                config["boundary_params"] = []
+        else:
+            raise ValueError("boundary must be a string name or callable function")
+
+    def simulate(self, theta, n_samples: int = 1000, delta_t: float = 0.001, max_t: float = 20,
+                 no_noise: bool = False, sigma_noise=None, smooth_unif: bool = True,
+                 random_state=None, return_option: str = "full", n_threads: int = 1,
+                 extra_fields: dict | None = None) -> dict:
+        cfg = deepcopy(self._config)
+        model_name = cfg.get("name", "").replace("_deadline", "")
+        is_deadline = "deadline" in cfg.get("params", [])
+        if random_state is None:
+            random_state = _get_unique_seed()
+        _validate_random_state_for_c_rng(random_state)
+        theta = _preprocess_theta_generic(theta)
+        n_trials, theta = _preprocess_theta_deadline(theta, is_deadline, cfg)
+        sim_params = {"max_t": max_t, "n_samples": n_samples, "n_trials": n_trials,
+                      "delta_t": delta_t, "random_state": random_state,
+                      "return_option": return_option, "smooth_unif": smooth_unif,
+                      "n_threads": n_threads}
+        noise = make_noise_vec(_noise(theta, model_name, no_noise, sigma_noise), n_trials,
+                               cfg["n_particles"])
+        theta["sd" if "lba" in model_name else "s"] = noise
+        if self._parameter_adapter is not None:
+            theta = self._parameter_adapter.adapt_parameters(theta, cfg, n_trials)
+        else:
+            theta = apply_all(cfg.get("parameter_transforms", {}).get("simulation", []), theta, cfg, n_trials)
+        for tr in self._custom_adaptations:
+            theta = tr.apply(theta, cfg, n_trials)
+        boundary_dict = make_boundary_dict(cfg, theta) if ("boundary_name" in cfg or "boundary" in cfg) else {}
+        validate_ssm_parameters(model_name, theta)
+        x = cfg["simulator"](**theta, **boundary_dict, **sim_params, **(extra_fields or {}))
+        if not isinstance(x, dict):
+            raise TypeError(f"Simulator returned {type(x).__name__}, expected dict")
+        if n_trials == 1:
+            x["rts"] = np.squeeze(x["rts"], axis=1)
+            x["choices"] = np.squeeze(x["choices"], axis=1)
+        if n_trials > 1 and n_samples == 1:
+            x["rts"] = np.squeeze(x["rts"], axis=0)
+            x["choices"] = np.squeeze(x["choices"], axis=0)
+        x["metadata"]["model"] = model_name
+        return x
+
+    def validate_params(self, theta: dict) -> None:
+        validate_ssm_parameters(self._config.get("name", ""), theta)
+
+    @property
+    def config(self) -> dict:
+        return deepcopy(self._config)
+
+    @property
+    def parameter_adapter(self):
+        return self._parameter_adapter
+
+
+def simulator(theta, model: str = "angle", n_samples: int = 1000, delta_t: float = 0.001,
+              max_t: float = 20, no_noise: bool = False, sigma_noise=None, smooth_unif: bool = True,
+              random_state=None, return_option: str = "full", n_threads: int = 1,
+              extra_fields: dict | None = None) -> dict:
+    """Functional interface (simulator.py:624-864) with the derived outputs."""
+    cfg = ModelConfigBuilder.from_model(model)
+    sim = Simulator(cfg)
+    theta_pre = _preprocess_theta_generic(theta)
+    n_trials = (theta_pre[cfg["params"][0]].shape[0] if isinstance(theta_pre, dict)
+                else (1 if np.ndim(theta_pre) == 1 else theta_pre.shape[0]))
+    x = sim.simulate(theta, n_samples=n_samples, delta_t=delta_t, max_t=max_t, no_noise=no_noise,
+                     sigma_noise=sigma_noise, smooth_unif=smooth_unif, random_state=random_state,
+                     return_option=return_option, n_threads=n_threads, extra_fields=extra_fields)
+    rts = x["rts"].reshape(n_samples, n_trials, 1)
+    chs = x["choices"].reshape(n_samples, n_trials, 1)
+    pc = x["metadata"]["possible_choices"]
+    x["choice_p"] = np.zeros((n_trials, len(pc)))
+    x["choice_p_no_omission"] = np.zeros((n_trials, len(pc)))
+    x["omission_p"] = np.zeros((n_trials, 1))
+    x["nogo_p"] = np.zeros((n_trials, 1))
+    x["go_p"] = np.zeros((n_trials, 1))
+    for k in range(n_trials):
+        r, c = rts[:, k, :], chs[:, k, :]
+        kept = r != OMISSION_SENTINEL
+        n_keep = int(kept.sum())
+        for i, ch in enumerate(pc):
+            x["choice_p"][k, i] = (c == ch).sum() / r.shape[0]
+            x["choice_p_no_omission"][k, i] = ((c[kept] == ch).sum() / n_keep) if n_keep > 0 else OMISSION_SENTINEL
+        x["omission_p"][k, 0] = (r == OMISSION_SENTINEL).sum() / r.shape[0]
+        x["nogo_p"][k, 0] = ((c != max(pc)) | (r == OMISSION_SENTINEL)).sum() / r.shape[0]
+        x["go_p"][k, 0] = 1 - x["nogo_p"][k, 0]
+    x["metadata"]["model"] = model
+    x["binned_128"] = np.expand_dims(bin_simulator_output(x, nbins=128, max_t=-1, freq_cnt=True), axis=0)
+    x["binned_256"] = np.expand_dims(bin_simulator_output(x, nbins=256, max_t=-1, freq_cnt=True), axis=0)
+    return x

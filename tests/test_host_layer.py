@@ -1,0 +1,106 @@
+"""Host layer of Simulator.simulate (no GPU): theta normalisation, noise
+vector, per-model parameter transforms and boundary dict must hand each
+simulator exactly the keyword arguments the reference hands it
+(tests/golden/adapter_kwargs.npz, produced by the reference itself)."""
+
+import json
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+
+from ssms_b200 import ModelConfigBuilder, Simulator, model_config
+from ssms_b200.simulator import bin_simulator_output
+
+ARR = dict(np.load(GOLDEN / "adapter_kwargs.npz"))
+META = json.loads((GOLDEN / "adapter_meta.json").read_text())
+MODELS = sorted({k.split("|")[0] for k in META})
+
+
+def _recording_config(name):
+    cfg = ModelConfigBuilder.from_model(name)
+    rec = {}
+
+    def recorder(**kw):
+        rec.update(kw)
+        n, k = kw["n_samples"], kw["n_trials"]
+        return {"rts": np.zeros((n, k, 1), np.float32), "choices": np.zeros((n, k, 1), np.int32),
+                "metadata": {"possible_choices": cfg["choices"]}}
+
+    cfg["simulator"] = recorder
+    return cfg, rec
+
+
+def test_all_reference_models_with_built_simulators_are_configured():
+    assert set(MODELS) == set(model_config)
+    assert len(MODELS) == 36
+
+
+@pytest.mark.parametrize("name", MODELS)
+def test_simulator_hands_the_reference_arguments(name):
+    cfg, rec = _recording_config(name)
+    params = cfg["params"]
+    theta_in = ARR[f"{name}|theta_in"]
+    theta = {p: theta_in[i] for i, p in enumerate(params)}
+    Simulator(cfg).simulate(theta, n_samples=3, random_state=5)
+    assert sorted(k for k, v in rec.items() if isinstance(v, np.ndarray)) == META[f"{name}|array_keys"]
+    for k in META[f"{name}|array_keys"]:
+        ref = ARR[f"{name}|{k}"]
+        assert rec[k].dtype == ref.dtype, (k, rec[k].dtype, ref.dtype)
+        np.testing.assert_array_equal(rec[k], ref, err_msg=k)
+    assert rec["boundary_fun"].__name__ == META[f"{name}|boundary_fun"]
+    assert sorted(rec["boundary_params"]) == META[f"{name}|bp_keys"]
+    for bk in META[f"{name}|bp_keys"]:
+        np.testing.assert_array_equal(rec["boundary_params"][bk], ARR[f"{name}|bp|{bk}"])
+    for key in ("n_samples", "n_trials", "max_t", "delta_t", "random_state", "return_option",
+                "smooth_unif", "n_threads", "nact"):
+        if f"{name}|{key}" in META:
+            assert rec[key] == META[f"{name}|{key}"], key
+
+
+def test_deadline_variant_and_overrides():
+    cfg = ModelConfigBuilder.from_model("angle_deadline")
+    assert cfg["params"][-1] == "deadline" and cfg["name"] == "angle_deadline"
+    assert cfg["param_bounds_dict"]["deadline"] == (0.001, 10.0)
+    cfg = ModelConfigBuilder.from_model("ddm", param_bounds=[[-4, 0.3, 0.1, 0], [4, 3, 0.9, 2]])
+    assert cfg["param_bounds_dict"]["v"] == (-4, 4)
+    with pytest.raises(ValueError, match="Unknown model"):
+        ModelConfigBuilder.from_model("not_a_model")
+
+
+def test_theta_forms_agree():
+    """dict, list, array and DataFrame thetas normalise to the same arguments."""
+    import pandas as pd
+
+    outs = []
+    for form in ("dict", "list", "array", "frame"):
+        cfg, rec = _recording_config("angle")
+        vals = [0.5, 1.2, 0.4, 0.3, 0.2]
+        theta = {"dict": dict(zip(cfg["params"], vals)), "list": vals, "array": np.array(vals),
+                 "frame": pd.DataFrame([dict(zip(cfg["params"], vals))])}[form]
+        Simulator(cfg).simulate(theta, n_samples=2, random_state=1)
+        outs.append({k: v for k, v in rec.items() if isinstance(v, np.ndarray)})
+    for o in outs[1:]:
+        for k in outs[0]:
+            np.testing.assert_array_equal(o[k], outs[0][k])
+
+
+def test_uneven_theta_vectors_raise():
+    cfg, _ = _recording_config("ddm")
+    with pytest.raises(ValueError):
+        Simulator(cfg).simulate({"v": [0.1, 0.2], "a": [1, 2, 3], "z": 0.5, "t": 0.1})
+
+
+def test_random_state_range_is_validated():
+    cfg, _ = _recording_config("ddm")
+    with pytest.raises(ValueError, match="outside"):
+        Simulator(cfg).simulate({"v": 0.1, "a": 1, "z": 0.5, "t": 0.1}, random_state=2**40)
+
+
+def test_bin_simulator_output_counts():
+    out = {"rts": np.array([[0.5], [1.0], [30.0], [2.0]], np.float32),
+           "choices": np.array([[1], [-1], [1], [1]], np.int32),
+           "metadata": {"max_t": 20.0, "possible_choices": [-1, 1], "n_samples": 4}}
+    h = bin_simulator_output(out, nbins=4, max_t=-1, freq_cnt=True)
+    assert h.shape == (4, 2) and h.sum() == 4 and h[3, 1] == 1  # rt 30 lands in the open last bin
