@@ -179,6 +179,66 @@ int ssm_lba_vanilla(const float *v, const float *a, const float *z, const float 
                     const int64_t *sample_offsets, uint64_t seed, const float *noise_u,
                     const float *noise_g, float *rts, int32_t *choices, void *stream);
 
+/* ---- log-rt Gaussian KDE (batched over parameter sets) ------------------ */
+/*
+ * ssm_kde_fit -- replaces LogKDE.__init__ / _attach_data_from_simulator /
+ * compute_bandwidths (ssms/support_utils/kde_class.py:48-186, 438-504) and
+ * bandwidth_silverman (:508-553) for n_sets simulated data sets at once.
+ * Set s owns rts/choices [sample_offsets[s], sample_offsets[s+1]).  Group
+ * g = s * n_choices + c collects log(rt - displace[s]) of the set's
+ * non-omitted samples with choice choice_values[c] into
+ * points[point_offsets[g] .. point_offsets[g+1]) (sample order), and gets
+ * count_all (omissions included), n_valid, proportion = count_all / n,
+ * bandwidth (Silverman on the group's log-rts, -1 when empty) and
+ * log_norm = log p - log n - log h - log(2 pi)/2.  points must hold the
+ * sets' total sample count.  displace may be NULL.
+ */
+int ssm_kde_fit(const float *rts, const int32_t *choices, int64_t n_sets,
+                const int64_t *sample_offsets, const int32_t *choice_values, int n_choices,
+                const float *displace, int64_t *count_all, int64_t *n_valid,
+                int64_t *point_offsets, float *points, double *bandwidth, double *log_norm,
+                double *proportion, void *stream);
+
+/*
+ * ssm_kde_eval -- replaces LogKDE.kde_eval (kde_class.py:188-329): for each
+ * query (rt, group), queries sorted by group with query_offsets[G+1],
+ * loglik = log_norm + log sum_j exp(-(q - x_j)^2 / 2h^2) - q with
+ * q = log(max(rt - displace, eps)); lb where that is <= lb or rt - displace
+ * <= 0; -log(n_set * max_t) for groups without data.  float64 output.
+ * query_split > 1 splits a group's queries over that many CTAs.
+ */
+int ssm_kde_eval(const float *points, const int64_t *point_offsets, const double *bandwidth,
+                 const double *log_norm, int64_t n_sets, int n_choices,
+                 const int64_t *sample_offsets, const float *displace,
+                 const int64_t *query_offsets, const double *query_rt, double lb, double eps,
+                 double max_t, int query_split, double *out_loglik, void *stream);
+
+/*
+ * ssm_kde_sample -- replaces LogKDE.kde_sample's per-choice draws
+ * (kde_class.py:331-434; KernelDensity.sample for a Gaussian kernel): group g
+ * fills out_rt[out_offsets[g] ..]: the first n_kde[g] slots with
+ * exp(x_J + h N(0,1)) + displace (J uniform over the group's points; U(0,
+ * max_t) + displace when the group is empty), the remaining slots with
+ * U(unif_lo, unif_hi) rts (the mixture's uniform component).
+ */
+int ssm_kde_sample(const float *points, const int64_t *point_offsets, const double *bandwidth,
+                   int64_t n_sets, int n_choices, const float *displace,
+                   const int64_t *out_offsets, const int64_t *n_kde, uint64_t seed, double max_t,
+                   double unif_lo, double unif_hi, double *out_rt, void *stream);
+
+/*
+ * ssm_kde_records -- the row layout of ResampleMixtureStrategy.generate
+ * (ssms/dataset_generators/strategies/resample_mixture_strategy.py:64-214):
+ * per set, rows [theta..., rt, choice, loglik] (float32) for its evaluated
+ * queries plus n_down rows with rt ~ U(-1, 0.0001) and loglik =
+ * negative_rt_loglik, shuffled within the set.  rows_per_set <= 12288.
+ */
+int ssm_kde_records(const float *theta, int n_params, int64_t n_sets, int n_choices,
+                    const int32_t *choice_values, const int64_t *query_offsets,
+                    const double *query_rt, const double *query_loglik, int64_t n_down,
+                    int64_t rows_per_set, float negative_rt_loglik, uint64_t seed, float *out,
+                    void *stream);
+
 /*
  * ssm_ddm_flexbound_static -- no counterpart in the reference.  The same
  * simulation as ssm_ddm_flexbound for callers that cannot allocate device
