@@ -100,10 +100,12 @@ int ssm_ddm_flexbound(const float *v, const float *a, const float *z, const floa
 
 /*
  * ssm_ddm -- replaces cssm.ddm (src/cssm/ddm_models.pyx:349-582): the legacy
- * DDM on [0, a] with start z a and exit when y > a or y < 0.
+ * DDM on [0, a] with start z a and exit when y > a or y < 0.  Layout and noise
+ * conventions as ssm_ddm_flexbound.
  */
 int ssm_ddm(const float *v, const float *a, const float *z, const float *t, const float *deadline,
-            const float *s, int64_t n_trials, int64_t n_samples, float max_t, float delta_t,
+            const float *s, int64_t n_trials, int64_t n_samples, const int64_t *sample_offsets,
+            float max_t, float delta_t,
             uint64_t seed, int smooth_unif, const float *noise_rows, int64_t noise_row_len,
             const float *noise_unif, float *rts, int32_t *choices, int32_t *steps, float *traj,
             int64_t traj_len, const ssm_launch *launch, void *workspace, size_t workspace_bytes,
@@ -238,6 +240,21 @@ int ssm_kde_records(const float *theta, int n_params, int64_t n_sets, int n_choi
                     const double *query_rt, const double *query_loglik, int64_t n_down,
                     int64_t rows_per_set, float negative_rt_loglik, uint64_t seed, float *out,
                     void *stream);
+
+/*
+ * ssm_set_summary -- the auxiliary labels of SimulationPipeline
+ * (ssms/dataset_generators/pipelines/simulation_pipeline.py:262-351) per set:
+ * choice counts [n_sets * n_choices], no-go counts ((choice != max choice) or
+ * rt == -999), omission counts (choices equal to -999, as the pipeline counts
+ * them) and per-choice rt histograms with np.histogram's rules over
+ * np.linspace(0, max_t, nbins + 1), omissions excluded, laid out
+ * [n_sets, nbins, n_choices].
+ */
+int ssm_set_summary(const float *rts, const int32_t *choices, int64_t n_sets,
+                    const int64_t *sample_offsets, const int32_t *choice_values, int n_choices,
+                    double max_t, int64_t *choice_counts, int64_t *nogo_counts,
+                    int64_t *omission_counts, int nbins_a, float *hist_a, int nbins_b,
+                    float *hist_b, void *stream);
 
 /*
  * ssm_ddm_flexbound_static -- no counterpart in the reference.  The same

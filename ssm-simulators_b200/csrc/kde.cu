@@ -398,9 +398,104 @@ __global__ void __launch_bounds__(256) k_kde_records(const KdeRecords a) {
     }
 }
 
+// Per-set summaries for the auxiliary labels of the data pipeline
+// (simulation_pipeline.py:262-351): choice counts, the pipeline's omission
+// count (choices equal to -999), no-go count ((choice != max choice) or rt ==
+// -999) and per-choice rt histograms over np.linspace(0, max_t, nb + 1) with
+// numpy's index rules (right edge inclusive in the last bin, float64 edges,
+// +-1 corrections at the edges), omissions excluded.
+struct SetSummary {
+    const float *rts;
+    const int32_t *choices;
+    const int64_t *soff;
+    const int32_t *cvals;
+    int nc;
+    double max_t;
+    int64_t *counts, *nogo, *omit;
+    int nb_a, nb_b;
+    float *hist_a, *hist_b;
+};
+
+__device__ __forceinline__ int np_hist_index(double v, double max_t, int nb) {
+    if (!(v >= 0.0) || !(v <= max_t)) return -1;
+    const double step = max_t / (double)nb;
+    int i = (int)((v / max_t) * (double)nb);
+    if (i == nb) i -= 1;
+    const double lo = (double)i * step;
+    if (v < lo) i -= 1;
+    const double hi = (i + 1 == nb) ? max_t : (double)(i + 1) * step;
+    if (i != nb - 1 && v >= hi) i += 1;
+    return i;
+}
+
+__global__ void __launch_bounds__(256) k_set_summary(const SetSummary a) {
+    extern __shared__ unsigned int sh[];  // [nc * (nb_a + nb_b)] histogram counters
+    __shared__ unsigned long long cnt[KDE_MAX_CHOICES];
+    __shared__ unsigned long long nogo, omit;
+    const int64_t s = blockIdx.x;
+    const int H = a.nc * (a.nb_a + a.nb_b);
+    int32_t max_choice = __ldg(a.cvals);
+    for (int c = 1; c < a.nc; ++c) max_choice = max(max_choice, __ldg(a.cvals + c));
+    for (int i = threadIdx.x; i < H; i += blockDim.x) sh[i] = 0u;
+    if (threadIdx.x < KDE_MAX_CHOICES) cnt[threadIdx.x] = 0ull;
+    if (threadIdx.x == 0) nogo = omit = 0ull;
+    __syncthreads();
+    for (int64_t i = a.soff[s] + threadIdx.x; i < a.soff[s + 1]; i += blockDim.x) {
+        const int32_t ch = a.choices[i];
+        const float rt = a.rts[i];
+        if (ch == -999) atomicAdd(&omit, 1ull);
+        if (ch != max_choice || rt == -999.f) atomicAdd(&nogo, 1ull);
+        const int c = choice_index(ch, a.cvals, a.nc);
+        if (c < 0) continue;
+        atomicAdd(&cnt[c], 1ull);
+        if (rt == -999.f) continue;
+        const int ia = np_hist_index((double)rt, a.max_t, a.nb_a);
+        if (ia >= 0) atomicAdd(&sh[c * a.nb_a + ia], 1u);
+        const int ib = np_hist_index((double)rt, a.max_t, a.nb_b);
+        if (ib >= 0) atomicAdd(&sh[a.nc * a.nb_a + c * a.nb_b + ib], 1u);
+    }
+    __syncthreads();
+    if (threadIdx.x < a.nc) a.counts[s * a.nc + threadIdx.x] = (int64_t)cnt[threadIdx.x];
+    if (threadIdx.x == 0) {
+        a.nogo[s] = (int64_t)nogo;
+        a.omit[s] = (int64_t)omit;
+    }
+    // layout [S, nb, nc] like the pipeline's binned_128 / binned_256 arrays
+    for (int i = threadIdx.x; i < a.nc * a.nb_a; i += blockDim.x) {
+        const int c = i / a.nb_a, b = i % a.nb_a;
+        a.hist_a[(s * a.nb_a + b) * a.nc + c] = (float)sh[i];
+    }
+    for (int i = threadIdx.x; i < a.nc * a.nb_b; i += blockDim.x) {
+        const int c = i / a.nb_b, b = i % a.nb_b;
+        a.hist_b[(s * a.nb_b + b) * a.nc + c] = (float)sh[a.nc * a.nb_a + i];
+    }
+}
+
 }  // namespace ssm
 
 extern "C" {
+
+int ssm_set_summary(const float *rts, const int32_t *choices, int64_t n_sets,
+                    const int64_t *sample_offsets, const int32_t *choice_values, int n_choices,
+                    double max_t, int64_t *choice_counts, int64_t *nogo_counts,
+                    int64_t *omission_counts, int nbins_a, float *hist_a, int nbins_b,
+                    float *hist_b, void *stream) {
+    using namespace ssm;
+    SSM_REQUIRE(n_sets >= 0 && n_choices >= 1 && n_choices <= KDE_MAX_CHOICES, "bad n_sets / n_choices");
+    SSM_REQUIRE(nbins_a >= 1 && nbins_b >= 1 && (size_t)n_choices * (nbins_a + nbins_b) * 4 <= 48 * 1024,
+                "histograms must fit in 48 KB of shared memory");
+    if (n_sets == 0) return SSM_OK;
+    SSM_REQUIRE(rts && choices && sample_offsets && choice_values && choice_counts && nogo_counts &&
+                omission_counts && hist_a && hist_b, "all buffers are required");
+    SetSummary a;
+    a.rts = rts; a.choices = choices; a.soff = sample_offsets; a.cvals = choice_values;
+    a.nc = n_choices; a.max_t = max_t; a.counts = choice_counts; a.nogo = nogo_counts;
+    a.omit = omission_counts; a.nb_a = nbins_a; a.nb_b = nbins_b; a.hist_a = hist_a; a.hist_b = hist_b;
+    const size_t smem = (size_t)n_choices * (nbins_a + nbins_b) * sizeof(unsigned int);
+    k_set_summary<<<(unsigned)n_sets, 256, smem, (cudaStream_t)stream>>>(a);
+    SSM_CUDA(cudaGetLastError());
+    return SSM_OK;
+}
 
 int ssm_kde_fit(const float *rts, const int32_t *choices, int64_t n_sets,
                 const int64_t *sample_offsets, const int32_t *choice_values, int n_choices,

@@ -583,13 +583,14 @@ int ssm_ddm_flexbound(const float *v, const float *a, const float *z, const floa
 }
 
 int ssm_ddm(const float *v, const float *a, const float *z, const float *t, const float *deadline,
-            const float *s, int64_t n_trials, int64_t n_samples, float max_t, float delta_t,
+            const float *s, int64_t n_trials, int64_t n_samples, const int64_t *sample_offsets,
+            float max_t, float delta_t,
             uint64_t seed, int smooth_unif, const float *noise_rows, int64_t noise_row_len,
             const float *noise_unif, float *rts, int32_t *choices, int32_t *steps, float *traj,
             int64_t traj_len, const ssm_launch *launch, void *workspace, size_t workspace_bytes,
             void *stream) {
     ssm::SingleCall c{ssm::M_LEGACY, v, a, z, nullptr, t, deadline, s, n_trials, n_samples,
-                      nullptr, max_t, nullptr, delta_t, SSM_BOUND_CONSTANT, nullptr, nullptr,
+                      sample_offsets, max_t, nullptr, delta_t, SSM_BOUND_CONSTANT, nullptr, nullptr,
                       nullptr, 0, 0, seed, smooth_unif, noise_rows, noise_row_len, noise_unif,
                       rts, choices, steps, traj, traj_len, launch, workspace, workspace_bytes,
                       stream};

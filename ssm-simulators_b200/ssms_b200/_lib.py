@@ -55,7 +55,7 @@ _SIGNATURES: dict[str, tuple] = {
     "ssm_ddm_flexbound": (_I, [_P, _P, _P, _P, _P, _P, _I64, _I64, _P, _F, _P, _F, _I, _P, _P, _P,
                                _I64, _I64, _U64, _I, _P, _I64, _P, _P, _P, _P, _P, _I64, _P, _P,
                                C.c_size_t, _P]),
-    "ssm_ddm": (_I, [_P, _P, _P, _P, _P, _P, _I64, _I64, _F, _F, _U64, _I, _P, _I64, _P, _P, _P, _P,
+    "ssm_ddm": (_I, [_P, _P, _P, _P, _P, _P, _I64, _I64, _P, _F, _F, _U64, _I, _P, _I64, _P, _P, _P, _P,
                      _P, _I64, _P, _P, C.c_size_t, _P]),
     "ssm_levy_flexbound": (_I, [_P, _P, _P, _P, _P, _P, _P, _I64, _I64, _P, _F, _F, _I, _P, _P, _P,
                                 _I64, _I64, _U64, _I, _P, _I64, _P, _P, _P, _P, _P, _I64, _P, _P,
@@ -76,6 +76,7 @@ _SIGNATURES: dict[str, tuple] = {
                           C.c_double, _I, _P, _P]),
     "ssm_kde_sample": (_I, [_P, _P, _P, _I64, _I, _P, _P, _P, _U64, C.c_double, C.c_double,
                             C.c_double, _P, _P]),
+    "ssm_set_summary": (_I, [_P, _P, _I64, _P, _P, _I, C.c_double, _P, _P, _P, _I, _P, _I, _P, _P]),
     "ssm_kde_records": (_I, [_P, _I, _I64, _I, _P, _P, _P, _P, _I64, _I64, _F, _U64, _P, _P]),
 }
 

@@ -116,7 +116,7 @@ def simulate_single(model: str, *, v, z, t, deadline, s, a=None, alpha=None,
     elif model == MODEL_LEGACY:
         status = L.ssm_ddm(
             D.ptr(vt), D.ptr(at), D.ptr(zt), D.ptr(tt), D.ptr(dlt), D.ptr(st), K, int(n_samples),
-            float(np.float32(max_t)), float(np.float32(delta_t)), *common_tail,
+            D.ptr(offs), float(np.float32(max_t)), float(np.float32(delta_t)), *common_tail,
             ctypes.addressof(lopt), D.ptr(ws), ws.numel(), sp)
     elif model == MODEL_LEVY:
         if alt is None:

@@ -240,10 +240,12 @@ class Simulator:
         else:
             raise ValueError("boundary must be a string name or callable function")
 
-    def simulate(self, theta, n_samples: int = 1000, delta_t: float = 0.001, max_t: float = 20,
-                 no_noise: bool = False, sigma_noise=None, smooth_unif: bool = True,
-                 random_state=None, return_option: str = "full", n_threads: int = 1,
-                 extra_fields: dict | None = None) -> dict:
+    def prepare(self, theta, n_samples: int = 1000, delta_t: float = 0.001, max_t: float = 20,
+                no_noise: bool = False, sigma_noise=None, smooth_unif: bool = True,
+                random_state=None, return_option: str = "full", n_threads: int = 1) -> dict:
+        """Everything simulate() does before calling the simulator: returns
+        {"config", "model_name", "n_trials", "theta" (adapted), "boundary",
+        "sim_params"} (simulator_class.py:511-660)."""
         cfg = deepcopy(self._config)
         model_name = cfg.get("name", "").replace("_deadline", "")
         is_deadline = "deadline" in cfg.get("params", [])
@@ -267,6 +269,19 @@ class Simulator:
             theta = tr.apply(theta, cfg, n_trials)
         boundary_dict = make_boundary_dict(cfg, theta) if ("boundary_name" in cfg or "boundary" in cfg) else {}
         validate_ssm_parameters(model_name, theta)
+        return {"config": cfg, "model_name": model_name, "n_trials": n_trials, "theta": theta,
+                "boundary": boundary_dict, "sim_params": sim_params}
+
+    def simulate(self, theta, n_samples: int = 1000, delta_t: float = 0.001, max_t: float = 20,
+                 no_noise: bool = False, sigma_noise=None, smooth_unif: bool = True,
+                 random_state=None, return_option: str = "full", n_threads: int = 1,
+                 extra_fields: dict | None = None) -> dict:
+        prep = self.prepare(theta, n_samples=n_samples, delta_t=delta_t, max_t=max_t,
+                            no_noise=no_noise, sigma_noise=sigma_noise, smooth_unif=smooth_unif,
+                            random_state=random_state, return_option=return_option,
+                            n_threads=n_threads)
+        cfg, model_name, n_trials = prep["config"], prep["model_name"], prep["n_trials"]
+        theta, boundary_dict, sim_params = prep["theta"], prep["boundary"], prep["sim_params"]
         x = cfg["simulator"](**theta, **boundary_dict, **sim_params, **(extra_fields or {}))
         if not isinstance(x, dict):
             raise TypeError(f"Simulator returned {type(x).__name__}, expected dict")
