@@ -193,13 +193,15 @@ int ssm_lba_vanilla(const float *v, const float *a, const float *z, const float 
  * count_all (omissions included), n_valid, proportion = count_all / n,
  * bandwidth (Silverman on the group's log-rts, -1 when empty) and
  * log_norm = log p - log n - log h - log(2 pi)/2.  points must hold the
- * sets' total sample count.  displace may be NULL.
+ * sets' total sample count.  displace (float64 per set) may be NULL; when
+ * given, displaced_logs (float64, total samples) receives the values the
+ * reference's bandwidth is computed from, log(exp(log_f32 rt) - displace).
  */
 int ssm_kde_fit(const float *rts, const int32_t *choices, int64_t n_sets,
                 const int64_t *sample_offsets, const int32_t *choice_values, int n_choices,
-                const float *displace, int64_t *count_all, int64_t *n_valid,
-                int64_t *point_offsets, float *points, double *bandwidth, double *log_norm,
-                double *proportion, void *stream);
+                const double *displace, double *displaced_logs, int64_t *count_all,
+                int64_t *n_valid, int64_t *point_offsets, float *points, double *bandwidth,
+                double *log_norm, double *proportion, void *stream);
 
 /*
  * ssm_kde_eval -- replaces LogKDE.kde_eval (kde_class.py:188-329): for each
@@ -211,7 +213,7 @@ int ssm_kde_fit(const float *rts, const int32_t *choices, int64_t n_sets,
  */
 int ssm_kde_eval(const float *points, const int64_t *point_offsets, const double *bandwidth,
                  const double *log_norm, int64_t n_sets, int n_choices,
-                 const int64_t *sample_offsets, const float *displace,
+                 const int64_t *sample_offsets, const double *displace,
                  const int64_t *query_offsets, const double *query_rt, double lb, double eps,
                  double max_t, int query_split, double *out_loglik, void *stream);
 
@@ -224,7 +226,7 @@ int ssm_kde_eval(const float *points, const int64_t *point_offsets, const double
  * U(unif_lo, unif_hi) rts (the mixture's uniform component).
  */
 int ssm_kde_sample(const float *points, const int64_t *point_offsets, const double *bandwidth,
-                   int64_t n_sets, int n_choices, const float *displace,
+                   int64_t n_sets, int n_choices, const double *displace,
                    const int64_t *out_offsets, const int64_t *n_kde, uint64_t seed, double max_t,
                    double unif_lo, double unif_hi, double *out_rt, void *stream);
 

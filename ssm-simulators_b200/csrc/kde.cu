@@ -28,7 +28,8 @@ struct KdeFit {
     const int64_t *soff;
     const int32_t *cvals;
     int nc;
-    const float *shift;  // per-set displacement (displace_t) or nullptr
+    const double *shift; // per-set displacement (displace_t) or nullptr
+    double *bwvals;      // [total] displaced-mode bandwidth inputs, or nullptr
     int64_t *count_all;  // [G] samples with choice c, omissions included
     int64_t *n_valid;    // [G] non-omitted samples
     int64_t *poff;       // [G + 1]
@@ -108,7 +109,7 @@ __global__ void __launch_bounds__(256) k_kde_scatter(const KdeFit a) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const unsigned lt = (1u << lane) - 1u;
     if (threadIdx.x < a.nc) base[threadIdx.x] = a.poff[s * a.nc + threadIdx.x];
-    const float sh = a.shift ? a.shift[s] : 0.f;
+    const double sh = a.shift ? a.shift[s] : 0.0;
     __syncthreads();
     const int64_t lo = a.soff[s], hi = a.soff[s + 1];
     for (int64_t c0 = lo; c0 < hi; c0 += blockDim.x) {
@@ -129,9 +130,13 @@ __global__ void __launch_bounds__(256) k_kde_scatter(const KdeFit a) {
         if (ci >= 0) {
             int64_t pos = base[ci] + rank;
             for (int w = 0; w < warp; ++w) pos += wcnt[w][ci];
-            // float32 log of the float32 (displaced) rt, correctly rounded
-            const float r = (a.shift ? __fsub_rn(rt, sh) : rt);
+            // kernels sit on float32 log of the float32 (displaced) rt; with a
+            // shift the rt is displaced in float64 and stored as float32, and the
+            // bandwidth uses log(exp(float32 log rt) - shift) in float64
+            // (kde_class.py:174-186, 478-493)
+            const float r = a.shift ? __double2float_rn((double)rt - sh) : rt;
             a.points[pos] = __double2float_rn(log((double)r));
+            if (a.bwvals) a.bwvals[pos] = log(exp((double)__double2float_rn(log((double)rt))) - sh);
         }
         __syncthreads();
         if (threadIdx.x < a.nc) {
@@ -166,11 +171,12 @@ __global__ void __launch_bounds__(256) k_kde_stats(const KdeFit a) {
     __shared__ double red[32];
     const int64_t lo = a.poff[g], n = a.poff[g + 1] - lo;
     double sum = 0.0;
-    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) sum += (double)a.points[lo + i];
+    for (int64_t i = threadIdx.x; i < n; i += blockDim.x)
+        sum += a.bwvals ? a.bwvals[lo + i] : (double)a.points[lo + i];
     const double mean = block_sum_f64(sum, red) / (double)(n > 0 ? n : 1);
     double ss = 0.0;
     for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
-        const double d = (double)a.points[lo + i] - mean;
+        const double d = (a.bwvals ? a.bwvals[lo + i] : (double)a.points[lo + i]) - mean;
         ss += d * d;
     }
     const double var = block_sum_f64(ss, red) / (double)(n > 0 ? n : 1);
@@ -200,7 +206,7 @@ struct KdeEval {
     double *out;
     int nc;
     const int64_t *soff;
-    const float *shift;
+    const double *shift;
     double lb, eps, max_t;
 };
 
@@ -215,7 +221,7 @@ __global__ void __launch_bounds__(128) k_kde_eval(const KdeEval a) {
     __shared__ __align__(16) float tile[KDE_TILE];
     const int64_t p0 = a.poff[g], n = a.poff[g + 1] - p0;
     const double hg = a.h[g];
-    const double sh = a.shift ? (double)a.shift[s] : 0.0;
+    const double sh = a.shift ? a.shift[s] : 0.0;
     // 2^(-(d*sc)^2) = exp(-d^2 / (2 h^2))
     const float sc = (n > 0) ? (float)(0.8493218002880191 / hg) : 0.f;  // sqrt(log2(e)/2) / h
     const int64_t QT = (int64_t)blockDim.x * QPT;
@@ -297,7 +303,7 @@ struct KdeSample {
     const int64_t *ooff;    // [G + 1] output slots per group
     const int64_t *nkde;    // [G] KDE samples at the start of each group's slots
     int64_t n_groups;
-    const float *shift;
+    const double *shift;
     int nc;
     double max_t, ulo, uhi;
     double *out_rt;
@@ -318,7 +324,7 @@ __global__ void k_kde_sample(const KdeSample a) {
         }
         const int64_t g = lo, j = i - a.ooff[g];
         const uint4 r = philox10(make_uint4((uint32_t)j, (uint32_t)g, (uint32_t)(g >> 32), 7u), a.key);
-        const double sh = a.shift ? (double)a.shift[g / a.nc] : 0.0;
+        const double sh = a.shift ? a.shift[g / a.nc] : 0.0;
         const int64_t n = a.poff[g + 1] - a.poff[g];
         double rt;
         if (j < a.nkde[g]) {
@@ -499,9 +505,9 @@ int ssm_set_summary(const float *rts, const int32_t *choices, int64_t n_sets,
 
 int ssm_kde_fit(const float *rts, const int32_t *choices, int64_t n_sets,
                 const int64_t *sample_offsets, const int32_t *choice_values, int n_choices,
-                const float *displace, int64_t *count_all, int64_t *n_valid,
-                int64_t *point_offsets, float *points, double *bandwidth, double *log_norm,
-                double *proportion, void *stream) {
+                const double *displace, double *displaced_logs, int64_t *count_all,
+                int64_t *n_valid, int64_t *point_offsets, float *points, double *bandwidth,
+                double *log_norm, double *proportion, void *stream) {
     using namespace ssm;
     SSM_REQUIRE(n_sets >= 0, "n_sets must be >= 0");
     SSM_REQUIRE(n_choices >= 1 && n_choices <= KDE_MAX_CHOICES, "n_choices must be in [1, %d]", KDE_MAX_CHOICES);
@@ -510,8 +516,10 @@ int ssm_kde_fit(const float *rts, const int32_t *choices, int64_t n_sets,
                 "all buffers are required");
     if (n_sets == 0) return SSM_OK;
     cudaStream_t st = (cudaStream_t)stream;
-    KdeFit a{rts, choices, n_sets, sample_offsets, choice_values, n_choices, displace, count_all,
-             n_valid, point_offsets, points, bandwidth, log_norm, proportion};
+    SSM_REQUIRE(!displace || displaced_logs, "displace needs the displaced_logs buffer");
+    KdeFit a{rts, choices, n_sets, sample_offsets, choice_values, n_choices, displace,
+             displace ? displaced_logs : nullptr, count_all, n_valid, point_offsets, points,
+             bandwidth, log_norm, proportion};
     const int64_t G = n_sets * n_choices;
     k_kde_count<<<(unsigned)n_sets, 256, 0, st>>>(a);
     SSM_CUDA(cudaGetLastError());
@@ -526,7 +534,7 @@ int ssm_kde_fit(const float *rts, const int32_t *choices, int64_t n_sets,
 
 int ssm_kde_eval(const float *points, const int64_t *point_offsets, const double *bandwidth,
                  const double *log_norm, int64_t n_sets, int n_choices,
-                 const int64_t *sample_offsets, const float *displace,
+                 const int64_t *sample_offsets, const double *displace,
                  const int64_t *query_offsets, const double *query_rt, double lb, double eps,
                  double max_t, int query_split, double *out_loglik, void *stream) {
     using namespace ssm;
@@ -545,7 +553,7 @@ int ssm_kde_eval(const float *points, const int64_t *point_offsets, const double
 }
 
 int ssm_kde_sample(const float *points, const int64_t *point_offsets, const double *bandwidth,
-                   int64_t n_sets, int n_choices, const float *displace,
+                   int64_t n_sets, int n_choices, const double *displace,
                    const int64_t *out_offsets, const int64_t *n_kde, uint64_t seed, double max_t,
                    double unif_lo, double unif_hi, double *out_rt, void *stream) {
     using namespace ssm;

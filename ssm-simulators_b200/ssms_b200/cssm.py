@@ -57,9 +57,8 @@ def _traj_host(traj_t, n):
     return traj
 
 
-def _run_flex(model, v, a, z, t, deadline, s, alpha, max_t, delta_t, n_samples, n_trials,
-              boundary_fun, boundary_params, random_state, return_option, smooth_unif,
-              **kwargs):
+def _run_flex(model, v, a, z, t, deadline, s, levy_alpha, max_t, delta_t, n_samples, n_trials,
+              boundary_fun, boundary_params, random_state, return_option, smooth_unif, extra):
     _check_return_option(return_option)
     n_trials = int(n_trials)
     n_samples = int(n_samples)
@@ -69,12 +68,13 @@ def _run_flex(model, v, a, z, t, deadline, s, alpha, max_t, delta_t, n_samples, 
                                ((v, "v"), (a, "a"), (z, "z"), (t, "t"), (deadline, "deadline"), (s, "s")))
     t_s = bf.make_t_s(max_t, delta_t)
     spec = bf.kernel_spec(boundary_fun, boundary_params, n_trials, t_s,
-                          force_table=bool(kwargs.get("_force_table", False)))
+                          force_table=bool(extra.get("_force_table", False)))
     full = return_option == "full"
     nd = _num_draws(max_t, delta_t)
+    alpha = None if levy_alpha is None else _f32(levy_alpha, "alpha")
     out = dev.simulate_single(
         model, v=v, z=z, t=t, deadline=deadline, s=s, a=spec["a"],
-        alpha=None if alpha is None else _f32(alpha, "alpha"), n_trials=n_trials,
+        alpha=alpha, n_trials=n_trials,
         n_samples=n_samples, max_t=max_t, delta_t=delta_t, bound_kind=spec["kind"],
         bound_p1=spec["p1"], bound_p2=spec["p2"], bound_table=spec["table"],
         seed=_seed(random_state), smooth_unif=smooth_unif,
@@ -109,7 +109,7 @@ def ddm_flexbound(v, a, z, t, deadline, s, max_t=20, delta_t=0.001, n_samples=20
     """DDM with flexible symmetric bounds +-b(t) (src/cssm/ddm_models.pyx:589-878)."""
     return _run_flex("ddm_flexbound", v, a, z, t, deadline, s, None, max_t, delta_t, n_samples,
                      n_trials, boundary_fun, boundary_params, random_state, return_option,
-                     smooth_unif, **kwargs)
+                     smooth_unif, kwargs)
 
 
 def levy_flexbound(v, z, alpha, t, deadline, s, delta_t=0.001, max_t=20, n_samples=20000,
@@ -119,7 +119,7 @@ def levy_flexbound(v, z, alpha, t, deadline, s, delta_t=0.001, max_t=20, n_sampl
     a = np.asarray(boundary_params.get("a", np.ones(int(n_trials))), dtype=np.float32)
     return _run_flex("levy_flexbound", v, a, z, t, deadline, s, alpha, max_t, delta_t, n_samples,
                      n_trials, boundary_fun, boundary_params, random_state, return_option,
-                     smooth_unif, **kwargs)
+                     smooth_unif, kwargs)
 
 
 def ddm(v, a, z, t, deadline, s, max_t=20, delta_t=0.001, n_samples=20000, n_trials=10,
@@ -154,7 +154,7 @@ def _param_dict(arr, prefix, n):
 
 
 def _run_race(model, v, z, t, s, deadline, g, b, delta_t, max_t, n_samples, n_trials,
-              boundary_fun, boundary_params, random_state, return_option, smooth_unif, **kwargs):
+              boundary_fun, boundary_params, random_state, return_option, smooth_unif, extra):
     _check_return_option(return_option)
     n_trials, n_samples = int(n_trials), int(n_samples)
     if boundary_fun is None:
@@ -165,7 +165,7 @@ def _run_race(model, v, z, t, s, deadline, g, b, delta_t, max_t, n_samples, n_tr
     n_part = v.shape[1]
     t_s = bf.make_t_s(max_t, delta_t)
     spec = bf.kernel_spec(boundary_fun, boundary_params, n_trials, t_s,
-                          force_table=bool(kwargs.get("_force_table", False)))
+                          force_table=bool(extra.get("_force_table", False)))
     full = return_option == "full"
     n_rows = int(np.float32(np.float32(max_t) / np.float32(delta_t))) + 1
     out = dev.simulate_race(
@@ -211,7 +211,7 @@ def race_model(v, z, t, s, deadline, delta_t=0.001, max_t=20, n_samples=2000, n_
     """Race of n accumulators clipped at 0 (src/cssm/race_models.pyx:141-506)."""
     return _run_race("race_model", v, z, t, s, deadline, None, None, delta_t, max_t, n_samples,
                      n_trials, boundary_fun, boundary_params, random_state, return_option,
-                     smooth_unif, **kwargs)
+                     smooth_unif, kwargs)
 
 
 def lca(v, z, g, b, t, s, deadline, delta_t=0.001, max_t=20, n_samples=2000, n_trials=1,
@@ -220,7 +220,7 @@ def lca(v, z, g, b, t, s, deadline, delta_t=0.001, max_t=20, n_samples=2000, n_t
     """Leaky competing accumulators (src/cssm/race_models.pyx:509-920)."""
     return _run_race("lca", v, z, t, s, deadline, g, b, delta_t, max_t, n_samples, n_trials,
                      boundary_fun, boundary_params, random_state, return_option, smooth_unif,
-                     **kwargs)
+                     kwargs)
 
 
 def lba_vanilla(v, a, z, deadline, sd, t, nact=3, n_samples=2000, n_trials=1, max_t=20,

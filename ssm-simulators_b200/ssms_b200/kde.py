@@ -62,7 +62,14 @@ class KdeBatch:
         self.rts = rts.to(dev, torch.float32).contiguous().reshape(-1)
         self.choices = choices.to(dev, torch.int32).contiguous().reshape(-1)
         self.cvals = torch.as_tensor(self.choice_values).to(dev)
-        self.displace = None if displace is None else D.to_dev_f32(displace, self.n_sets, "displace")
+        self.displace = None
+        self.displaced_logs = None
+        if displace is not None:
+            dsp = np.asarray(displace, dtype=np.float64).reshape(-1)
+            if dsp.shape[0] < self.n_sets:
+                raise ValueError("displace needs one value per set")
+            self.displace = torch.from_numpy(np.ascontiguousarray(dsp)).to(dev)
+            self.displaced_logs = torch.empty(max(total, 1), dtype=torch.float64, device=dev)
         self.count_all = torch.empty(G, dtype=torch.int64, device=dev)
         self.n_valid = torch.empty(G, dtype=torch.int64, device=dev)
         self.point_offsets = torch.empty(G + 1, dtype=torch.int64, device=dev)
@@ -73,7 +80,8 @@ class KdeBatch:
         self.stream = stream
         _lib.check(_lib.lib().ssm_kde_fit(
             D.ptr(self.rts), D.ptr(self.choices), self.n_sets, D.ptr(self.sample_offsets),
-            D.ptr(self.cvals), self.nc, D.ptr(self.displace), D.ptr(self.count_all),
+            D.ptr(self.cvals), self.nc, D.ptr(self.displace), D.ptr(self.displaced_logs),
+            D.ptr(self.count_all),
             D.ptr(self.n_valid), D.ptr(self.point_offsets), D.ptr(self.points),
             D.ptr(self.bandwidth), D.ptr(self.log_norm), D.ptr(self.proportion),
             D.stream_ptr(stream)))
