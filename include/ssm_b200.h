@@ -287,6 +287,50 @@ int ssm_ddm_flexbound_static(const float *v, const float *a, const float *z, con
                              int32_t *choices, int32_t *steps, float *traj, int64_t traj_len,
                              const ssm_launch *launch, void *stream);
 
+/*
+ * Likelihood surrogate -- no counterpart in the reference, which only writes
+ * the (theta, rt, choice, loglik) training records
+ * (ssms/dataset_generators/lan_mlp.py:66-133, the records of
+ * ResampleMixtureStrategy) for a network trained elsewhere.  A 7 -> 100 ->
+ * 100 -> 120 -> 1 tanh MLP: layers 1-3 run on the tensor cores with bf16
+ * weights and activations and fp32 accumulation, the 120 -> 1 output layer in
+ * fp32.  Inputs are [theta(5), rt, choice] rows, normalised as
+ * (x - norm_c[j]) * norm_s[j] before the first layer.
+ *
+ * Parameters live in one fp32 vector of SSM_MLP_NPARAMS floats in nn.Linear
+ * order (W1[100,7], b1, W2[100,100], b2, W3[120,100], b3, w4[120], b4).  The
+ * kernels read a packed image of SSM_MLP_IMAGE_BYTES bytes (16-byte aligned)
+ * made by ssm_mlp_pack and kept current by ssm_mlp_adam.  `status` (device int,
+ * may be NULL) receives SSM_MLP_ERR_TIMEOUT if a bounded wait expired.
+ */
+#define SSM_MLP_NPARAMS 23141
+#define SSM_MLP_PARTIAL_STRIDE 23168 /* floats per per-CTA gradient partial */
+#define SSM_MLP_IMAGE_BYTES 59280
+#define SSM_MLP_ERR_TIMEOUT 7
+int ssm_mlp_pack(const float *params, void *image, void *stream);
+
+/* out[i] = net(x[i]); with dx != NULL also dx[i, 0:7] = d out[i] / d x[i]. */
+int ssm_mlp_forward(const void *image, const float *x, int64_t n, int x_stride,
+                    const float *norm_c, const float *norm_s, float *out, float *dx,
+                    int dx_stride, int max_ctas, int *status, void *stream);
+
+/*
+ * One training gradient: records [n, rec_stride] = (x[0:7], target); loss
+ * Huber(delta 1) (loss_kind 0) or squared error (1) times inv_batch, summed.
+ * Each of n_ctas CTAs writes its gradient over its rows to
+ * partials[cta * SSM_MLP_PARTIAL_STRIDE + p] and its loss sum (before
+ * inv_batch) to loss_partials[cta]; out (may be NULL) receives predictions.
+ */
+int ssm_mlp_train_grad(const void *image, const float *records, int64_t n, int rec_stride,
+                       const float *norm_c, const float *norm_s, int loss_kind, float inv_batch,
+                       float *out, float *partials, float *loss_partials, int n_ctas,
+                       int *status, void *stream);
+
+/* Adam (Kingma & Ba) on the summed partials; bias_corr_k = 1 - beta_k^step. */
+int ssm_mlp_adam(float *params, float *m, float *v, const float *partials, int n_partials,
+                 float lr, float beta1, float beta2, float eps, float bias_corr1,
+                 float bias_corr2, void *image, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -78,7 +78,16 @@ _SIGNATURES: dict[str, tuple] = {
                             C.c_double, _P, _P]),
     "ssm_set_summary": (_I, [_P, _P, _I64, _P, _P, _I, C.c_double, _P, _P, _P, _I, _P, _I, _P, _P]),
     "ssm_kde_records": (_I, [_P, _I, _I64, _I, _P, _P, _P, _P, _I64, _I64, _F, _U64, _P, _P]),
+    "ssm_mlp_pack": (_I, [_P, _P, _P]),
+    "ssm_mlp_forward": (_I, [_P, _P, _I64, _I, _P, _P, _P, _P, _I, _I, _P, _P]),
+    "ssm_mlp_train_grad": (_I, [_P, _P, _I64, _I, _P, _P, _I, _F, _P, _P, _P, _I, _P, _P]),
+    "ssm_mlp_adam": (_I, [_P, _P, _P, _P, _I, _F, _F, _F, _F, _F, _F, _P, _P]),
 }
+
+MLP_NPARAMS = 23141
+MLP_PARTIAL_STRIDE = 23168
+MLP_IMAGE_BYTES = 59280
+MLP_ERR_TIMEOUT = 7
 
 _lib: C.CDLL | None = None
 
