@@ -288,6 +288,21 @@ int ssm_ddm_flexbound_static(const float *v, const float *a, const float *z, con
                              const ssm_launch *launch, void *stream);
 
 /*
+ * ssm_ddm_nf_loglik -- no counterpart in the reference.  float64
+ * Navarro-Fuss log-density of (rt, choice) under the constant-bound DDM in
+ * the reference's parameterisation (bounds +-a, start -a + 2 z a, choice +1 at
+ * the upper bound, non-decision t, noise s; src/cssm/ddm_models.pyx ddm /
+ * ddm_flexbound), and with out_grad != NULL its gradient [n, 4] w.r.t.
+ * (v, a, z, t).  Parameters are arrays of n entries (per_query_params = 1) or
+ * single values (0); s may be NULL (unit noise).  rt <= t gives -inf (NaN
+ * gradient).  eps is the series truncation error (1e-14 typical).
+ */
+int ssm_ddm_nf_loglik(const double *rt, const int32_t *choice, const double *v, const double *a,
+                      const double *z, const double *t, const double *s, int64_t n,
+                      int per_query_params, double eps, double *out_loglik, double *out_grad,
+                      void *stream);
+
+/*
  * Likelihood surrogate -- no counterpart in the reference, which only writes
  * the (theta, rt, choice, loglik) training records
  * (ssms/dataset_generators/lan_mlp.py:66-133, the records of

@@ -38,50 +38,60 @@ def _n_terms(u, eps):
 
 
 def _g_and_derivs(u, w, eps=1e-14, extra=4):
-    """Standardised density g(u, w) and dg/du, dg/dw (elementwise, float64)."""
+    """log g(u, w) and the ratios (dg/du) / g, (dg/dw) / g (elementwise, float64).
+
+    Each series is summed relative to its leading term (exp(-w^2 / 2u) for
+    the small-time series, exp(-pi^2 u / 2) for the large-time one), so the
+    logarithm stays finite far into the tails where g itself underflows."""
     u = np.asarray(u, np.float64)
     w = np.asarray(w, np.float64) + np.zeros_like(u)
     ks, kl = _n_terms(u, eps)
     small = ks < kl
-    g = np.zeros_like(u)
-    gu = np.zeros_like(u)
-    gw = np.zeros_like(u)
+    logg = np.zeros_like(u)
+    ru = np.zeros_like(u)
+    rw = np.zeros_like(u)
     # small-time series: sum over k in [-K, K]
     if np.any(small):
         us, ws = u[small], w[small]
         K = int(np.ceil(np.max(ks[small]))) + extra
         k = np.arange(-K, K + 1, dtype=np.float64)[:, None]
         c = ws[None, :] + 2 * k
-        e = np.exp(-c * c / (2 * us[None, :]))
-        pref = 1.0 / np.sqrt(2 * np.pi * us ** 3)
-        g[small] = pref * np.sum(c * e, axis=0)
-        gw[small] = pref * np.sum((1 - c * c / us[None, :]) * e, axis=0)
-        gu[small] = pref * np.sum(c * e * (c * c / (2 * us[None, :] ** 2) - 1.5 / us[None, :]), axis=0)
+        e = np.exp(-(c * c - ws[None, :] ** 2) / (2 * us[None, :]))
+        s0 = np.sum(c * e, axis=0)
+        logg[small] = -0.5 * np.log(2 * np.pi * us ** 3) - ws ** 2 / (2 * us) + np.log(s0)
+        rw[small] = np.sum((1 - c * c / us[None, :]) * e, axis=0) / s0
+        ru[small] = np.sum(c * e * (c * c / (2 * us[None, :] ** 2) - 1.5 / us[None, :]), axis=0) / s0
     large = ~small
     if np.any(large):
         ul, wl = u[large], w[large]
         K = int(np.ceil(np.max(kl[large]))) + extra
         k = np.arange(1, K + 1, dtype=np.float64)[:, None]
-        e = np.exp(-k * k * np.pi ** 2 * ul[None, :] / 2)
+        e = np.exp(-(k * k - 1) * np.pi ** 2 * ul[None, :] / 2)
         sn, cs = np.sin(k * np.pi * wl[None, :]), np.cos(k * np.pi * wl[None, :])
-        g[large] = np.pi * np.sum(k * e * sn, axis=0)
-        gw[large] = np.pi * np.sum(k * e * k * np.pi * cs, axis=0)
-        gu[large] = np.pi * np.sum(k * e * sn * (-k * k * np.pi ** 2 / 2), axis=0)
-    return g, gu, gw
+        s0 = np.sum(k * e * sn, axis=0)
+        logg[large] = np.log(np.pi) - np.pi ** 2 * ul / 2 + np.log(s0)
+        rw[large] = np.sum(k * e * k * np.pi * cs, axis=0) / s0
+        ru[large] = np.sum(k * e * sn * (-k * k * np.pi ** 2 / 2), axis=0) / s0
+    return logg, ru, rw
 
 
-def wfpt_lower(t, v, a, w, s=1.0):
-    """Density of hitting the lower barrier at decision time t (0 for t <= 0).
+def wfpt_lower_log(t, v, a, w, s=1.0):
+    """log density of hitting the lower barrier at decision time t (-inf for t <= 0).
     Noise s enters as drift v/s and separation a/s at unit noise."""
     t, v, a, w, s = np.broadcast_arrays(*(np.asarray(x, np.float64) for x in (t, v, a, w, s)))
     vs, as_ = v / s, a / s
-    out = np.zeros(t.shape)
+    out = np.full(t.shape, -np.inf)
     pos = t > 0
     if np.any(pos):
         u = t[pos] / as_[pos] ** 2
-        g, _, _ = _g_and_derivs(u, w[pos])
-        out[pos] = np.exp(-vs[pos] * as_[pos] * w[pos] - vs[pos] ** 2 * t[pos] / 2) * g / as_[pos] ** 2
+        logg, _, _ = _g_and_derivs(u, w[pos])
+        out[pos] = -vs[pos] * as_[pos] * w[pos] - vs[pos] ** 2 * t[pos] / 2 + logg - 2 * np.log(as_[pos])
     return out
+
+
+def wfpt_lower(t, v, a, w, s=1.0):
+    """Density of hitting the lower barrier at decision time t (0 for t <= 0)."""
+    return np.exp(wfpt_lower_log(t, v, a, w, s))
 
 
 def ddm_loglik(rt, choice, v, a, z, t, s=1.0):
@@ -89,11 +99,9 @@ def ddm_loglik(rt, choice, v, a, z, t, s=1.0):
     (bounds +-a, start -a + 2 z a, choice +1 upper / -1 lower, non-decision t)."""
     rt, choice = np.asarray(rt, np.float64), np.asarray(choice)
     T = rt - t
-    lower = wfpt_lower(T, v, 2 * a, z, s)
-    upper = wfpt_lower(T, -np.asarray(v), 2 * a, 1 - np.asarray(z), s)
-    dens = np.where(choice > 0, upper, lower)
-    with np.errstate(divide="ignore"):
-        return np.log(dens)
+    lower = wfpt_lower_log(T, v, 2 * a, z, s)
+    upper = wfpt_lower_log(T, -np.asarray(v), 2 * a, 1 - np.asarray(z), s)
+    return np.where(choice > 0, upper, lower)
 
 
 def prob_lower(v, a, w, s=1.0):
@@ -116,12 +124,12 @@ def ddm_loglik_grad(rt, choice, v, a, z, t):
     vv = np.where(up, -v, v)        # upper barrier: v -> -v, w -> 1 - w
     ww = np.where(up, 1 - z, z)
     u = np.maximum(T, 1e-300) / A ** 2
-    g, gu, gw = _g_and_derivs(u, ww)
+    _, ru, rw = _g_and_derivs(u, ww)
     # log f = -2 log A - vv A ww - vv^2 T / 2 + log g(T / A^2, ww)
     d_vv = -A * ww - vv * T
-    d_A = -2 / A - vv * ww + (gu / g) * (-2 * T / A ** 3)
-    d_ww = -vv * A + gw / g
-    d_T = -vv ** 2 / 2 + (gu / g) / A ** 2
+    d_A = -2 / A - vv * ww + ru * (-2 * T / A ** 3)
+    d_ww = -vv * A + rw
+    d_T = -vv ** 2 / 2 + ru / A ** 2
     sgn = np.where(up, -1.0, 1.0)
     grad = np.stack([sgn * d_vv, 2 * d_A, sgn * d_ww, -d_T], axis=-1)
     grad[T <= 0] = np.nan

@@ -78,6 +78,7 @@ _SIGNATURES: dict[str, tuple] = {
                             C.c_double, _P, _P]),
     "ssm_set_summary": (_I, [_P, _P, _I64, _P, _P, _I, C.c_double, _P, _P, _P, _I, _P, _I, _P, _P]),
     "ssm_kde_records": (_I, [_P, _I, _I64, _I, _P, _P, _P, _P, _I64, _I64, _F, _U64, _P, _P]),
+    "ssm_ddm_nf_loglik": (_I, [_P, _P, _P, _P, _P, _P, _P, _I64, _I, C.c_double, _P, _P, _P]),
     "ssm_mlp_pack": (_I, [_P, _P, _P]),
     "ssm_mlp_forward": (_I, [_P, _P, _I64, _I, _P, _P, _P, _P, _I, _I, _P, _P]),
     "ssm_mlp_train_grad": (_I, [_P, _P, _I64, _I, _P, _P, _I, _F, _P, _P, _P, _I, _P, _P]),

@@ -350,8 +350,10 @@ class BatchedKdePipeline:
         if bool(generator_config.get("estimator", {}).get("displace_t", False)):
             raise ValueError("displace_t is supported by the per-set pipeline; the batched pipeline uses unshifted rts")
 
-    def run_batch(self, theta: dict, seed: int) -> dict:
-        """One device pass over the parameter sets in ``theta`` (dict of arrays)."""
+    def run_batch(self, theta: dict, seed: int, on_device: bool = False) -> dict:
+        """One device pass over the parameter sets in ``theta`` (dict of arrays).
+        With ``on_device`` the result stays in device memory: ``records``
+        [K * n, P + 3] (theta..., rt, choice, loglik) and the summary tensors."""
         sc = self.generator_config["simulator"]
         tc = _training_cfg(self.generator_config)
         N, max_t, dt = int(sc["n_samples"]), float(sc["max_t"]), float(sc["delta_t"])
@@ -406,6 +408,10 @@ class BatchedKdePipeline:
         _lib.check(L.ssm_kde_records(D.ptr(th_t), P, K, C, D.ptr(cvals), D.ptr(qoff_t), D.ptr(q_rt),
                                      D.ptr(ll), n_down, n, float(tc["negative_rt_log_likelihood"]),
                                      _lib.U64_cast(seed + 2), D.ptr(rows), D.stream_ptr()))
+        if on_device:
+            return {"records": rows.reshape(K * n, P + 3), "theta": th_t, "choice_counts": counts.reshape(K, C),
+                    "nogo_counts": nogo, "omission_counts": omit, "binned_128": h128.reshape(K, 128, C),
+                    "binned_256": h256.reshape(K, 256, C)}
         rows = rows.reshape(K * n, P + 3).cpu().numpy()
         cnt = counts.reshape(K, C).cpu().numpy().astype(np.float64)
         cp = cnt / N
@@ -420,15 +426,17 @@ class BatchedKdePipeline:
                 "binned_128": h128.reshape(K, 128, C).cpu().numpy(),
                 "binned_256": h256.reshape(K, 256, C).cpu().numpy(), "theta": th}
 
-    def generate(self, n_parameter_sets: int, seed: int = 0) -> dict:
+    def generate(self, n_parameter_sets: int, seed: int = 0, on_device: bool = False) -> dict:
         rng = np.random.default_rng(seed)
         parts = []
         done = 0
         while done < n_parameter_sets:
             b = min(self.batch_size, n_parameter_sets - done)
             theta = self.sampler.sample(n_samples=b, rng=rng)
-            parts.append(self.run_batch(theta, seed=int(rng.integers(0, 2**62))))
+            parts.append(self.run_batch(theta, seed=int(rng.integers(0, 2**62)), on_device=on_device))
             done += b
+        if on_device:
+            return {k: torch.cat([p[k] for p in parts]) for k in parts[0]}
         return {k: np.concatenate([p[k] for p in parts]).astype(np.float32) for k in parts[0]}
 
 

@@ -1,0 +1,152 @@
+"""Train the likelihood surrogate on device-generated records and judge it
+against simulation + KDE.
+
+    python -m ssms_b200.surrogate_train --model angle --train-sets 100000 \\
+        --n-samples 100000 --epochs 20 --out angle_surrogate.pt --report report.json
+
+Records come from ``BatchedKdePipeline`` (the reference's LAN-KDE generator
+config: 1000 rows per parameter set, mixture 0.8 KDE resamples / 0.1 uniform
+rts / 0.1 negative rts) and never leave the device.  The judge draws fresh
+parameter sets, simulates ``n_samples`` trajectories for each, fits the LogKDE
+and evaluates it at uniform (rt, choice) queries; the error is the mean
+absolute difference of log-likelihoods with both sides raised to the
+surrogate's label lower bound.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import time
+
+import numpy as np
+import torch
+
+from .config import model_config
+from .dataset_generators import BatchedKdePipeline, get_lan_kde_config
+from .surrogate import DIN, MlpSurrogate, kde_loglik
+
+
+def make_records(model: str, n_sets: int, *, n_samples: int, seed: int, n_per_set: int = 1000,
+                 batch_size: int = 4096) -> torch.Tensor:
+    """[n_sets * n_per_set, 8] float32 training records on the device."""
+    cfg = get_lan_kde_config(model)
+    cfg["simulator"]["n_samples"] = int(n_samples)
+    cfg["training"]["n_samples_per_param"] = int(n_per_set)
+    pipe = BatchedKdePipeline(cfg, model_config[model], batch_size=batch_size)
+    return pipe.generate(n_sets, seed=seed, on_device=True)["records"]
+
+
+def uniform_queries(model: str, n_theta: int, n_per_theta: int, *, seed: int, rt_max: float = 20.0):
+    """theta [n_theta, 5] uniform in the model's box (as float32) and query rows
+    x [n_theta * n_per_theta, 7] with rt ~ U(0, rt_max), choice uniform."""
+    cfg = model_config[model]
+    lo, hi = (np.asarray(b, np.float64) for b in cfg["param_bounds"])
+    rng = np.random.default_rng(seed)
+    th = rng.uniform(lo, hi, (n_theta, lo.size)).astype(np.float32)
+    rt = rng.uniform(0.0, rt_max, (n_theta, n_per_theta)).astype(np.float32)
+    ch = rng.choice(np.asarray(cfg["choices"], np.float32), (n_theta, n_per_theta))
+    x = np.concatenate([np.repeat(th, n_per_theta, 0), rt.reshape(-1, 1), ch.reshape(-1, 1)], 1)
+    return th, np.ascontiguousarray(x, np.float32)
+
+
+def judge(net: MlpSurrogate, model: str, x: np.ndarray, *, n_samples: int, seed: int) -> dict:
+    """Surrogate vs simulation + KDE on query rows x (rows sharing theta share one simulation)."""
+    ref = kde_loglik(model, x[:, :DIN - 2], x[:, DIN - 2], x[:, DIN - 1], n_samples=n_samples, seed=seed)
+    # a second, independent simulation + KDE: the judge's own run-to-run noise
+    ref2 = kde_loglik(model, x[:, :DIN - 2], x[:, DIN - 2], x[:, DIN - 1], n_samples=n_samples, seed=seed + 1)
+    pred = net.forward(torch.from_numpy(x)).double().cpu().numpy()
+    lb = net.label_lower_bound if net.label_lower_bound is not None else -np.inf
+    r, r2, p = np.maximum(ref, lb), np.maximum(ref2, lb), np.maximum(pred, lb)
+    err = np.abs(p - r)
+    err2 = np.abs(r2 - r)
+    live = r > lb  # queries where the reference density is above the floor
+    return {"mae": float(err.mean()), "mae_above_floor": float(err[live].mean()) if live.any() else 0.0,
+            "kde_vs_kde_mae": float(err2.mean()),
+            "kde_vs_kde_mae_above_floor": float(err2[live].mean()) if live.any() else 0.0,
+            "frac_above_floor": float(live.mean()), "max_abs_err": float(err.max()), "n": int(x.shape[0])}
+
+
+def time_surrogate(net: MlpSurrogate, x: np.ndarray, *, want_dx: bool, reps: int = 20) -> float:
+    """Device-resident queries/s of the forward (or forward + input gradient) kernel."""
+    xd = torch.from_numpy(x).cuda()
+    out = torch.empty(xd.shape[0], device="cuda")
+    dx = torch.empty(xd.shape[0], DIN, device="cuda") if want_dx else None
+    for _ in range(3):
+        net.forward(xd, want_dx=want_dx, out=out, dx=dx)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(reps):
+        net.forward(xd, want_dx=want_dx, out=out, dx=dx)
+    e1.record()
+    torch.cuda.synchronize()
+    return xd.shape[0] * reps / (e0.elapsed_time(e1) * 1e-3)
+
+
+def time_sim_kde(model: str, x: np.ndarray, *, n_samples: int, seed: int) -> float:
+    """Queries/s of the simulation + KDE path on the same query rows, all
+    theta in one batch (simulate, fit, evaluate)."""
+    kde_loglik(model, x[:, :DIN - 2], x[:, DIN - 2], x[:, DIN - 1], n_samples=n_samples, seed=seed)  # warm
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    kde_loglik(model, x[:, :DIN - 2], x[:, DIN - 2], x[:, DIN - 1], n_samples=n_samples, seed=seed + 1)
+    torch.cuda.synchronize()
+    return x.shape[0] / (time.perf_counter() - t0)
+
+
+def main(argv=None) -> dict:
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--model", default="angle")
+    ap.add_argument("--train-sets", type=int, default=100_000)
+    ap.add_argument("--n-samples", type=int, default=100_000)
+    ap.add_argument("--epochs", type=int, default=20)
+    ap.add_argument("--batch", type=int, default=8192)
+    ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--lr-decay", type=float, default=1.0)
+    ap.add_argument("--loss", default="huber")
+    ap.add_argument("--judge-sets", type=int, default=1000)
+    ap.add_argument("--judge-per-set", type=int, default=1000)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--out", default=None)
+    ap.add_argument("--report", default=None)
+    a = ap.parse_args(argv)
+
+    rep: dict = {"model": a.model, "train_sets": a.train_sets, "n_samples": a.n_samples, "epochs": a.epochs,
+                 "batch": a.batch, "lr": a.lr, "loss": a.loss}
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    rec = make_records(a.model, a.train_sets, n_samples=a.n_samples, seed=a.seed)
+    torch.cuda.synchronize()
+    rep["records"] = int(rec.shape[0])
+    rep["datagen_s"] = time.perf_counter() - t0
+    hold = make_records(a.model, max(a.train_sets // 50, 64), n_samples=a.n_samples, seed=a.seed + 7)
+
+    net = MlpSurrogate(a.model, seed=a.seed, loss=a.loss)
+    t0 = time.perf_counter()
+    hist = net.fit(rec, epochs=a.epochs, batch_size=a.batch, lr=a.lr, lr_decay=a.lr_decay, seed=a.seed)
+    torch.cuda.synchronize()
+    rep["train_s"] = time.perf_counter() - t0
+    rep["loss_history"] = hist
+    rep["train_mae"] = net.mae(rec[: min(rec.shape[0], 2_000_000)])
+    rep["holdout_mae"] = net.mae(hold)
+    del rec
+
+    _, xq = uniform_queries(a.model, a.judge_sets, a.judge_per_set, seed=a.seed + 11)
+    rep["judge_uniform"] = judge(net, a.model, xq, n_samples=a.n_samples, seed=a.seed + 13)
+    rep["surrogate_evals_per_s"] = time_surrogate(net, xq, want_dx=False)
+    rep["surrogate_grad_evals_per_s"] = time_surrogate(net, xq, want_dx=True)
+    rep["sim_kde_evals_per_s"] = time_sim_kde(a.model, xq, n_samples=a.n_samples, seed=a.seed + 17)
+    rep["speedup_vs_sim_kde"] = rep["surrogate_evals_per_s"] / rep["sim_kde_evals_per_s"]
+    net.check()
+    if a.out:
+        net.save(a.out)
+    if a.report:
+        with open(a.report, "w") as f:
+            json.dump(rep, f, indent=1)
+    print(json.dumps(rep))
+    return rep
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,119 @@
+"""The trained surrogate: its error against simulation + KDE and against the
+analytic DDM density, its theta-gradient against finite differences and the
+analytic gradient, and what it gains over simulation + KDE.
+
+A network is trained once per module on device-generated records -- the full
+training-data configuration: 100000 ddm_angle parameter sets x 100000
+trajectories, 1000 records each, 30 epochs -- by the device kernels; this
+takes under a minute on one B200."""
+
+import numpy as np
+import pytest
+import torch
+
+import nf_oracle as NO
+from ssms_b200 import surrogate as S
+from ssms_b200 import surrogate_train as T
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def trained(cuda):
+    rec = T.make_records("angle", 100_000, n_samples=100_000, seed=1)
+    net = S.MlpSurrogate("angle", seed=0)
+    net.fit(rec, epochs=30, batch_size=8192, lr=1e-3, lr_decay=0.9, seed=0)
+    del rec
+    hold = T.make_records("angle", 400, n_samples=100_000, seed=2)
+    return net, hold
+
+
+def _slices():
+    """theta = 0 (constant bound a) slices over a grid of (v, a, z, t), rts on [0.01, 20], both choices"""
+    rows = []
+    for v in (-2.0, -1.0, 0.0, 1.0, 2.0):
+        for a in (0.6, 1.0, 1.6, 2.4):
+            for z in (0.3, 0.5, 0.7):
+                for t in (0.2, 1.0):
+                    rt = np.linspace(0.01, 20, 200)
+                    for c in (-1.0, 1.0):
+                        rows.append(np.stack([np.full_like(rt, v), np.full_like(rt, a), np.full_like(rt, z),
+                                              np.full_like(rt, t), np.zeros_like(rt), rt, np.full_like(rt, c)], 1))
+    return np.concatenate(rows).astype(np.float32)
+
+
+def test_error_against_simulation_kde(trained):
+    net, hold = trained
+    assert net.mae(hold) < 0.05           # held-out records, labels clipped at log(1e-7)
+    _, xq = T.uniform_queries("angle", 200, 1000, seed=5)
+    j = T.judge(net, "angle", xq, n_samples=100_000, seed=7)
+    # uniform queries: within the judge's own run-to-run noise (two independent
+    # simulation + KDE runs differ by kde_vs_kde_mae)
+    assert j["mae"] < 1.2 * j["kde_vs_kde_mae"], j
+
+
+def test_gain_over_simulation_kde(trained):
+    """Against the exact DDM density (theta = 0 slices) the surrogate is as
+    accurate as simulation + KDE with 100000 trajectories per theta, and more
+    than 100x faster per log-likelihood evaluation."""
+    net, _ = trained
+    x = _slices()
+    lb = net.label_lower_bound
+    exact = NO.ddm_loglik(x[:, 5].astype(np.float64), x[:, 6], x[:, 0].astype(np.float64),
+                          x[:, 1].astype(np.float64), x[:, 2].astype(np.float64), x[:, 3].astype(np.float64))
+    clip = lambda q: np.maximum(np.nan_to_num(q, neginf=-1e9), lb)  # noqa: E731
+    sur = net.forward(torch.from_numpy(x)).double().cpu().numpy()
+    kde = S.kde_loglik("angle", x[:, :5], x[:, 5], x[:, 6], n_samples=100_000, seed=3)
+    e_sur = np.abs(clip(sur) - clip(exact)).mean()
+    e_kde = np.abs(clip(kde) - clip(exact)).mean()
+    assert e_sur < 1.25 * e_kde, (e_sur, e_kde)
+    _, xq = T.uniform_queries("angle", 200, 1000, seed=9)
+    fast = T.time_surrogate(net, xq, want_dx=False, reps=10)
+    slow = T.time_sim_kde("angle", xq, n_samples=100_000, seed=4)
+    assert fast > 100 * slow, (fast, slow)
+
+
+def test_theta_gradient_against_analytic_gradient(trained):
+    net, _ = trained
+    x = _slices()
+    exact = NO.ddm_loglik(x[:, 5].astype(np.float64), x[:, 6], x[:, 0].astype(np.float64),
+                          x[:, 1].astype(np.float64), x[:, 2].astype(np.float64), x[:, 3].astype(np.float64))
+    g = NO.ddm_loglik_grad(x[:, 5].astype(np.float64), x[:, 6], x[:, 0].astype(np.float64),
+                           x[:, 1].astype(np.float64), x[:, 2].astype(np.float64), x[:, 3].astype(np.float64))
+    th = torch.tensor(x[:, :5], device="cuda", requires_grad=True)
+    ll = net.loglik(th, torch.tensor(x[:, 5], device="cuda"), torch.tensor(x[:, 6], device="cuda"))
+    ll.sum().backward()
+    d = th.grad.double().cpu().numpy()
+    core = np.isfinite(exact) & (exact > -8)
+    for j in range(3):  # v, a, z
+        a1, b1 = d[core, j], g[core, j]
+        cos = a1 @ b1 / np.linalg.norm(a1) / np.linalg.norm(b1)
+        assert cos > 0.9, ("vaz"[j], cos)
+
+
+def test_theta_gradient_against_finite_differences(trained):
+    """d out / d theta from the backward kernel against a least-squares slope
+    through six symmetric finite differences (steps of 1-3 % of each
+    parameter's range), which averages out the bf16 quantisation of the
+    forward pass."""
+    net, _ = trained
+    rng = np.random.default_rng(3)
+    th, xq = T.uniform_queries("angle", 500, 4, seed=13)
+    xq[:, 5] = xq[:, 3] + rng.uniform(0.2, 3.0, xq.shape[0])  # rts in the bulk after t
+    _, dx = net.forward(torch.from_numpy(xq), want_dx=True)
+    dx = dx.double().cpu().numpy()
+    f = lambda x: net.forward(torch.from_numpy(x)).double().cpu().numpy()  # noqa: E731
+    f0 = f(xq)
+    lo, hi = (np.asarray(b, np.float64) for b in S._model_config["angle"]["param_bounds"])
+    for j in range(5):
+        num = np.zeros(xq.shape[0])
+        den = np.zeros(xq.shape[0])
+        for m in (-3, -2, -1, 1, 2, 3):
+            xs = xq.copy()
+            xs[:, j] += m * 0.01 * (hi[j] - lo[j])
+            step = xs[:, j].astype(np.float64) - xq[:, j]
+            num += step * (f(xs) - f0)
+            den += step * step
+        fd = num / den
+        rel = np.linalg.norm(dx[:, j] - fd) / np.linalg.norm(fd)
+        assert rel < 0.15, (j, rel)

@@ -19,7 +19,8 @@ def test_density_integrates_to_choice_probability():
 def test_small_and_large_time_series_agree():
     u = np.linspace(0.05, 3.0, 50)
     for w in (0.1, 0.5, 0.9):
-        g_s, _, _ = NF._g_and_derivs(u, w, eps=1e-300, extra=40)  # forces many small-time terms
+        logg, _, _ = NF._g_and_derivs(u, w, eps=1e-300, extra=40)  # forces many small-time terms
+        g_s = np.exp(logg)
         # evaluate the large-time series directly for comparison
         k = np.arange(1, 200)[:, None]
         g_l = np.pi * np.sum(k * np.exp(-k * k * np.pi ** 2 * u[None, :] / 2) * np.sin(k * np.pi * w), axis=0)
