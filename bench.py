@@ -12,6 +12,10 @@ replayed from a CUDA graph.  Metric: trajectories/s (whole job, all ranks).
 sources into oracle/_ref; the C restatement in oracle/ if that build is absent)
 on every host core with a process pool, on a bounded sample of the same
 workload, and prints the same JSON line with "impl": "reference".
+
+On one GPU the line also carries a "surrogate" object: the likelihood
+surrogate trained in the same run on device-generated records and timed
+against simulation + KDE (see run_surrogate).
 """
 
 from __future__ import annotations
@@ -311,6 +315,135 @@ def run_ours(args, rank, world, local_rank):
     return line, theta, n_samples
 
 
+SUR_MODEL = "angle"
+SUR_QUERIES_THETA, SUR_QUERIES_PER_THETA = 1000, 1000
+TANH_PER_EVAL = 100 + 100 + 120     # MUFU.TANH per forward evaluation
+MUFU_PER_SM_CLK = 16
+
+
+def run_surrogate(args, clocks: dict) -> dict:
+    """The learned part, end to end on this GPU: training records from the
+    batched simulation + KDE pipeline (100000 ddm_angle parameter sets x
+    100000 trajectories, 1000 records each), Adam training on the tensor-core
+    kernels, then log-likelihood evaluations per second of the surrogate
+    (forward, and forward + theta-gradient) and of simulation + KDE on the same
+    10^6 uniform (theta, rt in [0, 20], choice) queries, with the surrogate's
+    error against simulation + KDE and against the analytic DDM density."""
+    import torch
+
+    from ssms_b200 import nf
+    from ssms_b200 import surrogate as S
+    from ssms_b200 import surrogate_train as T
+
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    rec = T.make_records(SUR_MODEL, args.surrogate_sets, n_samples=100_000, seed=SEED)
+    torch.cuda.synchronize()
+    datagen_s = time.perf_counter() - t0
+    n_rec = int(rec.shape[0])
+    hold = T.make_records(SUR_MODEL, 1000, n_samples=100_000, seed=SEED + 1)
+    net = S.MlpSurrogate(SUR_MODEL, seed=0)
+    t0 = time.perf_counter()
+    hist = net.fit(rec, epochs=args.surrogate_epochs, batch_size=8192, lr=1e-3, lr_decay=0.9, seed=0)
+    torch.cuda.synchronize()
+    train_s = time.perf_counter() - t0
+    del rec
+    mae_hold = net.mae(hold)
+
+    # 10^6 uniform queries: 1000 theta x 1000 (rt, choice)
+    _, xq = T.uniform_queries(SUR_MODEL, SUR_QUERIES_THETA, SUR_QUERIES_PER_THETA, seed=SEED + 2)
+    clk = ClockSampler(0).__enter__()  # sampled over the whole evaluation (timed launches are short)
+    judge = T.judge(net, SUR_MODEL, xq, n_samples=100_000, seed=SEED + 3)
+    n = xq.shape[0]
+    xd = torch.from_numpy(xq).cuda()
+    out = torch.empty(n, device="cuda")
+    dx = torch.empty(n, 7, device="cuda")
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+
+    def timed(want_dx):
+        for _ in range(args.warmup):
+            net.forward(xd, want_dx=want_dx, out=out, dx=dx if want_dx else None)
+        ms = []
+        for _ in range(args.steps):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            net.forward(xd, want_dx=want_dx, out=out, dx=dx if want_dx else None)
+            e1.record()
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        return n * len(ms) / (sum(ms) / 1e3), sum(ms) / len(ms)
+
+    fwd, fwd_ms = timed(False)
+    grad, grad_ms = timed(True)
+    # end to end through the public call: pinned host queries in, log-likelihoods out
+    xh = torch.from_numpy(xq).pin_memory()
+    oh = torch.empty(n, dtype=torch.float32).pin_memory()
+    e2e = []
+    for i in range(args.warmup + args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        xd.copy_(xh, non_blocking=True)
+        net.forward(xd, out=out)
+        oh.copy_(out, non_blocking=True)
+        torch.cuda.synchronize()
+        if i >= args.warmup:
+            e2e.append(time.perf_counter() - t0)
+    sim_kde = T.time_sim_kde(SUR_MODEL, xq, n_samples=100_000, seed=SEED + 4)
+    clk.__exit__(None, None, None)
+
+    # exact yardstick: theta = 0 (constant bound) slices against the float64 Navarro-Fuss density
+    rows = []
+    for v in (-2.0, -1.0, 0.0, 1.0, 2.0):
+        for a in (0.6, 1.0, 1.6, 2.4):
+            for z in (0.3, 0.5, 0.7):
+                for t in (0.2, 1.0):
+                    rt = np.linspace(0.01, 20, 200)
+                    for c in (-1.0, 1.0):
+                        rows.append(np.stack([np.full_like(rt, v), np.full_like(rt, a), np.full_like(rt, z),
+                                              np.full_like(rt, t), np.zeros_like(rt), rt,
+                                              np.full_like(rt, c)], 1))
+    xs = np.concatenate(rows).astype(np.float32)
+    ex, gex = nf.ddm_loglik(xs[:, 5], xs[:, 6], xs[:, 0], xs[:, 1], xs[:, 2], xs[:, 3], grad=True)
+    lb = net.label_lower_bound
+    clip = lambda q: np.maximum(np.nan_to_num(q, neginf=-1e9), lb)  # noqa: E731
+    so, sdx = net.forward(torch.from_numpy(xs), want_dx=True)
+    so, sdx = so.double().cpu().numpy(), sdx.double().cpu().numpy()
+    kd = S.kde_loglik(SUR_MODEL, xs[:, :5], xs[:, 5], xs[:, 6], n_samples=100_000, seed=SEED + 5)
+    core = np.isfinite(ex) & (ex > -8)
+    cos = {k: float(sdx[core, j] @ gex[core, j] / np.linalg.norm(sdx[core, j]) / np.linalg.norm(gex[core, j]))
+           for j, k in enumerate("vazt")}
+    net.check()
+    f_max = (clocks.get("sm_max_mhz") or 1965.0) * 1e6
+    peak = N_SM * MUFU_PER_SM_CLK * f_max / TANH_PER_EVAL
+    return {
+        "metric": "log-likelihood evaluations/s", "unit": "evals/s",
+        "value": fwd, "grad_value": grad, "sim_kde_value": sim_kde, "speedup_vs_sim_kde": fwd / sim_kde,
+        "queries": n, "ms_per_forward": fwd_ms, "ms_per_forward_grad": grad_ms,
+        "mae_vs_sim_kde_holdout_records": mae_hold,
+        "mae_vs_sim_kde_uniform_queries": judge["mae"],
+        "sim_kde_vs_sim_kde_mae_uniform_queries": judge["kde_vs_kde_mae"],
+        "mae_vs_exact_theta0": float(np.abs(clip(so) - clip(ex)).mean()),
+        "sim_kde_mae_vs_exact_theta0": float(np.abs(clip(kd) - clip(ex)).mean()),
+        "theta_grad_cosine_vs_exact_theta0": cos,
+        "error_scale": f"log-likelihoods raised to {lb:.4f} = log(1e-7) on both sides",
+        "roofline": {"bound": "xu", "achieved": fwd * TANH_PER_EVAL / 1e9, "peak": peak * TANH_PER_EVAL / 1e9,
+                     "unit": "G tanh/s", "frac": fwd / peak,
+                     "peak_basis": f"{N_SM} SMs x {MUFU_PER_SM_CLK} MUFU/clk x {f_max/1e6:.0f} MHz"},
+        "e2e": {"value": n * len(e2e) / sum(e2e), "unit": "evals/s", "h2d_bytes_per_step": n * 7 * 4,
+                "d2h_bytes_per_step": n * 4},
+        "gpu_launches": 2 * args.steps,
+        "clocks": clk.summary(),
+        "train": {"records": n_rec, "parameter_sets": args.surrogate_sets, "trajectories_per_set": 100_000,
+                  "datagen_s": datagen_s, "epochs": args.surrogate_epochs, "batch": 8192, "lr": 1e-3,
+                  "train_s": train_s, "final_epoch_loss": hist[-1], "loss": "huber"},
+        "config": {"model": "ddm_angle 7-100-100-120-1 tanh MLP, bf16 weights/activations, fp32 accumulate",
+                   "queries": f"{SUR_QUERIES_THETA} theta x {SUR_QUERIES_PER_THETA} (rt ~ U(0,20), choice +-1)",
+                   "sim_kde": "100000 trajectories per theta, LogKDE fit + eval, all theta in one batch",
+                   "l2": "flushed (256 MB write) between timed launches"},
+    }
+
+
 def run_reference(args):
     theta, n_samples = workload(SEED)
     pool = CpuPool()
@@ -346,6 +479,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-surrogate", action="store_true")
+    ap.add_argument("--surrogate-sets", type=int, default=100_000)
+    ap.add_argument("--surrogate-epochs", type=int, default=30)
     ap.add_argument("--n-theta", type=int, default=N_THETA,
                     help="parameter vectors per step (smaller values only for profiling captures)")
     args = ap.parse_args()
@@ -368,6 +504,8 @@ def main():
         torch.cuda.set_device(local_rank)
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     line, theta, n_samples = run_ours(args, rank, world, local_rank)
+    if rank == 0 and world == 1 and not args.no_surrogate:
+        line["surrogate"] = run_surrogate(args, line["clocks"])
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_record(theta, n_samples)
     if world > 1:
