@@ -8,9 +8,9 @@ ssms/dataset_generators/lan_mlp.py:66-133), so this oracle restates the model
 the device kernels define:
 
     x~  = (x - c) * s                 split x~ = hi + lo, both rounded to bf16
-    h1  = tanh(bf(W1) (hi + lo) + b1)
-    h2  = tanh(bf(W2) bf(h1) + b2)
-    h3  = tanh(bf(W3) bf(h2) + b3)
+    h1  = bf(tanh(bf(W1) (hi + lo) + b1))
+    h2  = bf(tanh(bf(W2) h1 + b2))
+    h3  = tanh(bf(W3) h2 + b3)
     out = w4 . h3 + b4                (fp32 output layer)
 
 bf(.) is round-to-nearest-even to bfloat16.  The backward mirrors the kernels
@@ -115,6 +115,11 @@ def _q(x, quantize):
     return bf16(x) if quantize else np.asarray(x, np.float64)
 
 
+def _hidden(pre, quantize):
+    """tanh of a hidden layer, stored as a bf16 GEMM operand on the device"""
+    return bf16(np.tanh(pre)) if quantize else np.tanh(pre)
+
+
 def forward(p, x, norm_c, norm_s, *, quantize=True, want_dx=False):
     """out [n] (and dx [n, 7] = d out / d x) for inputs x [n, >=7]."""
     W1, b1, W2, b2, W3, b3, w4, b4 = unpack(p)
@@ -129,10 +134,8 @@ def forward(p, x, norm_c, norm_s, *, quantize=True, want_dx=False):
         xin = hi + lo
     else:
         xin = xt.astype(np.float64)
-    h1 = np.tanh(xin @ W1q.T + b1)
-    h1q = _q(h1, quantize)
-    h2 = np.tanh(h1q @ W2q.T + b2)
-    h2q = _q(h2, quantize)
+    h1q = _hidden(xin @ W1q.T + b1, quantize)
+    h2q = _hidden(h1q @ W2q.T + b2, quantize)
     h3 = np.tanh(h2q @ W3q.T + b3)
     out = h3 @ w4 + b4
     if not want_dx:
@@ -161,10 +164,8 @@ def train_grad(p, rec, norm_c, norm_s, *, loss="huber", inv_batch=None, quantize
         xin = hi + lo
     else:
         xin = xt.astype(np.float64)
-    h1 = np.tanh(xin @ W1q.T + b1)
-    h1q = _q(h1, quantize)
-    h2 = np.tanh(h1q @ W2q.T + b2)
-    h2q = _q(h2, quantize)
+    h1q = _hidden(xin @ W1q.T + b1, quantize)
+    h2q = _hidden(h1q @ W2q.T + b2, quantize)
     h3 = np.tanh(h2q @ W3q.T + b3)
     h3q = _q(h3, quantize)
     out = h3 @ w4 + b4

@@ -230,6 +230,8 @@ __device__ __forceinline__ float tanh_fast(float x) {
     return y;
 }
 
+constexpr uint32_t BF16_ONE = 0x3F80u;
+
 __device__ __forceinline__ uint32_t pack2(float lo, float hi) {
     __nv_bfloat162 h = __floats2bfloat162_rn(lo, hi);
     return *reinterpret_cast<uint32_t *>(&h);
@@ -261,28 +263,48 @@ __device__ __forceinline__ void stage_x(uint8_t *X, int r, const float *xr, bool
     st_row(X, 1, r, c1);
 }
 
-// acc (NC columns at ta) + bias -> tanh -> bf16 tile (ones column set to 1);
-// optionally also stash the packed bf16 pairs in TMEM at ts.
-template <int NC, int ONES, bool STASH>
-__device__ __forceinline__ void epi_hidden(uint32_t ta, const float *bias, uint8_t *dst, int r, uint32_t ts) {
-#pragma unroll 1
-    for (int c = 0; c < NC / 16; ++c) {
-        float v[16];
-        tmem_ld16(ta + 16 * c, v);
-        uint32_t p[8];
+// Hidden layers 1 and 2: tanh(acc + bias) in fp32 (tanh.approx.f32), rounded
+// to bf16 pairs -> bf16 tile.  Columns from H (the real width) on are padding:
+// written as zeros without a tanh, except the ones column.  Optionally the
+// packed pairs are also stashed in TMEM at ts.  (tanh.approx.bf16x2 was
+// measured: it costs the XU pipe as much as two fp32 tanh, so it buys nothing.)
+template <bool EDGE, int H, int ONES, bool STASH>
+__device__ __forceinline__ void hidden_chunk(int c, uint32_t ta, const float4 *b4v, uint8_t *dst, int r,
+                                             uint32_t ts) {
+    float v[16];
+    tmem_ld16(ta + 16 * c, v);
+    uint32_t p[8];
 #pragma unroll
-        for (int j = 0; j < 8; ++j) {
-            const int col = 16 * c + 2 * j;
-            float a = tanh_fast(v[2 * j] + bias[col]);
-            float b = tanh_fast(v[2 * j + 1] + bias[col + 1]);
-            if (col == ONES) a = 1.f;
-            if (col + 1 == ONES) b = 1.f;
-            p[j] = pack2(a, b);
+    for (int q = 0; q < 4; ++q) {
+        const int col = 16 * c + 4 * q;
+        if (EDGE && col >= H) {
+            p[2 * q] = p[2 * q + 1] = 0u;
+        } else {
+            const float4 b = b4v[col / 4];
+            p[2 * q] = pack2(tanh_fast(v[4 * q] + b.x), tanh_fast(v[4 * q + 1] + b.y));
+            p[2 * q + 1] = pack2(tanh_fast(v[4 * q + 2] + b.z), tanh_fast(v[4 * q + 3] + b.w));
         }
-        st_row(dst, 2 * c, r, make_uint4(p[0], p[1], p[2], p[3]));
-        st_row(dst, 2 * c + 1, r, make_uint4(p[4], p[5], p[6], p[7]));
-        if (STASH) tmem_st8(ts + 8 * c, p);
+        if (EDGE) {
+#pragma unroll
+            for (int e = 0; e < 4; ++e)
+                if (col + e == ONES) {
+                    uint32_t &w = p[2 * q + e / 2];
+                    w = (e & 1) ? ((w & 0x0000FFFFu) | (BF16_ONE << 16)) : ((w & 0xFFFF0000u) | BF16_ONE);
+                }
+        }
     }
+    st_row(dst, 2 * c, r, make_uint4(p[0], p[1], p[2], p[3]));
+    st_row(dst, 2 * c + 1, r, make_uint4(p[4], p[5], p[6], p[7]));
+    if (STASH) tmem_st8(ts + 8 * c, p);
+}
+
+template <int NC, int H, int ONES, bool STASH>
+__device__ __forceinline__ void epi_hidden(uint32_t ta, const float *bias, uint8_t *dst, int r, uint32_t ts) {
+    static_assert(H > NC - 16 && ONES >= NC - 16 && ONES < NC, "padding and ones column lie in the last chunk");
+    const float4 *b4v = reinterpret_cast<const float4 *>(bias);
+#pragma unroll 1
+    for (int c = 0; c < NC / 16 - 1; ++c) hidden_chunk<false, H, ONES, STASH>(c, ta, b4v, dst, r, ts);
+    hidden_chunk<true, H, ONES, STASH>(NC / 16 - 1, ta, b4v, dst, r, ts);
 }
 
 // G = D (TMEM, NC cols) * (1 - h^2) with h read from this row of H; G -> dst
@@ -330,29 +352,52 @@ __device__ __forceinline__ void epi_dtanh_stash(uint32_t ta, uint32_t ts, uint8_
 // Layer-3 epilogue: h3 = tanh(acc + b3) in fp32, out = b4 + h3 . w4 (fp32),
 // and per KIND: 0 nothing else, 1 G3 = w4 (1 - h3^2) -> dst (d out / d acc3),
 // 2 bf16 h3 with the ones column -> dst (training operand).
+template <int KIND, bool EDGE>
+__device__ __forceinline__ void out_chunk(int c, uint32_t ta, const float4 *b3v, const float4 *w4v, float &o,
+                                          uint8_t *dst, int r) {
+    float v[16];
+    tmem_ld16(ta + 16 * c, v);
+    uint32_t p[8];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int col = 16 * c + 4 * q;
+        float h[4] = {0.f, 0.f, 0.f, 0.f}, w[4] = {0.f, 0.f, 0.f, 0.f};
+        if (!EDGE || col < H3) {
+            const float4 b = b3v[col / 4], ww = w4v[col / 4];
+            h[0] = tanh_fast(v[4 * q] + b.x);
+            h[1] = tanh_fast(v[4 * q + 1] + b.y);
+            h[2] = tanh_fast(v[4 * q + 2] + b.z);
+            h[3] = tanh_fast(v[4 * q + 3] + b.w);
+            w[0] = ww.x; w[1] = ww.y; w[2] = ww.z; w[3] = ww.w;
+#pragma unroll
+            for (int e = 0; e < 4; ++e) o = fmaf(w[e], h[e], o);
+        }
+        if (KIND == 1) {
+            p[2 * q] = pack2(w[0] * (1.f - h[0] * h[0]), w[1] * (1.f - h[1] * h[1]));
+            p[2 * q + 1] = pack2(w[2] * (1.f - h[2] * h[2]), w[3] * (1.f - h[3] * h[3]));
+        }
+        if (KIND == 2) {
+            if (EDGE && col == ONES3) h[0] = 1.f;
+            p[2 * q] = pack2(h[0], h[1]);
+            p[2 * q + 1] = pack2(h[2], h[3]);
+        }
+    }
+    if (KIND != 0) {
+        st_row(dst, 2 * c, r, make_uint4(p[0], p[1], p[2], p[3]));
+        st_row(dst, 2 * c + 1, r, make_uint4(p[4], p[5], p[6], p[7]));
+    }
+}
+
 template <int KIND>
 __device__ __forceinline__ float epi_out(uint32_t ta, const float *b3, const float *w4, float b4, uint8_t *dst,
                                          int r) {
+    static_assert(H3 > N3 - 16 && ONES3 >= N3 - 16, "padding and ones column lie in the last chunk");
+    const float4 *b3v = reinterpret_cast<const float4 *>(b3);
+    const float4 *w4v = reinterpret_cast<const float4 *>(w4);
     float o = b4;
 #pragma unroll 1
-    for (int c = 0; c < N3 / 16; ++c) {
-        float v[16];
-        tmem_ld16(ta + 16 * c, v);
-        uint32_t p[8];
-#pragma unroll
-        for (int j = 0; j < 16; j += 2) {
-            const int col = 16 * c + j;
-            const float ha = tanh_fast(v[j] + b3[col]), hb = tanh_fast(v[j + 1] + b3[col + 1]);
-            o = fmaf(w4[col], ha, o);
-            o = fmaf(w4[col + 1], hb, o);
-            if (KIND == 1) p[j / 2] = pack2(w4[col] * (1.f - ha * ha), w4[col + 1] * (1.f - hb * hb));
-            if (KIND == 2) p[j / 2] = pack2(col == ONES3 ? 1.f : ha, col + 1 == ONES3 ? 1.f : hb);
-        }
-        if (KIND != 0) {
-            st_row(dst, 2 * c, r, make_uint4(p[0], p[1], p[2], p[3]));
-            st_row(dst, 2 * c + 1, r, make_uint4(p[4], p[5], p[6], p[7]));
-        }
-    }
+    for (int c = 0; c < N3 / 16 - 1; ++c) out_chunk<KIND, false>(c, ta, b3v, w4v, o, dst, r);
+    out_chunk<KIND, true>(N3 / 16 - 1, ta, b3v, w4v, o, dst, r);
     return o;
 }
 
@@ -449,7 +494,7 @@ k_mlp(const uint8_t *__restrict__ image, const float *__restrict__ x, int64_t n,
                 }
                 late |= !mbar_wait(mbar, phase); phase ^= 1;
                 tc_after();
-                epi_hidden<N1, ONES1, MODE == FWD_DX>(tw, b1, B0, r, tstash);
+                epi_hidden<N1, H1, ONES1, MODE == FWD_DX>(tw, b1, B0, r, tstash);
                 if (MODE == FWD_DX) tmem_wait_st();
                 tc_before();
                 fence_async_smem();
@@ -462,7 +507,7 @@ k_mlp(const uint8_t *__restrict__ image, const float *__restrict__ x, int64_t n,
                 }
                 late |= !mbar_wait(mbar, phase); phase ^= 1;
                 tc_after();
-                epi_hidden<N2, ONES1, false>(tw, b2, Hb, r, 0);
+                epi_hidden<N2, H2, ONES1, false>(tw, b2, Hb, r, 0);
                 tc_before();
                 fence_async_smem();
                 bar_sync(bid, 128);
@@ -537,7 +582,7 @@ k_mlp(const uint8_t *__restrict__ image, const float *__restrict__ x, int64_t n,
                 }
                 late |= !mbar_wait(mbar, phase); phase ^= 1;
                 tc_after();
-                epi_hidden<N1, ONES1, false>(tw, b1, H1t, r, 0);
+                epi_hidden<N1, H1, ONES1, false>(tw, b1, H1t, r, 0);
                 tc_before();
                 fence_async_smem();
                 bar_sync(bid, 128);
@@ -549,7 +594,7 @@ k_mlp(const uint8_t *__restrict__ image, const float *__restrict__ x, int64_t n,
                 }
                 late |= !mbar_wait(mbar, phase); phase ^= 1;
                 tc_after();
-                epi_hidden<N2, ONES1, false>(tw, b2, H2t, r, 0);
+                epi_hidden<N2, H2, ONES1, false>(tw, b2, H2t, r, 0);
                 tc_before();
                 fence_async_smem();
                 bar_sync(bid, 128);

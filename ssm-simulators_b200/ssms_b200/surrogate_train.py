@@ -110,7 +110,20 @@ def main(argv=None) -> dict:
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--out", default=None)
     ap.add_argument("--report", default=None)
+    ap.add_argument("--forward-only", type=int, default=0, metavar="N",
+                    help="skip training: time the forward and forward+gradient kernels of a freshly "
+                         "initialised network on N uniform queries (for profiling)")
     a = ap.parse_args(argv)
+    if a.forward_only:
+        net = MlpSurrogate(a.model, seed=a.seed)
+        per = 1000
+        _, xq = uniform_queries(a.model, max(a.forward_only // per, 1), per, seed=a.seed)
+        rep = {"queries": int(xq.shape[0]),
+               "forward_evals_per_s": time_surrogate(net, xq, want_dx=False, reps=3),
+               "forward_grad_evals_per_s": time_surrogate(net, xq, want_dx=True, reps=3)}
+        net.check()
+        print(json.dumps(rep))
+        return rep
 
     rep: dict = {"model": a.model, "train_sets": a.train_sets, "n_samples": a.n_samples, "epochs": a.epochs,
                  "batch": a.batch, "lr": a.lr, "loss": a.loss}

@@ -93,9 +93,10 @@ def test_theta_gradient_against_analytic_gradient(trained):
 
 def test_theta_gradient_against_finite_differences(trained):
     """d out / d theta from the backward kernel against a least-squares slope
-    through six symmetric finite differences (steps of 1-3 % of each
+    through six symmetric finite differences (steps of 0.5-1.5 % of each
     parameter's range), which averages out the bf16 quantisation of the
-    forward pass."""
+    forward pass; points where the network sits at its label floor (a kink)
+    are left out."""
     net, _ = trained
     rng = np.random.default_rng(3)
     th, xq = T.uniform_queries("angle", 500, 4, seed=13)
@@ -104,16 +105,18 @@ def test_theta_gradient_against_finite_differences(trained):
     dx = dx.double().cpu().numpy()
     f = lambda x: net.forward(torch.from_numpy(x)).double().cpu().numpy()  # noqa: E731
     f0 = f(xq)
+    keep = f0 > -10.0
     lo, hi = (np.asarray(b, np.float64) for b in S._model_config["angle"]["param_bounds"])
     for j in range(5):
         num = np.zeros(xq.shape[0])
         den = np.zeros(xq.shape[0])
         for m in (-3, -2, -1, 1, 2, 3):
             xs = xq.copy()
-            xs[:, j] += m * 0.01 * (hi[j] - lo[j])
+            xs[:, j] += m * 0.005 * (hi[j] - lo[j])
             step = xs[:, j].astype(np.float64) - xq[:, j]
             num += step * (f(xs) - f0)
             den += step * step
         fd = num / den
-        rel = np.linalg.norm(dx[:, j] - fd) / np.linalg.norm(fd)
+        rel = np.linalg.norm(dx[keep, j] - fd[keep]) / np.linalg.norm(fd[keep])
+        print("fd-slope", j, rel)
         assert rel < 0.15, (j, rel)
