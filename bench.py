@@ -128,9 +128,11 @@ class CpuPool:
                 for i in range(m)]
 
     def run(self, rows) -> tuple[int, float]:
-        shards = [rows[i::self.cores] for i in range(self.cores)]
+        """Rows are handed out one at a time, longest first, so no core idles
+        while another still holds a queue of rows."""
+        order = sorted(rows, key=lambda r: -r[5])
         t0 = time.perf_counter()
-        done = sum(self.pool.map(_cpu_worker, [(self.kind, s) for s in shards]))
+        done = sum(self.pool.imap_unordered(_cpu_worker, [(self.kind, [r]) for r in order], chunksize=1))
         return done, time.perf_counter() - t0
 
     def close(self):
@@ -204,12 +206,12 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------------ GPU side
-def _traffic_record():
-    p = ROOT / "profiles" / "ddm_angle_batched_traffic.json"
-    try:
-        return json.loads(p.read_text())
-    except (OSError, ValueError):
-        return None
+# DRAM bytes (read + write) of one k_single launch on the 4096-theta workload,
+# from one ncu capture of that launch (dram__bytes_read.sum 10,920,448 +
+# dram__bytes_write.sum 285,464,064).
+# The algorithmic output is 8 B per trajectory (338 MB); part of it is still in
+# L2 when the kernel ends, so the measured writes sit slightly below it.
+K_SINGLE_TRAFFIC_BYTES = 10_920_448 + 285_464_064
 
 
 def run_ours(args, rank, world, local_rank):
@@ -292,7 +294,7 @@ def run_ours(args, rank, world, local_rank):
     f_max = (clocks.get("sm_max_mhz") or 1965.0) * 1e6
     peak_steps = N_SM * LANES_PER_SM_CLK * f_max / INSTR_PER_STEP
     achieved_steps = steps_per_launch / (ms_per_step / 1e3)
-    traffic = _traffic_record()
+    traffic = K_SINGLE_TRAFFIC_BYTES if args.n_theta == N_THETA else None
     line = {
         "metric": METRIC, "value": value, "unit": "trajectories/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
@@ -303,7 +305,8 @@ def run_ours(args, rank, world, local_rank):
                    "l2": "flushed (256 MB write) between timed steps", "parallelism": f"replicas x{world}"},
         "roofline": {"bound": "issue", "achieved": achieved_steps / 1e9, "peak": peak_steps / 1e9,
                      "unit": "G accumulator-steps/s", "frac": achieved_steps / peak_steps,
-                     "traffic": None if traffic is None else traffic.get("bytes_per_launch"),
+                     "traffic": traffic, "traffic_unit": "DRAM bytes per launch (ncu)",
+                     "algorithmic_bytes": total * 8,
                      "peak_basis": f"{N_SM} SMs x {LANES_PER_SM_CLK} lanes/clk x {f_max/1e6:.0f} MHz / "
                                    f"{INSTR_PER_STEP:.0f} lane-instructions per accumulator-step",
                      "output_hbm_gbs": total * 8 / (ms_per_step / 1e3) / 1e9},
@@ -444,6 +447,150 @@ def run_surrogate(args, clocks: dict) -> dict:
     }
 
 
+# ------------------------------------------------------------------ other workloads
+# Multi-choice and heavy-tailed mix: 1024 uniform parameter vectors per model,
+# n_samples = 10000, dt = 1e-3, max_t = 20; and the plain DDM case (one
+# parameter vector, 100000 samples) that the reference runs on one core.
+MIX_THETA, MIX_SAMPLES = 1024, 10_000
+_V4 = {f"v{j}": (0.0, 2.5) for j in range(4)}
+MIX_BOUNDS = {
+    "lca_no_bias_4": {**_V4, "a": (1.0, 3.0), "z": (0.0, 0.5), "g": (-1.0, 1.0), "b": (-1.0, 1.0),
+                      "t": (0.0, 2.0)},
+    "race_no_bias_angle_4": {**_V4, "a": (1.0, 3.0), "z": (0.0, 0.5), "t": (0.0, 2.0), "theta": (0.0, 1.45)},
+    "levy": {"v": (-3.0, 3.0), "a": (0.3, 3.0), "z": (0.1, 0.9), "alpha": (1.0, 2.0), "t": (0.001, 2.0)},
+}
+MIX_CPU_ROWS_PER_CORE = {"lca_no_bias_4": 1, "race_no_bias_angle_4": 6, "levy": 6}
+PLAIN_DDM = {"v": 1.0, "a": 1.5, "z": 0.5, "t": 0.2}
+PLAIN_SAMPLES = 100_000
+
+
+def mix_workload(model: str, seed: int) -> dict:
+    rng = np.random.default_rng(seed)
+    return {k: rng.uniform(lo, hi, MIX_THETA).astype(np.float32) for k, (lo, hi) in MIX_BOUNDS[model].items()}
+
+
+def _constant_host(t, a):
+    return np.full_like(t, a) if isinstance(t, np.ndarray) else a
+
+
+_HOST_BOUNDS = {"constant": _constant_host, "angle": _angle_host}
+_REF_MODULE = {"ddm_flexbound": "ddm_models", "levy_flexbound": "levy_models", "race_model": "race_models",
+               "lca": "race_models"}
+
+
+def _cpu_sim_worker(job):
+    """Run the reference's compiled simulator on a list of single-parameter-set calls."""
+    sim_name, calls = job
+    sys.path.insert(0, str(Path(__file__).resolve().parent / "oracle" / "_ref"))
+    import importlib
+
+    fn = getattr(importlib.import_module("cssm." + _REF_MODULE[sim_name]), sim_name)
+    done = 0
+    for kw, bname, bparams, n, seed in calls:
+        fn(**kw, boundary_fun=_HOST_BOUNDS[bname], boundary_params=bparams, max_t=20.0, delta_t=0.001,
+           n_samples=int(n), n_trials=1, random_state=int(seed), return_option="minimal", smooth_unif=True)
+        done += int(n)
+    return done
+
+
+def _row_calls(prep: dict, rows: int, n: int, seed0: int) -> list:
+    calls = []
+    for k in range(rows):
+        kw = {key: np.ascontiguousarray(np.asarray(v)[k:k + 1]) for key, v in prep["theta"].items()
+              if np.ndim(v) >= 1}
+        bp = {key: np.ascontiguousarray(np.asarray(v)[k:k + 1])
+              for key, v in prep["boundary"]["boundary_params"].items()}
+        calls.append((kw, prep["boundary"]["boundary_fun"].__name__, bp, n, seed0 + k))
+    return calls
+
+
+def run_other_workloads(args) -> dict:
+    """The mix workload (lca_no_bias_4, race_no_bias_angle_4, levy) and the
+    plain DDM case: device throughput (inputs resident, one launch per step,
+    CUDA events, L2 flushed), end to end through Simulator.simulate (host
+    arrays in and out), and the reference's compiled simulators on every host
+    core over a bounded sample of the same parameter sets."""
+    import multiprocessing as mp
+
+    import torch
+
+    from ssms_b200 import Simulator
+    from ssms_b200.batch_models import SetBatch
+
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    cases = [(m, mix_workload(m, SEED + 100 + i), MIX_SAMPLES) for i, m in enumerate(MIX_BOUNDS)]
+    cases.append(("ddm", {k: np.float32(v) for k, v in PLAIN_DDM.items()}, PLAIN_SAMPLES))
+    res, cpu_jobs = {}, []
+    for i, (model, theta, n) in enumerate(cases):
+        sim = Simulator(model)
+        prep = sim.prepare(theta, n_samples=n, random_state=SEED + i)
+        name = prep["config"]["simulator"].__name__
+        sb = SetBatch(name, prep["theta"], prep["boundary"], n, max_t=20.0, delta_t=0.001)
+        o = sb.run(SEED, want_steps=True)
+        steps = int(o.steps.to(torch.int64).sum().item())
+        for w in range(args.warmup):
+            sb.run(SEED + 1 + w)
+        ms = []
+        for k in range(args.steps):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            sb.run(SEED + 100 + k)
+            e1.record()
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        dev_ms = sum(ms) / len(ms)
+        e2e = []
+        for k in range(args.warmup + args.steps):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            sim.simulate(theta, n_samples=n, random_state=SEED + 200 + k)
+            if k >= args.warmup:
+                e2e.append(time.perf_counter() - t0)
+        label = model if model != "ddm" else "plain_ddm"
+        res[label] = {
+            "simulator": name, "parameter_sets": sb.K, "n_samples": n, "trajectories": sb.total,
+            "accumulators": sb.n_acc, "euler_steps": steps, "accumulator_steps": steps * sb.n_acc,
+            "ms_per_launch": dev_ms, "trajectories_per_s": sb.total / (dev_ms / 1e3),
+            "accumulator_steps_per_s": steps * sb.n_acc / (dev_ms / 1e3),
+            "e2e_trajectories_per_s": sb.total * len(e2e) / sum(e2e),
+        }
+        if name in _REF_MODULE:
+            cpu_jobs.append((label, name, prep, n))
+        del sb, o
+    if args.no_cpu_baseline:
+        return res
+    if _cpu_kind() != "reference":
+        for label in res:
+            res[label]["cpu_reference"] = "unavailable: the reference simulators are not built in oracle/_ref"
+        return res
+    cores = _cores()
+    pool = mp.get_context("spawn").Pool(cores)
+    try:
+        for label, name, prep, n in cpu_jobs:
+            if label == "plain_ddm":  # one parameter set: the samples are split over the cores
+                (kw, bn, bp, _, _), = _row_calls(prep, 1, n, 0)
+                per = [n // cores + (1 if c < n % cores else 0) for c in range(cores)]
+                jobs = [(name, [(kw, bn, bp, m, SEED + 300 + c)]) for c, m in enumerate(per)]
+            else:
+                calls = _row_calls(prep, MIX_CPU_ROWS_PER_CORE[label] * cores, n, SEED + 300)
+                jobs = [(name, [c]) for c in calls]
+            kw, bn, bp, _, _ = jobs[0][1][0]
+            pool.map(_cpu_sim_worker, [(name, [(kw, bn, bp, 10, 1)])] * cores)  # warm the workers
+            t0 = time.perf_counter()
+            done = sum(pool.imap_unordered(_cpu_sim_worker, jobs, chunksize=1))
+            sec = time.perf_counter() - t0
+            r = res[label]
+            r["cpu_reference"] = {"trajectories_per_s": done / sec, "cores": cores, "kind": "reference",
+                                  "sample": f"{done} trajectories ({len(jobs)} shards), wall {sec:.2f} s"}
+            r["speedup_device_vs_cpu"] = r["trajectories_per_s"] / (done / sec)
+            r["speedup_e2e_vs_cpu"] = r["e2e_trajectories_per_s"] / (done / sec)
+    finally:
+        pool.close()
+        pool.join()
+    return res
+
+
 def run_reference(args):
     theta, n_samples = workload(SEED)
     pool = CpuPool()
@@ -480,6 +627,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-surrogate", action="store_true")
+    ap.add_argument("--no-other-workloads", action="store_true")
     ap.add_argument("--surrogate-sets", type=int, default=100_000)
     ap.add_argument("--surrogate-epochs", type=int, default=30)
     ap.add_argument("--n-theta", type=int, default=N_THETA,
@@ -506,6 +654,8 @@ def main():
     line, theta, n_samples = run_ours(args, rank, world, local_rank)
     if rank == 0 and world == 1 and not args.no_surrogate:
         line["surrogate"] = run_surrogate(args, line["clocks"])
+    if rank == 0 and world == 1 and not args.no_other_workloads:
+        line["other_workloads"] = run_other_workloads(args)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_record(theta, n_samples)
     if world > 1:

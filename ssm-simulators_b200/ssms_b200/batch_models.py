@@ -1,10 +1,12 @@
 """Run any configured model for many parameter sets in one device launch.
 
-``simulate_sets`` takes the simulator keyword arguments that
-``Simulator.prepare`` builds (the reference's argument layout per simulator)
-and runs the matching sm_100a kernel with the ragged, set-major output layout:
-set k owns outputs [k * n_samples, (k + 1) * n_samples).  Outputs stay on the
-device for the KDE / training-data pipeline.
+``SetBatch`` takes the simulator keyword arguments that ``Simulator.prepare``
+builds (the reference's argument layout per simulator), uploads them once and
+runs the matching sm_100a kernel with the ragged, set-major output layout:
+set k owns outputs [k * n_samples, (k + 1) * n_samples) (or
+[offsets[k], offsets[k+1]) with per-set sample counts).  Outputs stay on the
+device for the KDE / training-data pipeline.  ``simulate_sets`` is the
+one-shot form.
 """
 
 from __future__ import annotations
@@ -12,8 +14,12 @@ from __future__ import annotations
 import numpy as np
 import torch
 
+from . import _device as D
 from . import boundary_functions as bf
 from . import device as dev
+
+SINGLE = ("ddm_flexbound", "levy_flexbound", "ddm")
+RACE = ("race_model", "lca")
 
 
 def _col(x, K):
@@ -21,51 +27,98 @@ def _col(x, K):
     return a.reshape(K, -1)[:, 0] if a.ndim == 2 else a.reshape(-1)
 
 
+def _dev(x, K=None, name="array"):
+    return None if x is None else D.to_dev_f32(x, K, name)
+
+
+class SetBatch:
+    """K parameter sets of one simulator, resident on the device.
+
+    ``run(seed)`` launches one simulation of every set (asynchronous, on the
+    current stream) and returns the ``SimOutput``; repeated runs reuse the
+    uploaded inputs, so a run costs one kernel launch plus its prologue.
+    """
+
+    def __init__(self, sim_name: str, kwargs: dict, boundary: dict, n_samples: int, *,
+                 max_t: float, delta_t: float, smooth_unif: bool = True, n_samples_per_set=None):
+        D.require_cuda()
+        K = int(np.asarray(kwargs["v"]).shape[0])
+        ns = (np.full(K, int(n_samples), np.int64) if n_samples_per_set is None
+              else np.asarray(n_samples_per_set, np.int64))
+        self.offsets_host = np.concatenate([[0], np.cumsum(ns)]).astype(np.int64)
+        self.total = int(self.offsets_host[-1])
+        self.offsets = torch.from_numpy(self.offsets_host).cuda()
+        self.sim_name, self.K = sim_name, K
+        self.n_samples = int(n_samples)
+        self.max_t, self.delta_t, self.smooth = float(max_t), float(delta_t), bool(smooth_unif)
+        self.n_acc = 1
+        if sim_name in SINGLE or sim_name in RACE:
+            if sim_name == "ddm":
+                spec = {"kind": 1, "a": _col(kwargs["a"], K), "p1": None, "p2": None, "table": None}
+            else:
+                spec = bf.kernel_spec(boundary["boundary_fun"], boundary["boundary_params"], K,
+                                      bf.make_t_s(max_t, delta_t))
+            self.kind = int(spec["kind"])
+            self.a, self.p1, self.p2 = _dev(spec["a"], K, "a"), _dev(spec["p1"], K), _dev(spec["p2"], K)
+            self.table = None if spec["table"] is None else D.to_dev_f32(np.ascontiguousarray(spec["table"]))
+            self.table_shape = None if spec["table"] is None else np.shape(spec["table"])
+        if sim_name in SINGLE:
+            self.v, self.z, self.t = (_dev(_col(kwargs[k], K), K, k) for k in ("v", "z", "t"))
+            self.deadline, self.s = _dev(_col(kwargs["deadline"], K), K), _dev(_col(kwargs["s"], K), K)
+            self.alpha = _dev(_col(kwargs["alpha"], K), K) if sim_name == "levy_flexbound" else None
+        elif sim_name in RACE:
+            v = np.asarray(kwargs["v"], np.float32)
+            self.n_acc = int(v.shape[1])
+            self.v = _dev(v)
+            self.z, self.s = _dev(np.asarray(kwargs["z"], np.float32)), _dev(np.asarray(kwargs["s"], np.float32))
+            self.t, self.deadline = _dev(_col(kwargs["t"], K), K), _dev(_col(kwargs["deadline"], K), K)
+            lca = sim_name == "lca"
+            self.g = _dev(_col(kwargs["g"], K), K) if lca else None
+            self.b = _dev(_col(kwargs["b"], K), K) if lca else None
+            self.v_shape = v.shape
+        elif sim_name == "lba_vanilla":
+            v = np.asarray(kwargs["v"], np.float32)
+            sd = np.asarray(kwargs["sd"], np.float32).reshape(K, -1)
+            if sd.shape[1] != v.shape[1]:
+                sd = np.repeat(sd[:, :1], v.shape[1], axis=1)
+            self.n_acc = int(v.shape[1])
+            self.v_shape = v.shape
+            self.v, self.sd = _dev(v), _dev(np.ascontiguousarray(sd))
+            self.a, self.z = _dev(_col(kwargs["a"], K), K), _dev(_col(kwargs["z"], K), K)
+            self.t, self.deadline = _dev(_col(kwargs["t"], K), K), _dev(_col(kwargs["deadline"], K), K)
+        else:
+            raise ValueError(f"no batched device path for simulator {sim_name!r}")
+
+    def run(self, seed: int, want_steps: bool = False) -> dev.SimOutput:
+        K, total = self.K, self.total
+        if self.sim_name in SINGLE:
+            rts = torch.empty(total, dtype=torch.float32, device="cuda")
+            chs = torch.empty(total, dtype=torch.int32, device="cuda")
+            return dev.simulate_single(
+                self.sim_name, v=self.v, z=self.z, t=self.t, deadline=self.deadline, s=self.s,
+                a=self.a, alpha=self.alpha, n_trials=K, sample_offsets=self.offsets,
+                max_t=self.max_t, delta_t=self.delta_t, bound_kind=self.kind, bound_p1=self.p1,
+                bound_p2=self.p2, bound_table=self._table(), seed=seed, smooth_unif=self.smooth,
+                want_steps=want_steps, out_rts=rts, out_choices=chs)
+        if self.sim_name in RACE:
+            return dev.simulate_race(
+                self.sim_name, v=self.v.reshape(self.v_shape), z=self.z, t=self.t, s=self.s,
+                deadline=self.deadline, n_trials=K, sample_offsets=self.offsets, g=self.g, b=self.b,
+                max_t=self.max_t, delta_t=self.delta_t, bound_kind=self.kind, a=self.a,
+                bound_p1=self.p1, bound_p2=self.p2, bound_table=self._table(), seed=seed,
+                smooth_unif=self.smooth, want_steps=want_steps, total=total)
+        return dev.simulate_lba(v=self.v.reshape(self.v_shape), a=self.a, z=self.z,
+                                deadline=self.deadline, sd=self.sd, t=self.t, n_trials=K,
+                                sample_offsets=self.offsets, seed=seed, total=total)
+
+    def _table(self):
+        return None if self.table is None else self.table.reshape(self.table_shape)
+
+
 def simulate_sets(sim_name: str, kwargs: dict, boundary: dict, n_samples: int, *,
                   max_t: float, delta_t: float, seed: int, smooth_unif: bool = True,
-                  n_samples_per_set=None) -> dev.SimOutput:
+                  n_samples_per_set=None, want_steps: bool = False) -> dev.SimOutput:
     """Simulate K parameter sets (K = len of the per-trial arrays) with
     n_samples each (or n_samples_per_set[k]) in the set-major ragged layout."""
-    K = int(np.asarray(kwargs["v"]).shape[0])
-    ns = (np.full(K, int(n_samples), np.int64) if n_samples_per_set is None
-          else np.asarray(n_samples_per_set, np.int64))
-    offsets = np.concatenate([[0], np.cumsum(ns)]).astype(np.int64)
-    total = int(offsets[-1])
-    offs_t = torch.from_numpy(offsets).cuda()
-    if sim_name in ("ddm_flexbound", "levy_flexbound", "ddm"):
-        if sim_name == "ddm":
-            spec = {"kind": 1, "a": _col(kwargs["a"], K), "p1": None, "p2": None, "table": None}
-        else:
-            spec = bf.kernel_spec(boundary["boundary_fun"], boundary["boundary_params"], K,
-                                  bf.make_t_s(max_t, delta_t))
-        rts = torch.empty(total, dtype=torch.float32, device="cuda")
-        chs = torch.empty(total, dtype=torch.int32, device="cuda")
-        return dev.simulate_single(
-            sim_name, v=_col(kwargs["v"], K), z=_col(kwargs["z"], K), t=_col(kwargs["t"], K),
-            deadline=_col(kwargs["deadline"], K), s=_col(kwargs["s"], K), a=spec["a"],
-            alpha=_col(kwargs["alpha"], K) if sim_name == "levy_flexbound" else None,
-            n_trials=K, sample_offsets=offs_t, max_t=max_t, delta_t=delta_t,
-            bound_kind=spec["kind"], bound_p1=spec["p1"], bound_p2=spec["p2"],
-            bound_table=spec["table"], seed=seed, smooth_unif=smooth_unif, out_rts=rts,
-            out_choices=chs)
-    if sim_name in ("race_model", "lca"):
-        spec = bf.kernel_spec(boundary["boundary_fun"], boundary["boundary_params"], K,
-                              bf.make_t_s(max_t, delta_t))
-        lca = sim_name == "lca"
-        return dev.simulate_race(
-            sim_name, v=np.asarray(kwargs["v"], np.float32), z=np.asarray(kwargs["z"], np.float32),
-            t=_col(kwargs["t"], K), s=np.asarray(kwargs["s"], np.float32),
-            deadline=_col(kwargs["deadline"], K), n_trials=K, sample_offsets=offs_t,
-            g=_col(kwargs["g"], K) if lca else None, b=_col(kwargs["b"], K) if lca else None,
-            max_t=max_t, delta_t=delta_t, bound_kind=spec["kind"], a=spec["a"],
-            bound_p1=spec["p1"], bound_p2=spec["p2"], bound_table=spec["table"], seed=seed,
-            smooth_unif=smooth_unif, total=total)
-    if sim_name == "lba_vanilla":
-        v = np.asarray(kwargs["v"], np.float32)
-        sd = np.asarray(kwargs["sd"], np.float32).reshape(K, -1)
-        if sd.shape[1] != v.shape[1]:
-            sd = np.repeat(sd[:, :1], v.shape[1], axis=1)
-        return dev.simulate_lba(v=v, a=_col(kwargs["a"], K), z=_col(kwargs["z"], K),
-                                deadline=_col(kwargs["deadline"], K), sd=sd, t=_col(kwargs["t"], K),
-                                n_trials=K, sample_offsets=offs_t, seed=seed, total=total)
-    raise ValueError(f"no batched device path for simulator {sim_name!r}")
+    return SetBatch(sim_name, kwargs, boundary, n_samples, max_t=max_t, delta_t=delta_t,
+                    smooth_unif=smooth_unif, n_samples_per_set=n_samples_per_set).run(seed, want_steps)

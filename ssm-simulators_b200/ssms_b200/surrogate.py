@@ -327,7 +327,9 @@ def kde_loglik(model: str, theta, rt, choice, *, n_samples: int = 100_000, delta
     """Simulation + KDE log-likelihood of each (theta_i, rt_i, choice_i): rows
     with equal theta share one simulation of n_samples trajectories and one
     LogKDE fit (the reference's kde_eval, lb = -66.774), all sets in one
-    device launch per stage."""
+    device launch per stage.  With ``group_rows`` equal theta rows are found
+    in linear time when they are adjacent (the usual layout: all queries of a
+    parameter set together) and by a sort otherwise."""
     from .batch_models import simulate_sets
     from .kde import KdeBatch
     from .simulator import Simulator
@@ -335,9 +337,14 @@ def kde_loglik(model: str, theta, rt, choice, *, n_samples: int = 100_000, delta
     th = np.asarray(theta, np.float32)
     rt = np.asarray(rt, np.float64).reshape(-1)
     ch = np.asarray(choice).reshape(-1)
-    if group_rows:
-        uniq, inv = np.unique(th, axis=0, return_inverse=True)
-        inv = inv.reshape(-1)
+    if group_rows and th.shape[0] > 0:
+        starts = np.concatenate([[True], np.any(th[1:] != th[:-1], axis=1)])
+        uniq = th[starts]
+        if np.unique(uniq.view(np.dtype((np.void, uniq.dtype.itemsize * uniq.shape[1]))).ravel()).size == uniq.shape[0]:
+            inv = np.cumsum(starts) - 1  # adjacent runs are the distinct parameter sets
+        else:
+            uniq, inv = np.unique(th, axis=0, return_inverse=True)
+            inv = inv.reshape(-1)
     else:
         uniq, inv = th, np.arange(th.shape[0])
     cfg = _model_config[model]
