@@ -205,17 +205,22 @@ int ssm_kde_fit(const float *rts, const int32_t *choices, int64_t n_sets,
 
 /*
  * ssm_kde_eval -- replaces LogKDE.kde_eval (kde_class.py:188-329): for each
- * query (rt, group), queries sorted by group with query_offsets[G+1],
- * loglik = log_norm + log sum_j exp(-(q - x_j)^2 / 2h^2) - q with
- * q = log(max(rt - displace, eps)); lb where that is <= lb or rt - displace
- * <= 0; -log(n_set * max_t) for groups without data.  float64 output.
- * query_split > 1 splits a group's queries over that many CTAs.
+ * query (rt, group), queries sorted by group with query_offsets[G+1] and
+ * n_queries = query_offsets[G], loglik = log_norm + log sum_j exp(-(q - x_j)^2
+ * / 2h^2) - q with q = log(max(rt - displace, eps)); lb where that is <= lb or
+ * rt - displace <= 0; -log(n_set * max_t) for groups without data.  float64
+ * output.  The work is spread evenly over a persistent grid whatever the
+ * groups' sizes; workspace (256-byte aligned, contents need not be cleared)
+ * must hold ssm_kde_eval_workspace_bytes(n_sets, n_choices, n_queries) bytes,
+ * computed with the same device current.  Results are deterministic.
  */
+size_t ssm_kde_eval_workspace_bytes(int64_t n_sets, int n_choices, int64_t n_queries);
 int ssm_kde_eval(const float *points, const int64_t *point_offsets, const double *bandwidth,
                  const double *log_norm, int64_t n_sets, int n_choices,
                  const int64_t *sample_offsets, const double *displace,
-                 const int64_t *query_offsets, const double *query_rt, double lb, double eps,
-                 double max_t, int query_split, double *out_loglik, void *stream);
+                 const int64_t *query_offsets, const double *query_rt, int64_t n_queries, double lb,
+                 double eps, double max_t, void *workspace, size_t workspace_bytes,
+                 double *out_loglik, void *stream);
 
 /*
  * ssm_kde_sample -- replaces LogKDE.kde_sample's per-choice draws

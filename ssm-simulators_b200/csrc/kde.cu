@@ -13,7 +13,14 @@
 // points through shared memory, keeps QPT queries per thread in registers
 // (q split into float hi + lo parts so q - x_j keeps full precision), evaluates
 // each kernel term as ex2(-(d s)^2) on the SFU and sums in float over 32 terms
-// before adding into a float64 accumulator.
+// before adding into a float64 accumulator.  Groups differ in cost by orders
+// of magnitude (queries x points), so the work is scheduled Stream-K style
+// (Osama, Merrill, Cecka, Garland & Owens, PPoPP'23): the iteration space
+// (group, query tile, point tile) is cut into equal contiguous ranges, one per
+// CTA of a persistent grid; query tiles cut between CTAs are finished by a
+// fix-up kernel that adds the CTAs' partial sums in CTA order.
+#include <algorithm>
+
 #include "common.cuh"
 
 namespace ssm {
@@ -205,43 +212,127 @@ struct KdeEval {
     const double *q_rt;
     double *out;
     int nc;
+    int64_t G;
     const int64_t *soff;
     const double *shift;
     double lb, eps, max_t;
+    // Stream-K schedule (see ssm_kde_eval): units are (group, tile of KDE_QT
+    // queries); a unit's iterations are its group's point tiles.
+    int64_t *uoff;     // [G + 1] first unit of each group
+    int64_t *ucnt;     // [G] units per group (scan input)
+    int64_t *ioff;     // [u_max + 1] first iteration of each unit
+    int64_t *icnt;     // [u_max] iterations per unit (scan input)
+    int64_t u_max;     // capacity of the unit arrays
+    double *slots;     // [P][2][KDE_QT] partial sums of units split between CTAs
+    int64_t P;         // CTAs of the evaluation grid
 };
 
 constexpr int KDE_TILE = 2048;
+constexpr int KDE_QPT = 4;
+constexpr int KDE_THREADS = 128;
+constexpr int KDE_QT = KDE_QPT * KDE_THREADS;
 
-template <int QPT>
-__global__ void __launch_bounds__(128) k_kde_eval(const KdeEval a) {
-    const int64_t g = blockIdx.x;
+__device__ __forceinline__ int64_t upper_index(const int64_t *off, int64_t n, int64_t x) {
+    // largest i in [0, n) with off[i] <= x (off non-decreasing, off[0] <= x)
+    int64_t lo = 0, hi = n;
+    while (hi - lo > 1) {
+        const int64_t mid = (lo + hi) >> 1;
+        if (off[mid] <= x) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
+__global__ void k_kde_units(const KdeEval a) {
+    for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < a.G; g += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t m = a.qoff[g + 1] - a.qoff[g];
+        a.ucnt[g] = (m + KDE_QT - 1) / KDE_QT;
+    }
+}
+
+__global__ void k_kde_unit_iters(const KdeEval a) {
+    const int64_t U = min(a.uoff[a.G], a.u_max);
+    for (int64_t u = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; u < a.u_max; u += (int64_t)gridDim.x * blockDim.x) {
+        int64_t it = 0;
+        if (u < U) {
+            const int64_t g = upper_index(a.uoff, a.G + 1, u);
+            const int64_t n = a.poff[g + 1] - a.poff[g];
+            it = (n > 0) ? (n + KDE_TILE - 1) / KDE_TILE : 1;
+        }
+        a.icnt[u] = it;
+    }
+}
+
+// first iteration of CTA c: floor(c * I / P) (c <= P < 2^16 and I < 2^46, so
+// the product fits in 64 bits)
+__device__ __forceinline__ int64_t sk_begin(int64_t c, int64_t I, int64_t P) {
+    return (c * I) / P;
+}
+// the CTA whose iteration range holds iteration i (empty CTAs own nothing)
+__device__ __forceinline__ int64_t sk_owner(int64_t i, int64_t I, int64_t P) {
+    int64_t c = (i * P) / I;
+    if (c > P - 1) c = P - 1;
+    while (c > 0 && sk_begin(c, I, P) > i) --c;
+    while (c + 1 < P && sk_begin(c + 1, I, P) <= i) ++c;
+    return c;
+}
+
+// log-likelihood of one query from its kernel sum acc (kde_class.py:188-329)
+__device__ __forceinline__ double kde_finalize(const KdeEval &a, int64_t g, int64_t n, double acc,
+                                               double disp, double lq) {
     const int64_t s = g / a.nc;
-    const int64_t q0 = a.qoff[g], q1 = a.qoff[g + 1];
-    if (q0 >= q1) return;
+    double ll;
+    if (n == 0) {
+        // choice without base data: log(1 / n_trials) + log(1 / max_t)
+        ll = -log((double)(a.soff[s + 1] - a.soff[s]) * a.max_t);
+    } else if (!(disp > 0.0)) {
+        ll = a.lb;
+    } else {
+        ll = a.lognorm[g] + log(acc) - lq;
+        if (!(ll > a.lb)) ll = a.lb;
+    }
+    return ll;
+}
+
+// Each thread holds KDE_QPT queries of the unit (q split into float hi + lo
+// parts so q - x_j keeps full precision), the group's points stream through
+// shared memory one tile per iteration, and each kernel term is
+// ex2(-(d s)^2) on the SFU, summed in float over 32 terms before it is added
+// into a float64 accumulator.
+__global__ void __launch_bounds__(KDE_THREADS, 7) k_kde_eval(const KdeEval a) {
     __shared__ __align__(16) float tile[KDE_TILE];
-    const int64_t p0 = a.poff[g], n = a.poff[g + 1] - p0;
-    const double hg = a.h[g];
-    const double sh = a.shift ? a.shift[s] : 0.0;
-    // 2^(-(d*sc)^2) = exp(-d^2 / (2 h^2))
-    const float sc = (n > 0) ? (float)(0.8493218002880191 / hg) : 0.f;  // sqrt(log2(e)/2) / h
-    const int64_t QT = (int64_t)blockDim.x * QPT;
-    for (int64_t t0 = q0 + (int64_t)blockIdx.y * QT; t0 < q1; t0 += (int64_t)gridDim.y * QT) {
-        float qhi[QPT], qlo[QPT], part[QPT];
-        double acc[QPT], lq[QPT], disp[QPT];
+    const int64_t U = min(a.uoff[a.G], a.u_max);
+    const int64_t I = a.ioff[a.u_max];
+    const int64_t c = blockIdx.x;
+    const int64_t i0 = sk_begin(c, I, a.P), i1 = sk_begin(c + 1, I, a.P);
+    if (i0 >= i1) return;
+    int64_t u = upper_index(a.ioff, U, i0);
+    int64_t g = upper_index(a.uoff, a.G + 1, u);
+    for (int64_t it = i0; it < i1;) {
+        while (a.uoff[g + 1] <= u) ++g;
+        const int64_t ubeg = a.ioff[u], uend = a.ioff[u + 1];
+        const int64_t lo = it, hi = (uend < i1) ? uend : i1;
+        const int64_t q0 = a.qoff[g] + (u - a.uoff[g]) * KDE_QT, q1 = a.qoff[g + 1];
+        const int64_t p0 = a.poff[g], n = a.poff[g + 1] - p0;
+        const double hg = a.h[g];
+        const double sh = a.shift ? a.shift[g / a.nc] : 0.0;
+        // 2^(-(d*sc)^2) = exp(-d^2 / (2 h^2))
+        const float sc = (n > 0) ? (float)(0.8493218002880191 / hg) : 0.f;  // sqrt(log2(e)/2) / h
+        float qhi[KDE_QPT], qlo[KDE_QPT], part[KDE_QPT];
+        double acc[KDE_QPT];
 #pragma unroll
-        for (int j = 0; j < QPT; ++j) {
-            const int64_t qi = t0 + threadIdx.x + (int64_t)j * blockDim.x;
-            disp[j] = (qi < q1) ? a.q_rt[qi] - sh : 1.0;
-            lq[j] = log(fmax(disp[j], a.eps));
-            qhi[j] = (float)lq[j];
-            qlo[j] = (float)(lq[j] - (double)qhi[j]);
+        for (int j = 0; j < KDE_QPT; ++j) {
+            const int64_t qi = q0 + threadIdx.x + (int64_t)j * KDE_THREADS;
+            const double lq = log(fmax((qi < q1) ? a.q_rt[qi] - sh : 1.0, a.eps));
+            qhi[j] = (float)lq;
+            qlo[j] = (float)(lq - (double)qhi[j]);
             part[j] = 0.f;
             acc[j] = 0.0;
         }
-        for (int64_t b0 = 0; b0 < n; b0 += KDE_TILE) {
+        for (int64_t t = lo - ubeg; t < hi - ubeg && n > 0; ++t) {
+            const int64_t b0 = t * KDE_TILE;
             const int cnt = (int)min((int64_t)KDE_TILE, n - b0);
             __syncthreads();
-            for (int i = threadIdx.x; i < KDE_TILE; i += blockDim.x)
+            for (int i = threadIdx.x; i < KDE_TILE; i += KDE_THREADS)
                 tile[i] = (i < cnt) ? __ldg(a.points + p0 + b0 + i) : qhi[0] + 1e30f;  // padding: zero weight
             __syncthreads();
             const float4 *t4 = reinterpret_cast<const float4 *>(tile);
@@ -252,7 +343,7 @@ __global__ void __launch_bounds__(128) k_kde_eval(const KdeEval a) {
                     const float4 x = t4[min(k0 + kk, KDE_TILE / 4 - 1)];
                     const bool live = (k0 + kk) < n4;
 #pragma unroll
-                    for (int j = 0; j < QPT; ++j) {
+                    for (int j = 0; j < KDE_QPT; ++j) {
                         float d, e, r0, r1, r2, r3;
                         d = ((qhi[j] - x.x) + qlo[j]) * sc; e = -d * d;
                         asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r0) : "f"(e));
@@ -266,27 +357,54 @@ __global__ void __launch_bounds__(128) k_kde_eval(const KdeEval a) {
                     }
                 }
 #pragma unroll
-                for (int j = 0; j < QPT; ++j) {
+                for (int j = 0; j < KDE_QPT; ++j) {
                     acc[j] += (double)part[j];
                     part[j] = 0.f;
                 }
             }
         }
+        if (lo == ubeg && hi == uend) {
 #pragma unroll
-        for (int j = 0; j < QPT; ++j) {
-            const int64_t qi = t0 + threadIdx.x + (int64_t)j * blockDim.x;
-            if (qi >= q1) continue;
-            double ll;
-            if (n == 0) {
-                // choice without base data: log(1 / n_trials) + log(1 / max_t)
-                ll = -log((double)(a.soff[s + 1] - a.soff[s]) * a.max_t);
-            } else if (!(disp[j] > 0.0)) {
-                ll = a.lb;
-            } else {
-                ll = a.lognorm[g] + log(acc[j]) - lq[j];
-                if (!(ll > a.lb)) ll = a.lb;
+            for (int j = 0; j < KDE_QPT; ++j) {
+                const int64_t qi = q0 + threadIdx.x + (int64_t)j * KDE_THREADS;
+                if (qi < q1) {
+                    const double disp = a.q_rt[qi] - sh;
+                    a.out[qi] = kde_finalize(a, g, n, acc[j], disp, log(fmax(disp, a.eps)));
+                }
             }
-            a.out[qi] = ll;
+        } else {
+            // split unit: slot 0 (head) if it began in an earlier CTA, else slot 1 (tail)
+            double *slot = a.slots + (c * 2 + (ubeg < i0 ? 0 : 1)) * KDE_QT;
+#pragma unroll
+            for (int j = 0; j < KDE_QPT; ++j) slot[threadIdx.x + j * KDE_THREADS] = acc[j];
+        }
+        it = hi;
+        ++u;
+    }
+}
+
+// Units split between CTAs: their partial sums are added in CTA order (a fixed
+// order, so results do not depend on timing) and finalised.
+__global__ void __launch_bounds__(KDE_THREADS) k_kde_fixup(const KdeEval a) {
+    const int64_t U = min(a.uoff[a.G], a.u_max);
+    const int64_t I = a.ioff[a.u_max];
+    for (int64_t u = blockIdx.x; u < U; u += gridDim.x) {
+        const int64_t ubeg = a.ioff[u], uend = a.ioff[u + 1];
+        const int64_t c0 = sk_owner(ubeg, I, a.P), c1 = sk_owner(uend - 1, I, a.P);
+        if (c0 == c1) continue;
+        const int64_t g = upper_index(a.uoff, a.G + 1, u);
+        const int64_t q0 = a.qoff[g] + (u - a.uoff[g]) * KDE_QT, q1 = a.qoff[g + 1];
+        const int64_t n = a.poff[g + 1] - a.poff[g];
+        const double sh = a.shift ? a.shift[g / a.nc] : 0.0;
+        for (int j = 0; j < KDE_QPT; ++j) {
+            const int r = threadIdx.x + j * KDE_THREADS;
+            const int64_t qi = q0 + r;
+            if (qi >= q1) continue;
+            double acc = a.slots[(c0 * 2 + 1) * KDE_QT + r];
+            for (int64_t cc = c0 + 1; cc <= c1; ++cc)
+                if (sk_begin(cc, I, a.P) < sk_begin(cc + 1, I, a.P)) acc += a.slots[(cc * 2) * KDE_QT + r];
+            const double disp = a.q_rt[qi] - sh;
+            a.out[qi] = kde_finalize(a, g, n, acc, disp, log(fmax(disp, a.eps)));
         }
     }
 }
@@ -532,22 +650,91 @@ int ssm_kde_fit(const float *rts, const int32_t *choices, int64_t n_sets,
     return SSM_OK;
 }
 
+}  // extern "C"
+
+namespace ssm {
+
+// CTAs of the evaluation grid: every SM filled to the kernel's occupancy.
+static int64_t kde_eval_ctas() {
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_kde_eval, KDE_THREADS, 0) != cudaSuccess ||
+        per_sm < 1)
+        per_sm = 1;
+    return (int64_t)per_sm * sm_count();
+}
+
+static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+struct KdeEvalLayout {
+    size_t uoff, ucnt, ioff, icnt, slots, total;
+    int64_t u_max, P;
+};
+
+static KdeEvalLayout kde_eval_layout(int64_t G, int64_t n_queries) {
+    KdeEvalLayout L;
+    L.P = kde_eval_ctas();
+    L.u_max = n_queries / KDE_QT + G + 1;
+    L.uoff = 0;
+    L.ucnt = L.uoff + align256((size_t)(G + 1) * 8);
+    L.ioff = L.ucnt + align256((size_t)G * 8);
+    L.icnt = L.ioff + align256((size_t)(L.u_max + 1) * 8);
+    L.slots = L.icnt + align256((size_t)L.u_max * 8);
+    L.total = L.slots + (size_t)L.P * 2 * KDE_QT * sizeof(double);
+    return L;
+}
+
+}  // namespace ssm
+
+extern "C" {
+
+size_t ssm_kde_eval_workspace_bytes(int64_t n_sets, int n_choices, int64_t n_queries) {
+    if (n_sets < 0 || n_choices < 1 || n_queries < 0) return 0;
+    return ssm::kde_eval_layout(n_sets * n_choices, n_queries).total;
+}
+
 int ssm_kde_eval(const float *points, const int64_t *point_offsets, const double *bandwidth,
                  const double *log_norm, int64_t n_sets, int n_choices,
                  const int64_t *sample_offsets, const double *displace,
-                 const int64_t *query_offsets, const double *query_rt, double lb, double eps,
-                 double max_t, int query_split, double *out_loglik, void *stream) {
+                 const int64_t *query_offsets, const double *query_rt, int64_t n_queries, double lb,
+                 double eps, double max_t, void *workspace, size_t workspace_bytes,
+                 double *out_loglik, void *stream) {
     using namespace ssm;
     SSM_REQUIRE(n_sets >= 0 && n_choices >= 1 && n_choices <= KDE_MAX_CHOICES, "bad n_sets / n_choices");
-    if (n_sets == 0) return SSM_OK;
+    SSM_REQUIRE(n_queries >= 0, "n_queries must be >= 0");
+    if (n_sets == 0 || n_queries == 0) return SSM_OK;
     SSM_REQUIRE(points && point_offsets && bandwidth && log_norm && sample_offsets && query_offsets &&
-                query_rt && out_loglik, "all buffers are required");
-    KdeEval a{points, point_offsets, bandwidth, log_norm, query_offsets, query_rt, out_loglik,
-              n_choices, sample_offsets, displace, lb, eps, max_t};
+                query_rt && out_loglik && workspace, "all buffers are required");
     const int64_t G = n_sets * n_choices;
-    SSM_REQUIRE(G < (1ll << 31), "too many groups for one launch");
-    dim3 grid((unsigned)G, (unsigned)(query_split > 0 ? query_split : 1));
-    k_kde_eval<4><<<grid, 128, 0, (cudaStream_t)stream>>>(a);
+    const KdeEvalLayout L = kde_eval_layout(G, n_queries);
+    SSM_REQUIRE(workspace_bytes >= L.total, "workspace too small: %zu bytes, need %zu (ssm_kde_eval_workspace_bytes)",
+                workspace_bytes, L.total);
+    SSM_REQUIRE(((uintptr_t)workspace & 255) == 0, "workspace must be 256-byte aligned");
+    uint8_t *ws = static_cast<uint8_t *>(workspace);
+    KdeEval a;
+    a.points = points; a.poff = point_offsets; a.h = bandwidth; a.lognorm = log_norm;
+    a.qoff = query_offsets; a.q_rt = query_rt; a.out = out_loglik; a.nc = n_choices; a.G = G;
+    a.soff = sample_offsets; a.shift = displace; a.lb = lb; a.eps = eps; a.max_t = max_t;
+    a.uoff = reinterpret_cast<int64_t *>(ws + L.uoff);
+    a.ucnt = reinterpret_cast<int64_t *>(ws + L.ucnt);
+    a.ioff = reinterpret_cast<int64_t *>(ws + L.ioff);
+    a.icnt = reinterpret_cast<int64_t *>(ws + L.icnt);
+    a.u_max = L.u_max;
+    a.slots = reinterpret_cast<double *>(ws + L.slots);
+    a.P = L.P;
+    cudaStream_t st = (cudaStream_t)stream;
+    const int ng = (int)std::min<int64_t>((G + 255) / 256, 4096);
+    k_kde_units<<<ng, 256, 0, st>>>(a);
+    SSM_CUDA(cudaGetLastError());
+    k_scan_i64<<<1, 1024, 0, st>>>(a.ucnt, G, a.uoff);
+    SSM_CUDA(cudaGetLastError());
+    const int nu = (int)std::min<int64_t>((L.u_max + 255) / 256, 4096);
+    k_kde_unit_iters<<<nu, 256, 0, st>>>(a);
+    SSM_CUDA(cudaGetLastError());
+    k_scan_i64<<<1, 1024, 0, st>>>(a.icnt, L.u_max, a.ioff);
+    SSM_CUDA(cudaGetLastError());
+    k_kde_eval<<<(unsigned)L.P, KDE_THREADS, 0, st>>>(a);
+    SSM_CUDA(cudaGetLastError());
+    k_kde_fixup<<<(unsigned)std::min<int64_t>(L.u_max, 65535), KDE_THREADS, 0, st>>>(a);
     SSM_CUDA(cudaGetLastError());
     return SSM_OK;
 }

@@ -72,8 +72,9 @@ _SIGNATURES: dict[str, tuple] = {
                      C.c_size_t, _P]),
     "ssm_lba_vanilla": (_I, [_P, _P, _P, _P, _P, _P, _I64, _I64, _I, _P, _U64, _P, _P, _P, _P, _P]),
     "ssm_kde_fit": (_I, [_P, _P, _I64, _P, _P, _I, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
-    "ssm_kde_eval": (_I, [_P, _P, _P, _P, _I64, _I, _P, _P, _P, _P, C.c_double, C.c_double,
-                          C.c_double, _I, _P, _P]),
+    "ssm_kde_eval_workspace_bytes": (C.c_size_t, [_I64, _I, _I64]),
+    "ssm_kde_eval": (_I, [_P, _P, _P, _P, _I64, _I, _P, _P, _P, _P, _I64, C.c_double, C.c_double,
+                          C.c_double, _P, C.c_size_t, _P, _P]),
     "ssm_kde_sample": (_I, [_P, _P, _P, _I64, _I, _P, _P, _P, _U64, C.c_double, C.c_double,
                             C.c_double, _P, _P]),
     "ssm_set_summary": (_I, [_P, _P, _I64, _P, _P, _I, C.c_double, _P, _P, _P, _I, _P, _I, _P, _P]),

@@ -398,7 +398,7 @@ class BatchedKdePipeline:
         qoff = np.concatenate([[0], np.cumsum(per_group)]).astype(np.int64)
         q_rt = kb.sample(qoff, nby.reshape(-1), seed=seed + 1, max_t=max_t, unif_lo=0.0001,
                          unif_hi=max_t if max_t < 100 else 100.0)
-        ll = kb.evaluate(qoff, q_rt, max_t=float(np.float32(max_t)), query_split=1)
+        ll = kb.evaluate(qoff, q_rt, max_t=float(np.float32(max_t)))
         params = self.model_config["params"]
         th = np.stack([np.asarray(theta[k], np.float32).reshape(-1) for k in params], axis=1)
         th_t = torch.from_numpy(np.ascontiguousarray(th)).cuda()

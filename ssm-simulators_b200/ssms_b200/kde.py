@@ -87,17 +87,23 @@ class KdeBatch:
             D.stream_ptr(stream)))
 
     def evaluate(self, query_offsets, query_rt: torch.Tensor, *, max_t: float, lb: float = -66.774,
-                 eps: float = 10e-5, query_split: int = 1) -> torch.Tensor:
+                 eps: float = 10e-5) -> torch.Tensor:
         """Log-likelihoods of queries sorted by group (query_offsets: [G + 1])."""
         dev = D.require_cuda()
+        qoff_host = None if isinstance(query_offsets, torch.Tensor) else np.asarray(query_offsets, np.int64)
         qoff = _i64(query_offsets, dev)
         q = query_rt.to(dev, torch.float64).contiguous().reshape(-1)
+        n_q = int(qoff_host[-1]) if qoff_host is not None else int(qoff[-1].item())
+        if n_q > q.numel():
+            raise ValueError("query_offsets address more queries than query_rt holds")
         out = torch.empty(q.numel(), dtype=torch.float64, device=dev)
-        _lib.check(_lib.lib().ssm_kde_eval(
+        L = _lib.lib()
+        ws = D.workspace(L.ssm_kde_eval_workspace_bytes(self.n_sets, self.nc, n_q), tag=2, stream=self.stream)
+        _lib.check(L.ssm_kde_eval(
             D.ptr(self.points), D.ptr(self.point_offsets), D.ptr(self.bandwidth),
             D.ptr(self.log_norm), self.n_sets, self.nc, D.ptr(self.sample_offsets),
-            D.ptr(self.displace), D.ptr(qoff), D.ptr(q), float(lb), float(eps), float(max_t),
-            int(query_split), D.ptr(out), D.stream_ptr(self.stream)))
+            D.ptr(self.displace), D.ptr(qoff), D.ptr(q), n_q, float(lb), float(eps), float(max_t),
+            D.ptr(ws), ws.numel(), D.ptr(out), D.stream_ptr(self.stream)))
         return out
 
     def sample(self, out_offsets, n_kde, *, seed: int, max_t: float, unif_lo: float = 0.0001,
@@ -199,8 +205,7 @@ class LogKDE:
         order = np.argsort(gid, kind="stable")
         qoff = np.concatenate([[0], np.cumsum(np.bincount(gid, minlength=len(self.data["choices"])))])
         ll_sorted = self._batch.evaluate(qoff, torch.from_numpy(rts[order]),
-                                         max_t=float(self.simulator_info["max_t"]), lb=lb, eps=eps,
-                                         query_split=max(1, int(np.ceil(rts.shape[0] / 512))))
+                                         max_t=float(self.simulator_info["max_t"]), lb=lb, eps=eps)
         out = np.empty(rts.shape[0])
         out[order] = ll_sorted.cpu().numpy()
         return np.squeeze(out) if log_eval else np.squeeze(np.exp(out))

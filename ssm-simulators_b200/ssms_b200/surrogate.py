@@ -365,7 +365,7 @@ def kde_loglik(model: str, theta, rt, choice, *, n_samples: int = 100_000, delta
     counts = np.bincount(grp, minlength=K * len(pc))
     qoff = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
     q = torch.from_numpy(np.ascontiguousarray(rt[order])).cuda()
-    ll = kb.evaluate(qoff, q, max_t=float(np.float32(max_t)), query_split=1).cpu().numpy()
+    ll = kb.evaluate(qoff, q, max_t=float(np.float32(max_t))).cpu().numpy()
     out = np.empty_like(ll)
     out[order] = ll
     return out

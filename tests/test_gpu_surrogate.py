@@ -11,6 +11,7 @@ import numpy as np
 import pytest
 import torch
 
+import mlp_oracle as MO
 import nf_oracle as NO
 from ssms_b200 import surrogate as S
 from ssms_b200 import surrogate_train as T
@@ -92,11 +93,20 @@ def test_theta_gradient_against_analytic_gradient(trained):
 
 
 def test_theta_gradient_against_finite_differences(trained):
-    """d out / d theta from the backward kernel against a least-squares slope
-    through six symmetric finite differences (steps of 0.5-1.5 % of each
-    parameter's range), which averages out the bf16 quantisation of the
-    forward pass; points where the network sits at its label floor (a kink)
-    are left out."""
+    """d out / d theta from the backward kernel against finite differences of
+    the same trained network.
+
+    (1) Central differences of the network evaluated in float64 (the oracle's
+    unquantised forward on the trained weights; steps of 0.1 % of each
+    parameter's range): the kernel's backward GEMMs take bf16 operands, whose
+    rounding (about 0.4 % per stage) is amplified where a gradient is a small
+    difference of large terms -- d/dt against d/drt is the worst case, at
+    about 6 % -- so the bound is 10 %.
+    (2) A least-squares slope through six symmetric finite differences of the
+    kernel's own forward pass (steps of 0.5-1.5 % of the range), which averages
+    out the bf16 quantisation of that forward pass; a looser bound, because the
+    quantised forward is a fine staircase in each input.
+    Points where the network sits at its label floor (a kink) are left out."""
     net, _ = trained
     rng = np.random.default_rng(3)
     th, xq = T.uniform_queries("angle", 500, 4, seed=13)
@@ -104,10 +114,17 @@ def test_theta_gradient_against_finite_differences(trained):
     _, dx = net.forward(torch.from_numpy(xq), want_dx=True)
     dx = dx.double().cpu().numpy()
     f = lambda x: net.forward(torch.from_numpy(x)).double().cpu().numpy()  # noqa: E731
+    p64 = net.params.detach().double().cpu().numpy()
+    f64 = lambda x: MO.forward(p64, x, net.norm_c, net.norm_s, quantize=False)  # noqa: E731
     f0 = f(xq)
     keep = f0 > -10.0
     lo, hi = (np.asarray(b, np.float64) for b in S._model_config["angle"]["param_bounds"])
     for j in range(5):
+        xp, xm = xq.copy(), xq.copy()
+        xp[:, j] += 0.001 * (hi[j] - lo[j])
+        xm[:, j] -= 0.001 * (hi[j] - lo[j])
+        fd64 = (f64(xp) - f64(xm)) / (xp[:, j].astype(np.float64) - xm[:, j])
+        rel64 = np.linalg.norm(dx[keep, j] - fd64[keep]) / np.linalg.norm(fd64[keep])
         num = np.zeros(xq.shape[0])
         den = np.zeros(xq.shape[0])
         for m in (-3, -2, -1, 1, 2, 3):
@@ -118,5 +135,6 @@ def test_theta_gradient_against_finite_differences(trained):
             den += step * step
         fd = num / den
         rel = np.linalg.norm(dx[keep, j] - fd[keep]) / np.linalg.norm(fd[keep])
-        print("fd-slope", j, rel)
-        assert rel < 0.15, (j, rel)
+        print("fd", j, "float64 network", rel64, "kernel forward slope", rel)
+        assert rel64 < 0.1, (j, rel64)
+        assert rel < 0.2, (j, rel)
