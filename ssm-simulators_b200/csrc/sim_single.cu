@@ -167,22 +167,65 @@ __device__ __forceinline__ float bound_at(const TrialRow &r, float ixf, int ix,
     }
 }
 
+// sin x and cos x on [0, pi/2] from their Taylor series through x^11 and x^12
+// (truncation errors below 6e-8 and 7e-9 there): short branch-free code for
+// the stable sampler, whose angles are always reduced to that interval.
+__device__ __forceinline__ float sin_q(float x) {
+    const float t = x * x;
+    float p = fmaf(t, -2.5052108e-08f, 2.7557319e-06f);  // -1/11!, 1/9!
+    p = fmaf(t, p, -1.9841270e-04f);                     // -1/7!
+    p = fmaf(t, p, 8.3333333e-03f);                      // 1/5!
+    p = fmaf(t, p, -1.6666667e-01f);                     // -1/3!
+    p = fmaf(t, p, 1.0f);
+    return x * p;
+}
+__device__ __forceinline__ float cos_q(float x) {
+    const float t = x * x;
+    float p = fmaf(t, 2.0876757e-09f, -2.7557319e-07f);  // 1/12!, -1/10!
+    p = fmaf(t, p, 2.4801587e-05f);                      // 1/8!
+    p = fmaf(t, p, -1.3888889e-03f);                     // -1/6!
+    p = fmaf(t, p, 4.1666667e-02f);                      // 1/4!
+    p = fmaf(t, p, -0.5f);
+    return fmaf(t, p, 1.0f);
+}
+
 // Symmetric alpha-stable variate by Chambers-Mallows-Stuck (Chambers, Mallows
 // & Stuck, JASA 71, 1976) with the reference's guards (_utils.pyx:426-472):
-// U ~ U(-pi/2 + 1e-7, pi/2 - 1e-7), W ~ Exp(1) floored at 1e-10, cosines
-// floored at 1e-10 in magnitude, output clipped to +-1e10 and NaN -> 0.
+// U ~ U(-pi/2 + 1e-7, pi/2 - 1e-7), W ~ Exp(1) floored at 1e-10, output
+// clipped to +-1e10 and NaN -> 0.
+//   X = sin(alpha U) / cos(U)^(1/alpha) * (cos((1 - alpha) U) / W)^((1 - alpha) / alpha)
+// (tan U for alpha = 1).  U = pi (u - 1/2) with u on a 2^-23 grid; the sampler
+// works with |U| and its complement V = pi/2 - |U| = pi min(u, 1 - u), which
+// carries one rounding only, so cos U = sin V keeps its relative precision as
+// |U| -> pi/2, where the heavy tail comes from.  Both powers are taken as one
+// power of two.
 __device__ __forceinline__ float cms_stable(uint32_t bu, uint32_t bw, const TrialRow &r) {
     const float u01 = bits_to_1_2(bu) - 1.0f;
-    const float U = fmaf(u01, 3.1415925f, -1.5707962f);
+    const float m = fmaxf(0.5f - fabsf(u01 - 0.5f), 3.1830988e-08f);  // V >= 1e-7 (the U clamp)
+    const float V = 3.14159265f * m;
+    const float aU = 1.57079633f - V;  // |U|
     const float W = fmaxf(-__logf(uniform_open(bw)), 1e-10f);
     float X;
     if (r.alpha == 1.0f) {
-        X = tanf(U);
+        X = cos_q(V) / sin_q(V);  // |tan U|
     } else {
-        const float cu = fmaxf(fabsf(cosf(U)), 1e-10f);
-        const float cua = fmaxf(fabsf(cosf(U * (1.0f - r.alpha))), 1e-10f);
-        X = (sinf(r.alpha * U) / __powf(cu, r.inv_alpha)) * __powf(cua / W, r.expo);
+        const float cu = sin_q(V);                                             // cos U > 0
+        // cos((1 - alpha) U) = cos(c |U|), c = |1 - alpha| <= 1; past pi/4 as
+        // sin(pi/2 - c |U|) = sin(pi/2 (1 - c) + c V), which does not cancel
+        const float c = fabsf(1.0f - r.alpha);
+        const float B = c * aU;
+        const float cua = fmaxf((B > 0.78539816f) ? sin_q(fmaf(c, V, 1.57079633f * (1.0f - c))) : cos_q(B),
+                                1e-10f);
+        // alpha |U| in [0, pi); past pi/2 use pi - alpha |U| = pi (1 - alpha/2) + alpha V,
+        // which does not cancel as alpha -> 2
+        float A = r.alpha * aU;
+        if (A > 1.57079633f) A = fmaf(r.alpha, V, 3.14159265f * fmaf(-0.5f, r.alpha, 1.0f));
+        const float e = fmaf(r.expo, __log2f(cua) - __log2f(W), -r.inv_alpha * __log2f(cu));
+        float p2;
+        asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(p2) : "f"(e));
+        X = sin_q(A) * p2;  // |sin(alpha U)| ...
     }
+    X = (u01 < 0.5f) ? -X : X;  // ... times sign(U): every factor but sin(alpha U) is even in U
     if (X != X) X = 0.f;
     return fminf(fmaxf(X, -1e10f), 1e10f);
 }
