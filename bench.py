@@ -47,6 +47,7 @@ WORKLOAD = ("ddm_flexbound angle boundary, 4096 theta ~ U(v[-3,3], a[0.3,3], z[0
 # normals -> 15; Box-Muller ~6.5 per normal incl. 2 SFU ops; update, boundary
 # and exit test ~6.5) -> 28 lane-instructions per accumulator-step.
 INSTR_PER_STEP = 28.0
+E2E_WINDOWS = 5
 N_SM = 148
 LANES_PER_SM_CLK = 128
 
@@ -277,9 +278,8 @@ def run_ours(args, rank, world, local_rank):
         sim.z.copy_(host_theta["z"], non_blocking=True)
         sim.t.copy_(host_theta["t"], non_blocking=True)
         sim.p1.copy_(slope_h, non_blocking=True)
-        sim.replay()
-        rts_h.copy_(sim.rts, non_blocking=True)
-        chs_h.copy_(sim.choices, non_blocking=True)
+        # trial windows whose output copies overlap the next windows' simulation
+        sim.run_to_host(rts_h, chs_h, chunks=args.e2e_windows)
         torch.cuda.synchronize()
         if i >= args.warmup:
             e2e_ms.append((time.perf_counter() - t0) * 1e3)
@@ -313,6 +313,7 @@ def run_ours(args, rank, world, local_rank):
         "e2e": {"value": e2e_value, "unit": "trajectories/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
         "gpu_launches": 2 * args.steps,
+        "e2e_launches": 2 * args.e2e_windows * args.steps,
         "clocks": clocks,
     }
     return line, theta, n_samples
@@ -628,6 +629,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-surrogate", action="store_true")
     ap.add_argument("--no-other-workloads", action="store_true")
+    ap.add_argument("--e2e-windows", type=int, default=E2E_WINDOWS,
+                    help="trial windows of the end-to-end leg (output copies overlap later windows)")
     ap.add_argument("--surrogate-sets", type=int, default=100_000)
     ap.add_argument("--surrogate-epochs", type=int, default=30)
     ap.add_argument("--n-theta", type=int, default=N_THETA,

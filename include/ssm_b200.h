@@ -53,6 +53,13 @@ typedef struct ssm_launch {
     int block_threads;     /* 0 = library default (autotuned value if set) */
     int blocks_per_sm;     /* 0 = as many as fit                            */
     int chunk;             /* trajectories a warp claims per queue access; 0 = default */
+    /* Index that trial 0 of this call has in the random streams (0 = none).
+     * A batch simulated as several calls over consecutive trial windows --
+     * each with its per-trial pointers advanced to the window, first_trial =
+     * the window's first trial, and the window's slice of the batch's ragged
+     * sample_offsets (whose values stay global output indices) -- gives the
+     * same outputs as one call over the whole batch. */
+    int64_t first_trial;
 } ssm_launch;
 
 /* Version / diagnostics -------------------------------------------------- */
@@ -80,7 +87,9 @@ size_t ssm_ddm_workspace_bytes(int64_t n_trials);
  * bound_table             : float32[n_trials * table_stride] (TABLE only)
  * sample_offsets          : NULL for n_samples per trial in the reference
  *                           layout, else int64[n_trials+1] ragged prefix sums
- *                           (output index sample_offsets[k] + n)
+ *                           (output index sample_offsets[k] + n; the call
+ *                           simulates outputs sample_offsets[0] ..
+ *                           sample_offsets[n_trials] - 1)
  * max_t_per_trial         : NULL (use max_t) or float32[n_trials]
  * noise_rows / noise_row_len / noise_unif : NULL for the device RNG
  * traj                    : NULL or float32[traj_len]; receives trial 0 /

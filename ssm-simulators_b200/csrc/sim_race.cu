@@ -36,7 +36,8 @@ struct RaceParams {
     const float *rows;
     int64_t row_floats;
     const int64_t *offsets;
-    int64_t n_trials, total;
+    int64_t n_trials, total;  // total -1: offsets[n_trials] - offsets[0]
+    uint32_t k_base;          // random-stream index of trial 0 (trial windows of a larger batch)
     int np;
     float dt;
     int smooth, chunk;
@@ -154,7 +155,7 @@ __device__ __forceinline__ bool race_step(const RaceParams &p, RaceLane<NP> &L, 
 #pragma unroll
         for (int j0 = 0; j0 < NP; j0 += 4) {
             if (j0 < np) {
-                const uint4 r = philox10(make_uint4(ctr, L.n, L.k, 0u), p.key);
+                const uint4 r = philox10(make_uint4(ctr, L.n, L.k + p.k_base, 0u), p.key);
                 ctr += 1;
                 const float2 a = std_normal_pair(r.x, r.y);
                 const float2 b = std_normal_pair(r.z, r.w);
@@ -213,7 +214,7 @@ __device__ __forceinline__ void race_finalize(const RaceParams &p, const RaceLan
                                               const RaceHead &h, int np) {
     float u;
     if (NOISE) u = __ldg(p.nunif + L.w);
-    else u = uniform_co(philox10(make_uint4(0xFFFFFFFFu, L.n, L.k, 1u), p.key).x);
+    else u = uniform_co(philox10(make_uint4(0xFFFFFFFFu, L.n, L.k + p.k_base, 1u), p.key).x);
     // compute_smooth_unif receives the time as a C float (_utils.pyx:668-695)
     const float tpf = LCA ? __double2float_rn(L.tpd) : L.tp;
     float sm = 0.f;
@@ -262,6 +263,7 @@ __device__ __forceinline__ void race_init(const RaceParams &p, RaceLane<NP> &L, 
         k = w % p.n_trials;
         n = w / p.n_trials;
     } else {
+        w += __ldg(p.offsets);  // global output index (trial windows start past 0)
         k = race_find(p.offsets, p.n_trials, w, hint);
         n = w - __ldg(p.offsets + k);
         hint = k;
@@ -288,7 +290,7 @@ __global__ void __launch_bounds__(256) k_race(const __grid_constant__ RaceParams
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const unsigned lt_mask = (1u << lane) - 1u;
-    const int64_t total = (p.total >= 0) ? p.total : __ldg(p.offsets + p.n_trials);
+    const int64_t total = (p.total >= 0) ? p.total : __ldg(p.offsets + p.n_trials) - __ldg(p.offsets);
     const int np = (NP == RACE_MAX_NP) ? p.np : NP;
     RaceLane<NP> L;
     RaceHead h;
@@ -478,6 +480,7 @@ static int run_race(bool lca, const float *v, const float *z, const float *t, co
     p.key = philox_keys(seed);
     p.rows = rows; p.row_floats = race_row_floats(np); p.offsets = offsets;
     p.n_trials = n_trials; p.total = total; p.np = np; p.dt = dt; p.smooth = smooth ? 1 : 0;
+    p.k_base = (uint32_t)((launch && launch->first_trial > 0) ? launch->first_trial : 0);
     p.chunk = (launch && launch->chunk >= 32) ? launch->chunk : 64;
     p.table = table; p.tstride = tstride; p.tlen = tlen;
     p.noise = noise; p.nlen = nlen; p.nunif = nunif;

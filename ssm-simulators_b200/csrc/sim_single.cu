@@ -59,7 +59,8 @@ struct SingleParams {
     const TrialRow *rows;
     const int64_t *offsets;  // ragged prefix sums (n_trials + 1) or nullptr
     int64_t n_trials;
-    int64_t total;           // number of trajectories; -1 = read offsets[n_trials]
+    int64_t total;           // number of trajectories; -1 = offsets[n_trials] - offsets[0]
+    uint32_t k_base;         // random-stream index of trial 0 (trial windows of a larger batch)
     float dt;
     int smooth;
     int chunk;
@@ -268,16 +269,16 @@ __device__ __forceinline__ void draw_block(const SingleParams &p, const Lane &L,
     } else if (MODEL == M_LEVY) {
 #pragma unroll
         for (int h = 0; h < BLK / 2; h += 2) {
-            const uint4 b = philox10(make_uint4(L.blk, L.n, L.k, 2u + (uint32_t)h), p.key);
+            const uint4 b = philox10(make_uint4(L.blk, L.n, L.k + p.k_base, 2u + (uint32_t)h), p.key);
             g[2 * h + 0] = fmaf(r.scale, cms_stable(b.x, b.y, r), r.drift);
             g[2 * h + 1] = fmaf(r.scale, cms_stable(b.z, b.w, r), r.drift);
-            const uint4 c = philox10(make_uint4(L.blk, L.n, L.k, 3u + (uint32_t)h), p.key);
+            const uint4 c = philox10(make_uint4(L.blk, L.n, L.k + p.k_base, 3u + (uint32_t)h), p.key);
             g[2 * h + 2] = fmaf(r.scale, cms_stable(c.x, c.y, r), r.drift);
             g[2 * h + 3] = fmaf(r.scale, cms_stable(c.z, c.w, r), r.drift);
         }
     } else {
-        const uint4 b0 = philox10(make_uint4(2u * L.blk, L.n, L.k, 0u), p.key);
-        const uint4 b1 = philox10(make_uint4(2u * L.blk + 1u, L.n, L.k, 0u), p.key);
+        const uint4 b0 = philox10(make_uint4(2u * L.blk, L.n, L.k + p.k_base, 0u), p.key);
+        const uint4 b1 = philox10(make_uint4(2u * L.blk + 1u, L.n, L.k + p.k_base, 0u), p.key);
         bm_increment(b0.x, b0.y, r.c2, r.drift, g[0], g[1]);
         bm_increment(b0.z, b0.w, r.c2, r.drift, g[2], g[3]);
         bm_increment(b1.x, b1.y, r.c2, r.drift, g[4], g[5]);
@@ -336,7 +337,7 @@ __device__ __forceinline__ void finalize(const SingleParams &p, const Lane &L) {
     const float t = __ldg(&row->t), deadline = __ldg(&row->deadline), dl = __ldg(&row->dl_tmp);
     float u;
     if (NOISE) u = __ldg(p.nunif + L.w);
-    else u = uniform_co(philox10(make_uint4(0u, L.n, L.k, 1u), p.key).x);
+    else u = uniform_co(philox10(make_uint4(0u, L.n, L.k + p.k_base, 1u), p.key).x);
     // compute_smooth_unif (_utils.pyx:668-695): double arithmetic, float result
     float sm = 0.f;
     if (p.smooth) {
@@ -358,6 +359,7 @@ __device__ __forceinline__ void lane_init(const SingleParams &p, Lane &L, TrialR
         k = w % p.n_trials;
         n = w / p.n_trials;
     } else {
+        w += __ldg(p.offsets);  // global output index (trial windows start past 0)
         k = ragged_find(p.offsets, p.n_trials, w, hint);
         n = w - __ldg(p.offsets + k);
         hint = k;
@@ -382,7 +384,7 @@ __global__ void __launch_bounds__(256, SSM_MIN_CTAS) k_single(const __grid_const
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const unsigned lt_mask = (1u << lane) - 1u;
-    const int64_t total = (p.total >= 0) ? p.total : __ldg(p.offsets + p.n_trials);
+    const int64_t total = (p.total >= 0) ? p.total : __ldg(p.offsets + p.n_trials) - __ldg(p.offsets);
 
     Lane L;
     TrialRow r;
@@ -579,6 +581,7 @@ static int run_single(const SingleCall &c) {
     p.offsets = c.offsets;
     p.n_trials = c.n_trials;
     p.total = c.offsets ? -1 : c.n_trials * c.n_samples;
+    p.k_base = (uint32_t)((c.launch && c.launch->first_trial > 0) ? c.launch->first_trial : 0);
     p.dt = c.dt;
     p.smooth = c.smooth ? 1 : 0;
     p.chunk = (c.launch && c.launch->chunk >= 32) ? c.launch->chunk : 64;

@@ -72,5 +72,6 @@ def workspace(nbytes: int, tag: int = 0, stream: torch.cuda.Stream | None = None
     return buf[off:off + max(int(nbytes), 256)]
 
 
-def launch_opts(block_threads: int = 0, blocks_per_sm: int = 0, chunk: int = 0) -> _lib.SsmLaunch:
-    return _lib.SsmLaunch(int(block_threads), int(blocks_per_sm), int(chunk))
+def launch_opts(block_threads: int = 0, blocks_per_sm: int = 0, chunk: int = 0,
+                first_trial: int = 0) -> _lib.SsmLaunch:
+    return _lib.SsmLaunch(int(block_threads), int(blocks_per_sm), int(chunk), int(first_trial))

@@ -18,6 +18,7 @@ from . import _device as D
 from . import _lib
 from . import boundary_functions as bf
 from . import device as dev
+from .tuning import launch_for
 
 # model name -> (simulator family, boundary name, boundary parameter names)
 BATCH_MODELS = {
@@ -81,6 +82,7 @@ class BatchedSimulator:
         self.choices = torch.empty(self.total, dtype=torch.int32, device="cuda")
         self.graph: torch.cuda.CUDAGraph | None = None
         self.last = None
+        self._streams = None
 
     def run(self, want_steps: bool = False, launch=None) -> dev.SimOutput:
         """Launch the batch on the current stream (asynchronous)."""
@@ -111,6 +113,72 @@ class BatchedSimulator:
         if self.graph is None:
             self.capture()
         self.graph.replay()
+
+    def window_bounds(self, chunks: int) -> np.ndarray:
+        """Trial boundaries of ``chunks`` windows holding about 1/2, 1/4, ... of
+        the trajectories (the last one the remainder): each window's output
+        copy overlaps the simulation of all later windows, and only the last,
+        smallest copy is left exposed."""
+        chunks = max(1, min(int(chunks), self.n_trials))
+        frac = np.cumsum([2.0 ** -(i + 1) for i in range(chunks - 1)])
+        b = np.searchsorted(self.offsets_host, frac * self.total, side="left")
+        return np.unique(np.concatenate([[0], b, [self.n_trials]])).astype(np.int64)
+
+    def run_to_host(self, rts_host: torch.Tensor, choices_host: torch.Tensor, *, chunks: int = 8) -> None:
+        """Simulate the batch and copy rts and choices into host tensors (pinned
+        memory lets the copies overlap the simulation).
+
+        The trials are cut into ``chunks`` windows (``window_bounds``).
+        Window i's outputs are copied on a copy stream while later
+        windows simulate, and consecutive windows alternate between two
+        compute streams, so one window's last trajectories share the GPU with
+        the next window's first ones.  Every window keeps the batch's
+        random-stream indices (``first_trial``), so the outputs are identical
+        to ``run()``.  Work queued on the current stream before the call (for
+        example copies of new parameters) is waited for; the call returns once
+        the host tensors hold the results.
+        """
+        if self.family == "ddm" and self.max_t_k is not None:
+            raise ValueError("per-trial max_t is supported by the flexible-bound families")
+        if rts_host.numel() < self.total or choices_host.numel() < self.total:
+            raise ValueError("host buffers must hold one slot per trajectory")
+        cur = torch.cuda.current_stream()
+        if self._streams is None:
+            self._streams = (torch.cuda.Stream(), torch.cuda.Stream(), torch.cuda.Stream())
+        cs0, cs1, copy_s = self._streams
+        bounds = self.window_bounds(chunks)
+        base = launch_for(self.family) if self.launch is None else self.launch
+        L = _lib.lib()
+        span = int(np.max(np.diff(bounds)))
+        for tag in (10, 11):  # reserve both workspaces before any window runs
+            D.workspace(L.ssm_ddm_workspace_bytes(span), tag=tag)
+        cs0.wait_stream(cur)
+        cs1.wait_stream(cur)
+        sl = lambda x, k0, k1: None if x is None else x[k0:k1]  # noqa: E731
+        for i in range(len(bounds) - 1):
+            k0, k1 = int(bounds[i]), int(bounds[i + 1])
+            o0, o1 = int(self.offsets_host[k0]), int(self.offsets_host[k1])
+            st = cs0 if i % 2 == 0 else cs1
+            lopt = _lib.SsmLaunch(base.block_threads, base.blocks_per_sm, base.chunk, k0)
+            with torch.cuda.stream(st):
+                dev.simulate_single(
+                    self.family, v=self.v[k0:k1], z=self.z[k0:k1], t=self.t[k0:k1],
+                    deadline=self.deadline[k0:k1], s=self.s[k0:k1], a=self.a[k0:k1],
+                    alpha=sl(self.alpha, k0, k1), n_trials=k1 - k0,
+                    sample_offsets=self.offsets[k0:k1 + 1], max_t=self.max_t,
+                    max_t_per_trial=sl(self.max_t_k, k0, k1), delta_t=self.delta_t,
+                    bound_kind=self.spec["kind"], bound_p1=sl(self.p1, k0, k1),
+                    bound_p2=sl(self.p2, k0, k1), bound_table=sl(self.table, k0, k1),
+                    seed=self.seed, smooth_unif=self.smooth, out_rts=self.rts,
+                    out_choices=self.choices, launch=lopt, stream=st, ws_tag=10 + i % 2)
+                done = torch.cuda.Event()
+                done.record(st)
+            copy_s.wait_event(done)
+            with torch.cuda.stream(copy_s):
+                rts_host[o0:o1].copy_(self.rts[o0:o1], non_blocking=True)
+                choices_host[o0:o1].copy_(self.choices[o0:o1], non_blocking=True)
+        copy_s.synchronize()
+        cur.wait_stream(copy_s)
 
     def to_host(self) -> tuple[np.ndarray, np.ndarray]:
         return self.rts.cpu().numpy(), self.choices.cpu().numpy()

@@ -44,12 +44,14 @@ def simulate_single(model: str, *, v, z, t, deadline, s, a=None, alpha=None,
                     noise_rows=None, noise_unif=None, want_steps: bool = False,
                     traj_len: int = 0, out_rts: torch.Tensor | None = None,
                     out_choices: torch.Tensor | None = None, launch=None,
-                    stream: torch.cuda.Stream | None = None) -> SimOutput:
+                    stream: torch.cuda.Stream | None = None, ws_tag: int = 0) -> SimOutput:
     """Simulate the single-accumulator family on the current CUDA device.
 
     ``sample_offsets`` (int64 [n_trials+1]) switches to the ragged layout where
     trial k owns outputs [offsets[k], offsets[k+1]); otherwise the output index
-    of (sample n, trial k) is n * n_trials + k as in the reference.
+    of (sample n, trial k) is n * n_trials + k as in the reference.  Calls that
+    may overlap on different streams need different ``ws_tag`` values (each
+    tag owns one cached workspace).
     """
     dev = D.require_cuda()
     K = int(n_trials)
@@ -95,7 +97,7 @@ def simulate_single(model: str, *, v, z, t, deadline, s, a=None, alpha=None,
         if nrows.numel() < total * nlen:
             raise ValueError("noise_rows must hold one row per trajectory")
     L = _lib.lib()
-    ws = D.workspace(L.ssm_ddm_workspace_bytes(K), tag=0, stream=stream)
+    ws = D.workspace(L.ssm_ddm_workspace_bytes(K), tag=ws_tag, stream=stream)
     if K == 0 or (offs is None and total == 0):
         # nothing to simulate (zero-length inputs map to null pointers)
         if traj is not None:
@@ -153,7 +155,9 @@ def simulate_race(model: str, *, v, z, t, s, deadline, n_trials: int, n_samples:
                   bound_kind: int = _lib.BOUND_CONSTANT, a=None, bound_p1=None, bound_p2=None,
                   bound_table=None, seed: int = 0, smooth_unif: bool = False, noise_rows=None,
                   noise_unif=None, want_steps: bool = False, traj_len: int = 0, total=None,
-                  launch=None, stream: torch.cuda.Stream | None = None) -> SimOutput:
+                  launch=None, stream: torch.cuda.Stream | None = None, ws_tag: int = 0,
+                  out_rts: torch.Tensor | None = None,
+                  out_choices: torch.Tensor | None = None) -> SimOutput:
     """race_model / lca on the GPU.  v, z, s: [n_trials, n_particles]; t: [n_trials]
     (or [n_trials, 1]); g, b: [n_trials] for lca."""
     dev = D.require_cuda()
@@ -180,8 +184,8 @@ def simulate_race(model: str, *, v, z, t, s, deadline, n_trials: int, n_samples:
     offs = _offsets(sample_offsets, K, dev)
     if total is None:
         total = int(offs[-1].item()) if offs is not None else K * int(n_samples)
-    rts = torch.empty(total, dtype=torch.float32, device=dev)
-    chs = torch.empty(total, dtype=torch.int32, device=dev)
+    rts = out_rts if out_rts is not None else torch.empty(total, dtype=torch.float32, device=dev)
+    chs = out_choices if out_choices is not None else torch.empty(total, dtype=torch.int32, device=dev)
     steps = torch.empty(total, dtype=torch.int32, device=dev) if want_steps else None
     traj = torch.empty(int(traj_len), dtype=torch.float32, device=dev) if traj_len > 0 else None
     nrows = nunif = None
@@ -193,7 +197,7 @@ def simulate_race(model: str, *, v, z, t, s, deadline, n_trials: int, n_samples:
         if nrows.numel() < total * nlen:
             raise ValueError("noise_rows must hold one row per trajectory")
     L = _lib.lib()
-    ws = D.workspace(L.ssm_race_workspace_bytes(K, n_part), tag=0, stream=stream)
+    ws = D.workspace(L.ssm_race_workspace_bytes(K, n_part), tag=ws_tag, stream=stream)
     if K == 0 or (offs is None and total == 0):
         if traj is not None:
             traj.fill_(-999.0)
