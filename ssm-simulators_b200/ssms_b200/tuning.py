@@ -6,7 +6,12 @@ atomic; with the ragged layout, a chunk of consecutive trajectories mostly
 belongs to one parameter vector, so it is also the lanes-per-theta grain).
 Results do not depend on them: the Philox stream of a trajectory is keyed by
 (seed, trial, sample) only.  Tuned values persist in ``_tuned.json`` next to
-this file and are looked up per model.
+this file and are looked up per simulator family (``ddm_flexbound``, ...).
+
+    python -m ssms_b200.tuning --model angle --persist
+
+tunes on the batched workload of the benchmark (4096 parameter vectors drawn
+from the model's bounds, n_samples ~ U{1000..20000}).
 """
 
 from __future__ import annotations
@@ -33,6 +38,11 @@ def _load() -> dict[str, dict]:
     return _cache
 
 
+# (block_threads, blocks_per_sm, chunk): CTA size, CTAs per SM (0 = as many as
+# fit) and the warp's claim size
+DEFAULT_CANDIDATES = [(bt, bps, ch) for bt in (128, 256) for bps in (0, 3) for ch in (32, 64, 128, 256)]
+
+
 def launch_for(model: str) -> _lib.SsmLaunch:
     cfg = _load().get(model, {})
     return _lib.SsmLaunch(int(cfg.get("block_threads", 0)), int(cfg.get("blocks_per_sm", 0)),
@@ -56,7 +66,7 @@ def autotune(model: str, run, candidates=None, repeats: int = 2, persist: bool =
     import torch
 
     if candidates is None:
-        candidates = [(bt, bps, ch) for bt in (128, 256) for bps in (0,) for ch in (32, 64, 128, 256)]
+        candidates = DEFAULT_CANDIDATES
     timings = []
     for bt, bps, ch in candidates:
         opt = _lib.SsmLaunch(bt, bps, ch)
@@ -76,3 +86,42 @@ def autotune(model: str, run, candidates=None, repeats: int = 2, persist: bool =
     set_launch(model, bt, bps, ch, persist=persist)
     return {"best": {"block_threads": bt, "blocks_per_sm": bps, "chunk": ch},
             "timings": timings, "when": time.time()}
+
+
+def tune_batched(model: str = "angle", n_theta: int = 4096, seed: int = 0, persist: bool = False,
+                 candidates=None, repeats: int = 2) -> dict:
+    """Autotune the persistent simulator of ``model`` (a batched single-accumulator
+    model: ddm, angle, weibull, levy, ...) on uneven n_samples and store the
+    winner under its simulator family."""
+    import numpy as np
+
+    from .batch import BATCH_MODELS, BatchedSimulator
+    from .config import model_config
+
+    cfg = model_config[model]
+    lo, hi = (np.asarray(b, np.float64) for b in cfg["param_bounds"])
+    rng = np.random.default_rng(seed)
+    theta = {k: rng.uniform(lo[i], hi[i], n_theta).astype(np.float32) for i, k in enumerate(cfg["params"])}
+    n_samples = rng.integers(1000, 20001, n_theta)
+    sim = BatchedSimulator(model, theta, n_samples, seed=seed, smooth_unif=True)
+    res = autotune(BATCH_MODELS[model][0], lambda opt: sim.run(launch=opt), candidates=candidates,
+                   repeats=repeats, persist=persist)
+    res["model"], res["family"], res["trajectories"] = model, BATCH_MODELS[model][0], sim.total
+    return res
+
+
+def main(argv=None) -> dict:
+    import argparse
+
+    ap = argparse.ArgumentParser(description="autotune the persistent simulators' launch configuration")
+    ap.add_argument("--model", default="angle")
+    ap.add_argument("--n-theta", type=int, default=4096)
+    ap.add_argument("--persist", action="store_true")
+    a = ap.parse_args(argv)
+    res = tune_batched(a.model, n_theta=a.n_theta, persist=a.persist)
+    print(json.dumps(res))
+    return res
+
+
+if __name__ == "__main__":
+    main()
