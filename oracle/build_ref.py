@@ -33,7 +33,8 @@ OUT_PKG = HERE / "_ref" / "cssm"
 BUILD = HERE / "_ref" / "_build"
 
 # Modules on the simulated hot path (plus the two they import at module level).
-MODULES = ["_utils", "_openmp_status", "ddm_models", "race_models", "levy_models", "lba_models"]
+MODULES = ["_utils", "_openmp_status", "ddm_models", "race_models", "levy_models", "lba_models",
+           "ornstein_models"]
 
 CXX_FLAGS = ["-O3", "-ffast-math", "-march=x86-64-v2", "-funroll-loops", "-fopenmp",
              "-fPIC", "-shared", "-DHAVE_OPENMP=1", "-w"]

@@ -161,6 +161,120 @@ int64_t oracle_ddm_trial(int64_t k, int64_t n_samples, int64_t n_trials, float v
 }
 
 /*
+ * One trial of ddm_sdv (variant 0; ddm_models.pyx:2612-2668) or full_ddm
+ * (variant 1; ddm_models.pyx:2233-2316): the flexible-bound DDM with a drift
+ * drawn per sample, v + sv * N(0,1), and for full_ddm a start point displaced
+ * by U(-sz, sz) and a non-decision time displaced by U(-st, st).
+ *
+ * Stream order per sample (full_ddm): the drift normal is read, the t and y
+ * uniforms are consumed, then the drift normal is consumed; ddm_sdv consumes
+ * its drift normal at once.  Row mode: row w = [drift normal, walk normals...];
+ * uniform row w (stride ustride) = [u_t, u_y, u_smooth] (full_ddm) or
+ * [u_smooth] (ddm_sdv).
+ */
+static inline float peek_g(oracle_noise *nz, int64_t w) {
+    if (nz->rows) return nz->rows[w * nz->row_len];
+    return nz->gbuf[nz->m];
+}
+static inline void advance_g(oracle_noise *nz, int64_t trial) {
+    if (nz->rows) return;
+    nz->m += 1;
+    if (nz->m == nz->gn) {
+        nz->refill_g(nz->gbuf, nz->gn, trial);
+        nz->m = 0;
+    }
+}
+static inline float next_u_at(oracle_noise *nz, int64_t w, int64_t ustride, int64_t j, int64_t trial) {
+    if (nz->rows) return nz->urows[w * ustride + j];
+    return next_u(nz, w, trial);
+}
+
+int64_t oracle_var_trial(int64_t k, int64_t n_samples, int64_t n_trials, int variant, float v,
+                         float z, float t, float sz, float sv, float st, float deadline,
+                         float sqrt_st, const float *bound, int64_t nb, float max_t, float dt,
+                         int smooth, oracle_noise *nz, float *rts, int32_t *choices,
+                         int32_t *steps, float *traj, int64_t traj_len) {
+    const float dl = deadline_tmp(max_t, deadline, t);
+    const int64_t ustride = variant ? 3 : 1;
+    int64_t total_steps = 0;
+    for (int64_t n = 0; n < n_samples; ++n) {
+        const int64_t w = n * n_trials + k;
+        float y = (float)((-1.0 * (double)bound[0]) + (((double)z * 2.0) * (double)bound[0]));
+        const float drift = (v + (sv * peek_g(nz, w))) * dt;
+        float t_tmp = t;
+        if (variant) {
+            /* t + 2 (u - 0.5) st and y + 2 (u - 0.5) sz, in double as the generated C */
+            const float ut = next_u_at(nz, w, ustride, 0, k);
+            t_tmp = (float)((double)t + ((2.0 * ((double)ut - 0.5)) * (double)st));
+            const float uy = next_u_at(nz, w, ustride, 1, k);
+            y = (float)((double)y + ((2.0 * ((double)uy - 0.5)) * (double)sz));
+        }
+        advance_g(nz, k);
+        float tp = 0.0f;
+        int64_t ix = 0;
+        const int rec = (traj != 0 && n == 0 && k == 0);
+        if (rec && traj_len > 0) traj[0] = y;
+        for (;;) {
+            const float b = bound[ix < nb ? ix : nb - 1];
+            if (!((y >= (-1.0 * (double)b)) && (y <= b) && (tp <= dl))) break;
+            const float g = next_g(nz, w, ix + 1, k);
+            y = (y + drift) + (sqrt_st * g);
+            tp = tp + dt;
+            ix += 1;
+            if (rec && ix < traj_len) traj[ix] = y;
+        }
+        const float u = next_u_at(nz, w, ustride, ustride - 1, k);
+        const float sm = smooth_jitter(smooth, tp, dl, dt, u);
+        float rt = (tp + t_tmp) + sm;
+        if (rt >= deadline || deadline <= 0) rt = -999.0f;
+        rts[w] = rt;
+        choices[w] = sign_f(y);
+        if (steps) steps[w] = (int32_t)ix;
+        total_steps += ix;
+    }
+    return total_steps;
+}
+
+/*
+ * One trial of ornstein_uhlenbeck (src/cssm/ornstein_models.pyx:157-199):
+ * y += (v - g y) dt + sqrt(dt) s N(0,1) between the boundaries +-b(t).
+ */
+int64_t oracle_ou_trial(int64_t k, int64_t n_samples, int64_t n_trials, float v, float z, float g,
+                        float t, float deadline, float sqrt_st, const float *bound, int64_t nb,
+                        float max_t, float dt, int smooth, oracle_noise *nz, float *rts,
+                        int32_t *choices, int32_t *steps, float *traj, int64_t traj_len) {
+    const float dl = deadline_tmp(max_t, deadline, t);
+    int64_t total_steps = 0;
+    for (int64_t n = 0; n < n_samples; ++n) {
+        const int64_t w = n * n_trials + k;
+        /* (-1) * b0 + z * 2 * b0: all float in the generated C (int literals) */
+        float y = (-bound[0]) + ((z * 2.0f) * bound[0]);
+        float tp = 0.0f;
+        int64_t ix = 0;
+        const int rec = (traj != 0 && n == 0 && k == 0);
+        if (rec && traj_len > 0) traj[0] = y;
+        for (;;) {
+            const float b = bound[ix < nb ? ix : nb - 1];
+            if (!((y >= (-1.0 * (double)b)) && (y <= b) && (tp <= dl))) break;
+            const float gm = next_g(nz, w, ix, k);
+            y = (y + ((v - (g * y)) * dt)) + (sqrt_st * gm);
+            tp = tp + dt;
+            ix += 1;
+            if (rec && ix < traj_len) traj[ix] = y;
+        }
+        const float u = next_u(nz, w, k);
+        const float sm = smooth_jitter(smooth, tp, dl, dt, u);
+        float rt = (tp + t) + sm;
+        if (rt >= deadline || deadline <= 0) rt = -999.0f;
+        rts[w] = rt;
+        choices[w] = sign_f(y);
+        if (steps) steps[w] = (int32_t)ix;
+        total_steps += ix;
+    }
+    return total_steps;
+}
+
+/*
  * One trial of race_model (race_models.pyx:417-464) or lca
  * (race_models.pyx:825-879), selected by `lca`.  v, z, sqrt_st hold the
  * trial's np particle values; increments are consumed particle-major within a

@@ -66,6 +66,12 @@ def lib():
         L.oracle_race_trial.restype = I64
         L.oracle_race_trial.argtypes = [I64, I64, I64, I, I, P, P, P, F, F, F, F, P, I64, F, F, I,
                                         NP, P, P, P, P, I64]
+        L.oracle_var_trial.restype = I64
+        L.oracle_var_trial.argtypes = [I64, I64, I64, I, F, F, F, F, F, F, F, F, P, I64, F, F, I, NP,
+                                       P, P, P, P, I64]
+        L.oracle_ou_trial.restype = I64
+        L.oracle_ou_trial.argtypes = [I64, I64, I64, F, F, F, F, F, F, P, I64, F, F, I, NP, P, P, P, P,
+                                      I64]
         L.oracle_lba_f32.restype = None
         L.oracle_lba_f32.argtypes = [I64, I64, I, P, P, P, P, P, P, P]
         _lib = L
@@ -212,6 +218,61 @@ def flex(model, v, z, t, deadline, s, *, max_t, delta_t, n_samples, n_trials, bo
         L.oracle_flex_trial(k, n_samples, n_trials, v[k], z[k], t[k], deadline[k], scales[k],
                             _p(tab), tab.shape[0], f32(max_t), f32(delta_t), int(bool(smooth_unif)),
                             C.byref(nz), _p(rts), _p(chs), _p(steps), _p(traj), traj_len)
+    if rows is not None and nz.overrun:
+        raise ValueError("noise rows too short for the simulated trajectories")
+    del keep
+    return rts, chs, steps, traj
+
+
+def ddm_variability(model, v, z, t, sz, sv, st, deadline, s, *, max_t, delta_t, n_samples, n_trials,
+                    boundary_fun, boundary_params, smooth_unif, random_state=None, rows=None, unif=None,
+                    traj_len=0):
+    """full_ddm / ddm_sdv (stream or row mode).  Row mode: rows[w] = [drift
+    normal, walk normals...]; unif[w] = [u_t, u_y, u_smooth] (full_ddm) or
+    [u_smooth] (ddm_sdv).  ddm_sdv ignores sz and st."""
+    L = lib()
+    variant = {"ddm_sdv": 0, "full_ddm": 1}[model]
+    v, z, t, sz, sv, st_, deadline, s = (np.asarray(x, np.float32) for x in (v, z, t, sz, sv, st, deadline, s))
+    nd = num_draws(max_t, delta_t)
+    t_s = t_grid(max_t, delta_t)
+    if rows is None:
+        strm = _Stream(random_state, _normal_init(nd), _normal_refill)
+        nz, keep = strm.noise, strm
+    else:
+        nz, keep = _rows_noise(rows, unif)
+    rts, chs, steps = _outputs(n_samples, n_trials)
+    traj = np.full(traj_len, -999, np.float32) if traj_len else None
+    scales = (sqrt_dt(delta_t) * s).astype(np.float32)
+    for k, tab in enumerate(_bound_tables(boundary_fun, boundary_params, n_trials, t_s)):
+        L.oracle_var_trial(k, n_samples, n_trials, variant, v[k], z[k], t[k], sz[k], sv[k], st_[k],
+                           deadline[k], scales[k], _p(tab), tab.shape[0], f32(max_t), f32(delta_t),
+                           int(bool(smooth_unif)), C.byref(nz), _p(rts), _p(chs), _p(steps), _p(traj),
+                           traj_len)
+    if rows is not None and nz.overrun:
+        raise ValueError("noise rows too short for the simulated trajectories")
+    del keep
+    return rts, chs, steps, traj
+
+
+def ornstein(v, z, g, t, deadline, s, *, max_t, delta_t, n_samples, n_trials, boundary_fun,
+             boundary_params, smooth_unif, random_state=None, rows=None, unif=None, traj_len=0):
+    """ornstein_uhlenbeck (stream or row mode)."""
+    L = lib()
+    v, z, g, t, deadline, s = (np.asarray(x, np.float32) for x in (v, z, g, t, deadline, s))
+    nd = num_draws(max_t, delta_t)
+    t_s = t_grid(max_t, delta_t)
+    if rows is None:
+        strm = _Stream(random_state, _normal_init(nd), _normal_refill)
+        nz, keep = strm.noise, strm
+    else:
+        nz, keep = _rows_noise(rows, unif)
+    rts, chs, steps = _outputs(n_samples, n_trials)
+    traj = np.full(traj_len, -999, np.float32) if traj_len else None
+    scales = (sqrt_dt(delta_t) * s).astype(np.float32)
+    for k, tab in enumerate(_bound_tables(boundary_fun, boundary_params, n_trials, t_s)):
+        L.oracle_ou_trial(k, n_samples, n_trials, v[k], z[k], g[k], t[k], deadline[k], scales[k],
+                          _p(tab), tab.shape[0], f32(max_t), f32(delta_t), int(bool(smooth_unif)),
+                          C.byref(nz), _p(rts), _p(chs), _p(steps), _p(traj), traj_len)
     if rows is not None and nz.overrun:
         raise ValueError("noise rows too short for the simulated trajectories")
     del keep

@@ -96,3 +96,36 @@ def test_timeout_rt_is_float32_accumulated_time(oracle):
     assert steps[0] == 20000
     assert abs(float(rts[0]) - 20.000637) < 2e-6
     assert chs[0] == 0  # sign(0) at y = 0
+
+
+@pytest.mark.parametrize("name", ["full_ddm_constant", "full_ddm_angle", "ddm_sdv_constant"])
+def test_variability_models_match_reference(oracle, name):
+    g = _load(name)
+    theta = {k[len("theta_"):]: g[k] for k in g if k.startswith("theta_")}
+    n, K = int(g["n"]), theta["v"].shape[0]
+    zero = np.zeros(K, np.float32)
+    bp = {k: theta[k] for k in [str(x) for x in g["bkeys"]]}
+    rts, chs, steps, traj = oracle.ddm_variability(
+        str(g["model"]), theta["v"], theta["z"], theta["t"], theta.get("sz", zero), theta["sv"],
+        theta.get("st", zero), g["deadline"], g["s"], max_t=float(g["max_t"]), delta_t=float(g["dt"]),
+        n_samples=n, n_trials=K, boundary_fun=BOUNDS[str(g["boundary"])], boundary_params=bp,
+        smooth_unif=bool(g["smooth"]), random_state=int(g["seed"]), traj_len=g["trajectory"].shape[0])
+    np.testing.assert_array_equal(_bits(rts), _bits(g["rts"].reshape(-1)))
+    np.testing.assert_array_equal(chs, g["choices"].reshape(-1).astype(np.int32))
+    np.testing.assert_array_equal(_bits(traj), _bits(g["trajectory"][:, 0]))
+
+
+@pytest.mark.parametrize("name", ["ornstein_constant", "ornstein_angle"])
+def test_ornstein_matches_reference(oracle, name):
+    g = _load(name)
+    theta = {k[len("theta_"):]: g[k] for k in g if k.startswith("theta_")}
+    n, K = int(g["n"]), theta["v"].shape[0]
+    bp = {k: theta[k] for k in [str(x) for x in g["bkeys"]]}
+    rts, chs, steps, traj = oracle.ornstein(
+        theta["v"], theta["z"], theta["g"], theta["t"], g["deadline"], g["s"], max_t=float(g["max_t"]),
+        delta_t=float(g["dt"]), n_samples=n, n_trials=K, boundary_fun=BOUNDS[str(g["boundary"])],
+        boundary_params=bp, smooth_unif=bool(g["smooth"]), random_state=int(g["seed"]),
+        traj_len=g["trajectory"].shape[0])
+    np.testing.assert_array_equal(_bits(rts), _bits(g["rts"].reshape(-1)))
+    np.testing.assert_array_equal(chs, g["choices"].reshape(-1).astype(np.int32))
+    np.testing.assert_array_equal(_bits(traj), _bits(g["trajectory"][:, 0]))
