@@ -138,6 +138,55 @@ int ssm_levy_flexbound(const float *v, const float *a, const float *z, const flo
                        const ssm_launch *launch, void *workspace, size_t workspace_bytes,
                        void *stream);
 
+/*
+ * ssm_ddm_sdv -- replaces cssm.ddm_sdv (src/cssm/ddm_models.pyx:2500-2797):
+ * ddm_flexbound with the drift drawn per trajectory, v + sv * N(0,1).
+ * Noise injection: row w = [drift normal, walk normals...] (noise_row_len >=
+ * 1 + steps), noise_unif[w] = the jitter uniform.
+ */
+int ssm_ddm_sdv(const float *v, const float *a, const float *z, const float *t, const float *sv,
+                const float *deadline, const float *s, int64_t n_trials, int64_t n_samples,
+                const int64_t *sample_offsets, float max_t, float delta_t, int bound_kind,
+                const float *bound_p1, const float *bound_p2, const float *bound_table,
+                int64_t table_stride, int64_t table_len, uint64_t seed, int smooth_unif,
+                const float *noise_rows, int64_t noise_row_len, const float *noise_unif, float *rts,
+                int32_t *choices, int32_t *steps, float *traj, int64_t traj_len,
+                const ssm_launch *launch, void *workspace, size_t workspace_bytes, void *stream);
+
+/*
+ * ssm_full_ddm -- replaces cssm.full_ddm (src/cssm/ddm_models.pyx:2177-2497):
+ * as ssm_ddm_sdv, plus a start point displaced by U(-sz, sz) and a
+ * non-decision time displaced by U(-st, st) per trajectory (the deadline
+ * horizon still uses t).  Noise injection: rows as ssm_ddm_sdv; three
+ * uniforms per trajectory, noise_unif[3w .. 3w+2] = [u_t, u_y, u_jitter].
+ */
+int ssm_full_ddm(const float *v, const float *a, const float *z, const float *t, const float *sz,
+                 const float *sv, const float *st, const float *deadline, const float *s,
+                 int64_t n_trials, int64_t n_samples, const int64_t *sample_offsets, float max_t,
+                 float delta_t, int bound_kind, const float *bound_p1, const float *bound_p2,
+                 const float *bound_table, int64_t table_stride, int64_t table_len, uint64_t seed,
+                 int smooth_unif, const float *noise_rows, int64_t noise_row_len,
+                 const float *noise_unif, float *rts, int32_t *choices, int32_t *steps, float *traj,
+                 int64_t traj_len, const ssm_launch *launch, void *workspace,
+                 size_t workspace_bytes, void *stream);
+
+/*
+ * ssm_ornstein_uhlenbeck -- replaces cssm.ornstein_uhlenbeck
+ * (src/cssm/ornstein_models.pyx:47-330): y += (v - g y) dt + sqrt(dt) s N(0,1)
+ * between +-b(t).  `a` is the boundary height (the reference passes it in
+ * boundary_params).  Layout and noise conventions as ssm_ddm_flexbound.
+ */
+int ssm_ornstein_uhlenbeck(const float *v, const float *a, const float *z, const float *g,
+                           const float *t, const float *deadline, const float *s, int64_t n_trials,
+                           int64_t n_samples, const int64_t *sample_offsets, float max_t,
+                           float delta_t, int bound_kind, const float *bound_p1,
+                           const float *bound_p2, const float *bound_table, int64_t table_stride,
+                           int64_t table_len, uint64_t seed, int smooth_unif,
+                           const float *noise_rows, int64_t noise_row_len, const float *noise_unif,
+                           float *rts, int32_t *choices, int32_t *steps, float *traj,
+                           int64_t traj_len, const ssm_launch *launch, void *workspace,
+                           size_t workspace_bytes, void *stream);
+
 /* ---- multi-accumulator race / LCA --------------------------------------- */
 
 /* Bytes of scratch ssm_race_model / ssm_lca need. */

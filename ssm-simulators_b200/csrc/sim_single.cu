@@ -32,10 +32,13 @@
 
 namespace ssm {
 
-enum Model { M_FLEX = 0, M_LEGACY = 1, M_LEVY = 2 };
+// M_SDV: ddm_sdv (drift v + sv N(0,1) per trajectory); M_FULL: full_ddm (and
+// start point + U(-sz, sz), non-decision time + U(-st, st)); M_OU:
+// ornstein_uhlenbeck (drift v - g y).
+enum Model { M_FLEX = 0, M_LEGACY = 1, M_LEVY = 2, M_SDV = 3, M_FULL = 4, M_OU = 5 };
 
 struct alignas(16) TrialRow {
-    float drift;     // v * dt
+    float drift;     // v * dt ; SDV/FULL: v
     float scale;     // sqrt(dt) * s ;  Levy: s * dt^(1/alpha)
     float y0;        // start point
     float dl_tmp;    // min(max_t, deadline - t): the walk runs while t <= dl_tmp
@@ -46,9 +49,9 @@ struct alignas(16) TrialRow {
     float p2;        // WEIBULL: scale beta
     float dtp1;      // dt * p1 (linear boundary per step, fast path)
     float inv_beta;  // 1 / beta
-    float alpha;     // Levy stability index
-    float inv_alpha; // 1 / alpha
-    float expo;      // (1 - alpha) / alpha
+    float alpha;     // Levy: stability index ; SDV/FULL: sv ; OU: v
+    float inv_alpha; // Levy: 1 / alpha ; FULL: sz ; OU: g
+    float expo;      // Levy: (1 - alpha) / alpha ; FULL: st ; OU: 1 - g dt
     float capf;      // hard limit on Euler steps: a walk reaching it raises SSM_ERR_DEVICE
     float c2;        // -2 ln(2) * scale^2: folds the noise scale into Box-Muller's radius
 };
@@ -61,6 +64,7 @@ struct SingleParams {
     int64_t n_trials;
     int64_t total;           // number of trajectories; -1 = offsets[n_trials] - offsets[0]
     uint32_t k_base;         // random-stream index of trial 0 (trial windows of a larger batch)
+    int ustride;             // injected uniforms per trajectory (3 for full_ddm: u_t, u_y, u_smooth)
     float dt;
     int smooth;
     int chunk;
@@ -79,6 +83,7 @@ struct SingleParams {
 
 struct PrepArgs {
     const float *v, *a, *z, *t, *deadline, *s, *alpha, *p1, *p2, *maxt_k, *table;
+    const float *sv, *sz, *st, *g;  // variability (SDV/FULL) and leak (OU) parameters
     int64_t n_trials, tstride;
     float dt, sqrt_dt, max_t;
     int model, bound;
@@ -105,6 +110,16 @@ __global__ void k_prep(const PrepArgs A) {
     r.alpha = A.alpha ? A.alpha[k] : 2.f;
     r.inv_alpha = (float)(1.0 / (double)r.alpha);
     r.expo = (float)((1.0 - (double)r.alpha) / (double)r.alpha);
+    if (A.model == M_SDV || A.model == M_FULL) {
+        r.drift = A.v[k];  // the drift increment (v + sv g) dt is drawn per trajectory
+        r.alpha = A.sv[k];
+        r.inv_alpha = (A.model == M_FULL) ? A.sz[k] : 0.f;
+        r.expo = (A.model == M_FULL) ? A.st[k] : 0.f;
+    } else if (A.model == M_OU) {
+        r.alpha = A.v[k];
+        r.inv_alpha = A.g[k];
+        r.expo = 1.0f - A.g[k] * dt;
+    }
     // The walk stops once the float32 time passes dl_tmp, i.e. after about
     // dl_tmp/dt steps; twice that plus slack bounds every legal walk.  A stalled
     // accumulator (dt below half an ulp of t) or an infinite horizon hits the cap.
@@ -121,6 +136,10 @@ __global__ void k_prep(const PrepArgs A) {
     r.c2 = -1.3862944f * r.scale * r.scale;
     if (A.model == M_LEGACY) {
         r.y0 = __fmul_rn(A.z[k], r.a);  // ddm_models.pyx:451
+    } else if (A.model == M_OU) {
+        // (-1) * b0 + z * 2 * b0 with integer literals: float arithmetic (ornstein_models.pyx:167)
+        const float b0 = (A.bound == SSM_BOUND_TABLE) ? A.table[k * A.tstride] : r.a;
+        r.y0 = __fadd_rn(-b0, __fmul_rn(__fmul_rn(A.z[k], 2.0f), b0));
     } else {
         const float b0 = (A.bound == SSM_BOUND_TABLE) ? A.table[k * A.tstride] : r.a;
         // -b0 + z*2*b0, evaluated in double as the generated C does (ddm_models.pyx:709)
@@ -239,7 +258,11 @@ struct Lane {
     uint32_t k, n, blk;
     int ix;           // steps taken (maintained where an integer index is needed)
     float y, tp, ixf; // position, float32 time accumulator, steps taken as float
+    float dinc;       // SDV/FULL: this trajectory's drift increment (v + sv g) dt
 };
+
+// models whose drift is drawn once per trajectory
+template <int MODEL> struct DrawnDrift { static constexpr bool value = (MODEL == M_SDV || MODEL == M_FULL); };
 
 // Box-Muller pair already scaled into Euler increments: drift + scale * N(0,1).
 // c2 = -2 ln(2) scale^2, so r = sqrt(c2 * log2(u1)) = scale * sqrt(-2 ln u1).
@@ -263,9 +286,11 @@ template <int MODEL, bool NOISE>
 __device__ __forceinline__ void draw_block(const SingleParams &p, const Lane &L, const TrialRow &r,
                                            float g[BLK]) {
     if (NOISE) {
-        const float *row = p.noise + L.w * p.nlen;
+        // SDV/FULL rows start with the trajectory's drift normal
+        constexpr int OFF = DrawnDrift<MODEL>::value ? 1 : 0;
+        const float *row = p.noise + L.w * p.nlen + OFF;
 #pragma unroll
-        for (int q = 0; q < BLK; ++q) g[q] = (L.ix + q < p.nlen) ? __ldg(row + L.ix + q) : 0.f;
+        for (int q = 0; q < BLK; ++q) g[q] = (L.ix + OFF + q < p.nlen) ? __ldg(row + L.ix + q) : 0.f;
     } else if (MODEL == M_LEVY) {
 #pragma unroll
         for (int h = 0; h < BLK / 2; h += 2) {
@@ -277,12 +302,13 @@ __device__ __forceinline__ void draw_block(const SingleParams &p, const Lane &L,
             g[2 * h + 3] = fmaf(r.scale, cms_stable(c.z, c.w, r), r.drift);
         }
     } else {
+        const float drift = DrawnDrift<MODEL>::value ? L.dinc : r.drift;
         const uint4 b0 = philox10(make_uint4(2u * L.blk, L.n, L.k + p.k_base, 0u), p.key);
         const uint4 b1 = philox10(make_uint4(2u * L.blk + 1u, L.n, L.k + p.k_base, 0u), p.key);
-        bm_increment(b0.x, b0.y, r.c2, r.drift, g[0], g[1]);
-        bm_increment(b0.z, b0.w, r.c2, r.drift, g[2], g[3]);
-        bm_increment(b1.x, b1.y, r.c2, r.drift, g[4], g[5]);
-        bm_increment(b1.z, b1.w, r.c2, r.drift, g[6], g[7]);
+        bm_increment(b0.x, b0.y, r.c2, drift, g[0], g[1]);
+        bm_increment(b0.z, b0.w, r.c2, drift, g[2], g[3]);
+        bm_increment(b1.x, b1.y, r.c2, drift, g[4], g[5]);
+        bm_increment(b1.z, b1.w, r.c2, drift, g[6], g[7]);
     }
 }
 
@@ -308,17 +334,25 @@ __device__ __forceinline__ bool step_block(const SingleParams &p, Lane &L, const
             const float b = bound_at<BOUND, NOISE>(r, L.ixf, L.ix, p, L.k);
             inside = live && (fabsf(L.y) <= b) && (L.tp <= r.dl_tmp);
         }
-        if (NOISE && inside && L.ix >= p.nlen) {
+        if (NOISE && inside && L.ix + (DrawnDrift<MODEL>::value ? 1 : 0) >= p.nlen) {
             raise_error(p.hdr, SSM_ERR_NOISE_RANGE, (int)L.w);
             inside = false;
         }
         if (inside) {
             if (NOISE) {
-                // (y + v*dt) + scale*g: the association the reference build uses
-                L.y = __fadd_rn(__fadd_rn(L.y, r.drift), __fmul_rn(r.scale, g[q]));
+                if (MODEL == M_OU) {
+                    // (y + (v - g y) dt) + scale*g (ornstein_models.pyx:177)
+                    const float lk = __fmul_rn(__fsub_rn(r.alpha, __fmul_rn(r.inv_alpha, L.y)), p.dt);
+                    L.y = __fadd_rn(__fadd_rn(L.y, lk), __fmul_rn(r.scale, g[q]));
+                } else {
+                    // (y + v*dt) + scale*g: the association the reference build uses
+                    const float dr = DrawnDrift<MODEL>::value ? L.dinc : r.drift;
+                    L.y = __fadd_rn(__fadd_rn(L.y, dr), __fmul_rn(r.scale, g[q]));
+                }
                 L.tp = __fadd_rn(L.tp, p.dt);
             } else {
-                L.y += g[q];
+                if (MODEL == M_OU) L.y = fmaf(L.y, r.expo, g[q]);  // y (1 - g dt) + v dt + noise
+                else L.y += g[q];
                 L.tp += p.dt;
             }
             L.ixf += 1.0f;
@@ -330,21 +364,29 @@ __device__ __forceinline__ bool step_block(const SingleParams &p, Lane &L, const
     return live;
 }
 
-template <bool NOISE>
+template <int MODEL, bool NOISE>
 __device__ __forceinline__ void finalize(const SingleParams &p, const Lane &L) {
     // fields needed only here are re-read instead of being held across the walk
     const TrialRow *row = p.rows + L.k;
     const float t = __ldg(&row->t), deadline = __ldg(&row->deadline), dl = __ldg(&row->dl_tmp);
     float u;
-    if (NOISE) u = __ldg(p.nunif + L.w);
+    if (NOISE) u = __ldg(p.nunif + L.w * p.ustride + (p.ustride - 1));
     else u = uniform_co(philox10(make_uint4(0u, L.n, L.k + p.k_base, 1u), p.key).x);
+    float tt = t;
+    if (MODEL == M_FULL) {
+        // t + 2 (u - 0.5) st in double (ddm_models.pyx:2253); the same uniform as at the start
+        float ut;
+        if (NOISE) ut = __ldg(p.nunif + L.w * p.ustride);
+        else ut = uniform_co(philox10(make_uint4(0u, L.n, L.k + p.k_base, 3u), p.key).z);
+        tt = __double2float_rn((double)t + (2.0 * ((double)ut - 0.5)) * (double)__ldg(&row->expo));
+    }
     // compute_smooth_unif (_utils.pyx:668-695): double arithmetic, float result
     float sm = 0.f;
     if (p.smooth) {
         if (L.tp == 0.f) sm = __double2float_rn(((double)u * 0.5) * (double)p.dt);
         else if (L.tp < dl) sm = __double2float_rn((0.5 - (double)u) * (double)p.dt);
     }
-    float rt = __fadd_rn(__fadd_rn(L.tp, t), sm);
+    float rt = __fadd_rn(__fadd_rn(L.tp, tt), sm);
     if (rt >= deadline || deadline <= 0.f) rt = -999.f;  // enforce_deadline
     const int choice = (L.y > 0.f) - (L.y < 0.f);         // sign(y)
     p.rts[L.w] = rt;
@@ -352,6 +394,7 @@ __device__ __forceinline__ void finalize(const SingleParams &p, const Lane &L) {
     if (p.steps) p.steps[L.w] = (int)L.ixf;
 }
 
+template <int MODEL, bool NOISE>
 __device__ __forceinline__ void lane_init(const SingleParams &p, Lane &L, TrialRow &r, int64_t w,
                                           int64_t &hint) {
     int64_t k, n;
@@ -376,6 +419,22 @@ __device__ __forceinline__ void lane_init(const SingleParams &p, Lane &L, TrialR
     L.ixf = 0.f;
     L.tp = 0.f;
     L.y = r.y0;
+    if (DrawnDrift<MODEL>::value) {
+        // per-trajectory drift normal and (full_ddm) start-point uniform
+        // (ddm_models.pyx:2249-2266): injected, or drawn from the trajectory's stream
+        float g0, uy = 0.5f;
+        if (NOISE) {
+            g0 = __ldg(p.noise + L.w * p.nlen);
+            if (MODEL == M_FULL) uy = __ldg(p.nunif + L.w * p.ustride + 1);
+        } else {
+            const uint4 b = philox10(make_uint4(0u, L.n, L.k + p.k_base, 3u), p.key);
+            g0 = box_muller(b.x, b.y).x;
+            uy = uniform_co(b.w);
+        }
+        L.dinc = __fmul_rn(__fadd_rn(r.drift, __fmul_rn(r.alpha, g0)), p.dt);
+        if (MODEL == M_FULL)
+            L.y = __double2float_rn((double)L.y + (2.0 * ((double)uy - 0.5)) * (double)r.inv_alpha);
+    }
 }
 
 // ------------------------------------------------------------------ main kernel
@@ -388,7 +447,7 @@ __global__ void __launch_bounds__(256, SSM_MIN_CTAS) k_single(const __grid_const
 
     Lane L;
     TrialRow r;
-    L.w = 0; L.k = L.n = L.blk = 0; L.ix = 0; L.y = L.tp = L.ixf = 0.f;
+    L.w = 0; L.k = L.n = L.blk = 0; L.ix = 0; L.y = L.tp = L.ixf = L.dinc = 0.f;
     bool active = false;
     bool exhausted = false;
     int64_t q_next = 0, q_end = 0, hint = 0;
@@ -409,7 +468,7 @@ __global__ void __launch_bounds__(256, SSM_MIN_CTAS) k_single(const __grid_const
                 const int rank = __popc(need & lt_mask);
                 const int64_t w = (rank < avail) ? q_next + rank : base + (rank - avail);
                 if (w < total) {
-                    lane_init(p, L, r, w, hint);
+                    lane_init<MODEL, NOISE>(p, L, r, w, hint);
                     active = true;
                 }
             }
@@ -427,7 +486,7 @@ __global__ void __launch_bounds__(256, SSM_MIN_CTAS) k_single(const __grid_const
             const bool live = step_block<MODEL, BOUND, NOISE, false>(p, L, r, g);
             L.blk += 1;
             if (!live) {
-                finalize<NOISE>(p, L);
+                finalize<MODEL, NOISE>(p, L);
                 active = false;
             }
         }
@@ -444,7 +503,7 @@ __global__ void k_record(const __grid_constant__ SingleParams p) {
     Lane L;
     TrialRow r;
     int64_t hint = 0;
-    lane_init(p, L, r, 0, hint);
+    lane_init<MODEL, NOISE>(p, L, r, 0, hint);
     if (p.traj_len > 0) p.traj[0] = L.y;
     for (;;) {
         float g[BLK];
@@ -514,6 +573,7 @@ static size_t single_ws_bytes(int64_t n_trials) {
 struct SingleCall {
     int model;
     const float *v, *a, *z, *alpha, *t, *deadline, *s;
+    const float *sv, *sz, *st, *g;
     int64_t n_trials, n_samples;
     const int64_t *offsets;
     float max_t;
@@ -546,6 +606,9 @@ static int run_single(const SingleCall &c) {
     SSM_REQUIRE((c.rts && c.choices) || (!c.offsets && c.n_trials * c.n_samples == 0),
                 "rts and choices outputs are required");
     SSM_REQUIRE(c.model != M_LEVY || c.alpha, "alpha is required for the Levy model");
+    SSM_REQUIRE((c.model != M_SDV && c.model != M_FULL) || c.sv, "sv is required");
+    SSM_REQUIRE(c.model != M_FULL || (c.sz && c.st), "sz and st are required");
+    SSM_REQUIRE(c.model != M_OU || c.g, "g is required for the Ornstein-Uhlenbeck model");
     if (c.model != M_LEGACY) {
         SSM_REQUIRE(c.bound >= SSM_BOUND_TABLE && c.bound <= SSM_BOUND_WEIBULL, "unknown boundary kind %d", c.bound);
         SSM_REQUIRE(c.bound != SSM_BOUND_LINEAR || c.p1, "linear boundary needs bound_p1");
@@ -569,6 +632,7 @@ static int run_single(const SingleCall &c) {
     PrepArgs A;
     A.v = c.v; A.a = c.a; A.z = c.z; A.t = c.t; A.deadline = c.deadline; A.s = c.s;
     A.alpha = c.alpha; A.p1 = c.p1; A.p2 = c.p2; A.maxt_k = c.maxt_k; A.table = c.table;
+    A.sv = c.sv; A.sz = c.sz; A.st = c.st; A.g = c.g;
     A.n_trials = c.n_trials; A.tstride = c.tstride; A.dt = c.dt;
     A.sqrt_dt = (float)sqrt((double)c.dt);  // setup_simulation: sqrt(delta_t) -> float
     A.max_t = c.max_t; A.model = c.model; A.bound = c.bound; A.rows = rows;
@@ -582,6 +646,7 @@ static int run_single(const SingleCall &c) {
     p.n_trials = c.n_trials;
     p.total = c.offsets ? -1 : c.n_trials * c.n_samples;
     p.k_base = (uint32_t)((c.launch && c.launch->first_trial > 0) ? c.launch->first_trial : 0);
+    p.ustride = (c.model == M_FULL) ? 3 : 1;
     p.dt = c.dt;
     p.smooth = c.smooth ? 1 : 0;
     p.chunk = (c.launch && c.launch->chunk >= 32) ? c.launch->chunk : 64;
@@ -600,6 +665,9 @@ static int run_single(const SingleCall &c) {
     switch (c.model) {
         case M_FLEX: return Launcher::dispatch<M_FLEX>(c.bound, noise, p, c.launch, st);
         case M_LEGACY: return Launcher::dispatch<M_LEGACY>(c.bound, noise, p, c.launch, st);
+        case M_SDV: return Launcher::dispatch<M_SDV>(c.bound, noise, p, c.launch, st);
+        case M_FULL: return Launcher::dispatch<M_FULL>(c.bound, noise, p, c.launch, st);
+        case M_OU: return Launcher::dispatch<M_OU>(c.bound, noise, p, c.launch, st);
         default: return Launcher::dispatch<M_LEVY>(c.bound, noise, p, c.launch, st);
     }
 }
@@ -620,7 +688,8 @@ int ssm_ddm_flexbound(const float *v, const float *a, const float *z, const floa
                       int32_t *choices, int32_t *steps, float *traj, int64_t traj_len,
                       const ssm_launch *launch, void *workspace, size_t workspace_bytes,
                       void *stream) {
-    ssm::SingleCall c{ssm::M_FLEX, v, a, z, nullptr, t, deadline, s, n_trials, n_samples,
+    ssm::SingleCall c{ssm::M_FLEX, v, a, z, nullptr, t, deadline, s, nullptr, nullptr, nullptr, nullptr,
+                      n_trials, n_samples,
                       sample_offsets, max_t, max_t_per_trial, delta_t, bound_kind, bound_p1,
                       bound_p2, bound_table, table_stride, table_len, seed, smooth_unif,
                       noise_rows, noise_row_len, noise_unif, rts, choices, steps, traj,
@@ -635,7 +704,8 @@ int ssm_ddm(const float *v, const float *a, const float *z, const float *t, cons
             const float *noise_unif, float *rts, int32_t *choices, int32_t *steps, float *traj,
             int64_t traj_len, const ssm_launch *launch, void *workspace, size_t workspace_bytes,
             void *stream) {
-    ssm::SingleCall c{ssm::M_LEGACY, v, a, z, nullptr, t, deadline, s, n_trials, n_samples,
+    ssm::SingleCall c{ssm::M_LEGACY, v, a, z, nullptr, t, deadline, s, nullptr, nullptr, nullptr, nullptr,
+                      n_trials, n_samples,
                       sample_offsets, max_t, nullptr, delta_t, SSM_BOUND_CONSTANT, nullptr, nullptr,
                       nullptr, 0, 0, seed, smooth_unif, noise_rows, noise_row_len, noise_unif,
                       rts, choices, steps, traj, traj_len, launch, workspace, workspace_bytes,
@@ -653,11 +723,63 @@ int ssm_levy_flexbound(const float *v, const float *a, const float *z, const flo
                        int32_t *choices, int32_t *steps, float *traj, int64_t traj_len,
                        const ssm_launch *launch, void *workspace, size_t workspace_bytes,
                        void *stream) {
-    ssm::SingleCall c{ssm::M_LEVY, v, a, z, alpha, t, deadline, s, n_trials, n_samples,
+    ssm::SingleCall c{ssm::M_LEVY, v, a, z, alpha, t, deadline, s, nullptr, nullptr, nullptr, nullptr,
+                      n_trials, n_samples,
                       sample_offsets, max_t, nullptr, delta_t, bound_kind, bound_p1, bound_p2,
                       bound_table, table_stride, table_len, seed, smooth_unif, noise_rows,
                       noise_row_len, noise_unif, rts, choices, steps, traj, traj_len, launch,
                       workspace, workspace_bytes, stream};
+    return ssm::run_single(c);
+}
+
+int ssm_ddm_sdv(const float *v, const float *a, const float *z, const float *t, const float *sv,
+                const float *deadline, const float *s, int64_t n_trials, int64_t n_samples,
+                const int64_t *sample_offsets, float max_t, float delta_t, int bound_kind,
+                const float *bound_p1, const float *bound_p2, const float *bound_table,
+                int64_t table_stride, int64_t table_len, uint64_t seed, int smooth_unif,
+                const float *noise_rows, int64_t noise_row_len, const float *noise_unif, float *rts,
+                int32_t *choices, int32_t *steps, float *traj, int64_t traj_len,
+                const ssm_launch *launch, void *workspace, size_t workspace_bytes, void *stream) {
+    ssm::SingleCall c{ssm::M_SDV, v, a, z, nullptr, t, deadline, s, sv, nullptr, nullptr, nullptr,
+                      n_trials, n_samples, sample_offsets, max_t, nullptr, delta_t, bound_kind,
+                      bound_p1, bound_p2, bound_table, table_stride, table_len, seed, smooth_unif,
+                      noise_rows, noise_row_len, noise_unif, rts, choices, steps, traj, traj_len,
+                      launch, workspace, workspace_bytes, stream};
+    return ssm::run_single(c);
+}
+
+int ssm_full_ddm(const float *v, const float *a, const float *z, const float *t, const float *sz,
+                 const float *sv, const float *st, const float *deadline, const float *s,
+                 int64_t n_trials, int64_t n_samples, const int64_t *sample_offsets, float max_t,
+                 float delta_t, int bound_kind, const float *bound_p1, const float *bound_p2,
+                 const float *bound_table, int64_t table_stride, int64_t table_len, uint64_t seed,
+                 int smooth_unif, const float *noise_rows, int64_t noise_row_len,
+                 const float *noise_unif, float *rts, int32_t *choices, int32_t *steps, float *traj,
+                 int64_t traj_len, const ssm_launch *launch, void *workspace,
+                 size_t workspace_bytes, void *stream) {
+    ssm::SingleCall c{ssm::M_FULL, v, a, z, nullptr, t, deadline, s, sv, sz, st, nullptr,
+                      n_trials, n_samples, sample_offsets, max_t, nullptr, delta_t, bound_kind,
+                      bound_p1, bound_p2, bound_table, table_stride, table_len, seed, smooth_unif,
+                      noise_rows, noise_row_len, noise_unif, rts, choices, steps, traj, traj_len,
+                      launch, workspace, workspace_bytes, stream};
+    return ssm::run_single(c);
+}
+
+int ssm_ornstein_uhlenbeck(const float *v, const float *a, const float *z, const float *g,
+                           const float *t, const float *deadline, const float *s, int64_t n_trials,
+                           int64_t n_samples, const int64_t *sample_offsets, float max_t,
+                           float delta_t, int bound_kind, const float *bound_p1,
+                           const float *bound_p2, const float *bound_table, int64_t table_stride,
+                           int64_t table_len, uint64_t seed, int smooth_unif,
+                           const float *noise_rows, int64_t noise_row_len, const float *noise_unif,
+                           float *rts, int32_t *choices, int32_t *steps, float *traj,
+                           int64_t traj_len, const ssm_launch *launch, void *workspace,
+                           size_t workspace_bytes, void *stream) {
+    ssm::SingleCall c{ssm::M_OU, v, a, z, nullptr, t, deadline, s, nullptr, nullptr, nullptr, g,
+                      n_trials, n_samples, sample_offsets, max_t, nullptr, delta_t, bound_kind,
+                      bound_p1, bound_p2, bound_table, table_stride, table_len, seed, smooth_unif,
+                      noise_rows, noise_row_len, noise_unif, rts, choices, steps, traj, traj_len,
+                      launch, workspace, workspace_bytes, stream};
     return ssm::run_single(c);
 }
 

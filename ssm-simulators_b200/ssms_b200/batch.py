@@ -28,7 +28,12 @@ BATCH_MODELS = {
     "ddm_legacy": ("ddm", None, []),
     "levy": ("levy_flexbound", "constant", ["a"]),
     "levy_angle": ("levy_flexbound", "angle", ["a", "theta"]),
+    "full_ddm": ("full_ddm", "constant", ["a"]),
+    "ornstein": ("ornstein_uhlenbeck", "constant", ["a"]),
+    "ornstein_angle": ("ornstein_uhlenbeck", "angle", ["a", "theta"]),
 }
+# per-trial parameters beyond v, a, z, t of each family
+_EXTRA = {"full_ddm": ("sz", "sv", "st"), "ddm_sdv": ("sv",), "ornstein_uhlenbeck": ("g",)}
 
 
 class BatchedSimulator:
@@ -60,6 +65,7 @@ class BatchedSimulator:
         self.s = D.to_dev_f32(np.ones(K, np.float32) if s is None else f(s), K, "s")
         self.deadline = D.to_dev_f32(np.full(K, 999.0, np.float32) if deadline is None else f(deadline), K, "deadline")
         self.alpha = D.to_dev_f32(th["alpha"], K, "alpha") if family == "levy_flexbound" else None
+        self.extra = {k: D.to_dev_f32(th[k], K, k) for k in _EXTRA.get(family, ())}
         self.max_t = float(max_t)
         self.max_t_k = None if max_t_per_trial is None else D.to_dev_f32(f(max_t_per_trial), K, "max_t_per_trial")
         self.delta_t = float(delta_t)
@@ -95,7 +101,7 @@ class BatchedSimulator:
             bound_kind=self.spec["kind"], bound_p1=self.p1, bound_p2=self.p2,
             bound_table=self.table, seed=self.seed, smooth_unif=self.smooth,
             want_steps=want_steps, out_rts=self.rts, out_choices=self.choices,
-            launch=launch if launch is not None else self.launch)
+            launch=launch if launch is not None else self.launch, **self.extra)
         return self.last
 
     def capture(self) -> torch.cuda.CUDAGraph:
@@ -170,7 +176,8 @@ class BatchedSimulator:
                     bound_kind=self.spec["kind"], bound_p1=sl(self.p1, k0, k1),
                     bound_p2=sl(self.p2, k0, k1), bound_table=sl(self.table, k0, k1),
                     seed=self.seed, smooth_unif=self.smooth, out_rts=self.rts,
-                    out_choices=self.choices, launch=lopt, stream=st, ws_tag=10 + i % 2)
+                    out_choices=self.choices, launch=lopt, stream=st, ws_tag=10 + i % 2,
+                    **{k: x[k0:k1] for k, x in self.extra.items()})
                 done = torch.cuda.Event()
                 done.record(st)
             copy_s.wait_event(done)

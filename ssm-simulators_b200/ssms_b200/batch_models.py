@@ -18,7 +18,8 @@ from . import _device as D
 from . import boundary_functions as bf
 from . import device as dev
 
-SINGLE = ("ddm_flexbound", "levy_flexbound", "ddm")
+SINGLE = ("ddm_flexbound", "levy_flexbound", "ddm", "full_ddm", "ddm_sdv", "ornstein_uhlenbeck")
+_PER_TRIAL = {"full_ddm": ("sz", "sv", "st"), "ddm_sdv": ("sv",), "ornstein_uhlenbeck": ("g",)}
 RACE = ("race_model", "lca")
 
 
@@ -66,6 +67,7 @@ class SetBatch:
             self.v, self.z, self.t = (_dev(_col(kwargs[k], K), K, k) for k in ("v", "z", "t"))
             self.deadline, self.s = _dev(_col(kwargs["deadline"], K), K), _dev(_col(kwargs["s"], K), K)
             self.alpha = _dev(_col(kwargs["alpha"], K), K) if sim_name == "levy_flexbound" else None
+            self.extra = {k: _dev(_col(kwargs[k], K), K, k) for k in _PER_TRIAL.get(sim_name, ())}
         elif sim_name in RACE:
             v = np.asarray(kwargs["v"], np.float32)
             self.n_acc = int(v.shape[1])
@@ -99,7 +101,7 @@ class SetBatch:
                 a=self.a, alpha=self.alpha, n_trials=K, sample_offsets=self.offsets,
                 max_t=self.max_t, delta_t=self.delta_t, bound_kind=self.kind, bound_p1=self.p1,
                 bound_p2=self.p2, bound_table=self._table(), seed=seed, smooth_unif=self.smooth,
-                want_steps=want_steps, out_rts=rts, out_choices=chs)
+                want_steps=want_steps, out_rts=rts, out_choices=chs, **self.extra)
         if self.sim_name in RACE:
             return dev.simulate_race(
                 self.sim_name, v=self.v.reshape(self.v_shape), z=self.z, t=self.t, s=self.s,

@@ -36,6 +36,7 @@ DEADLINE_PARAM_CONFIG = {"name": "deadline", "default_bounds": (0.001, 10.0), "d
 _SIMULATORS = {
     "ddm_flexbound": cssm.ddm_flexbound, "ddm": cssm.ddm, "race_model": cssm.race_model,
     "lca": cssm.lca, "levy_flexbound": cssm.levy_flexbound, "lba_vanilla": cssm.lba_vanilla,
+    "full_ddm": cssm.full_ddm, "ddm_sdv": cssm.ddm_sdv, "ornstein_uhlenbeck": cssm.ornstein_uhlenbeck,
 }
 
 

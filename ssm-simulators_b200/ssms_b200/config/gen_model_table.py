@@ -21,7 +21,8 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 REPO = HERE.parents[2]
-SIMULATORS = {"ddm_flexbound", "ddm", "race_model", "lca", "levy_flexbound", "lba_vanilla"}
+SIMULATORS = {"ddm_flexbound", "ddm", "race_model", "lca", "levy_flexbound", "lba_vanilla", "full_ddm",
+              "ddm_sdv", "ornstein_uhlenbeck"}
 
 
 def _import_reference(root: Path):
@@ -34,7 +35,7 @@ def _import_reference(root: Path):
     sys.path.insert(0, str(REPO / "oracle" / "_ref"))
     import cssm  # the compiled reference simulators
 
-    for name in ("ddm_models", "race_models", "levy_models", "lba_models"):
+    for name in ("ddm_models", "race_models", "levy_models", "lba_models", "ornstein_models"):
         mod = __import__(f"cssm.{name}", fromlist=["x"])
         for k in dir(mod):
             if not k.startswith("_"):

@@ -58,7 +58,12 @@ def _traj_host(traj_t, n):
 
 
 def _run_flex(model, v, a, z, t, deadline, s, levy_alpha, max_t, delta_t, n_samples, n_trials,
-              boundary_fun, boundary_params, random_state, return_option, smooth_unif, extra):
+              boundary_fun, boundary_params, random_state, return_option, smooth_unif, extra,
+              per_trial=None, meta_params=None):
+    """Shared driver of the flexible-bound single-accumulator simulators.
+    ``per_trial``: extra float32 per-trial arrays of the model (sv, sz, st, g);
+    ``meta_params``: the parameter entries of the full metadata, in the
+    reference's order (default: the DDM's)."""
     _check_return_option(return_option)
     n_trials = int(n_trials)
     n_samples = int(n_samples)
@@ -72,9 +77,10 @@ def _run_flex(model, v, a, z, t, deadline, s, levy_alpha, max_t, delta_t, n_samp
     full = return_option == "full"
     nd = _num_draws(max_t, delta_t)
     alpha = None if levy_alpha is None else _f32(levy_alpha, "alpha")
+    per_trial = {k: _f32(x, k) for k, x in (per_trial or {}).items()}
     out = dev.simulate_single(
         model, v=v, z=z, t=t, deadline=deadline, s=s, a=spec["a"],
-        alpha=alpha, n_trials=n_trials,
+        alpha=alpha, n_trials=n_trials, **per_trial,
         n_samples=n_samples, max_t=max_t, delta_t=delta_t, bound_kind=spec["kind"],
         bound_p1=spec["p1"], bound_p2=spec["p2"], bound_table=spec["table"],
         seed=_seed(random_state), smooth_unif=smooth_unif,
@@ -85,7 +91,9 @@ def _run_flex(model, v, a, z, t, deadline, s, levy_alpha, max_t, delta_t, n_samp
     if not full:
         return {"rts": rts, "choices": choices, "metadata": minimal}
     meta = dict(minimal)
-    if model == "levy_flexbound":
+    if meta_params is not None:
+        meta.update(meta_params)
+    elif model == "levy_flexbound":
         meta.update({"v": v, "z": z, "t": t, "alpha": alpha, "s": s})
     else:
         meta.update({"v": v, "a": a, "z": z, "t": t, "s": s, "deadline": deadline})
@@ -120,6 +128,42 @@ def levy_flexbound(v, z, alpha, t, deadline, s, delta_t=0.001, max_t=20, n_sampl
     return _run_flex("levy_flexbound", v, a, z, t, deadline, s, alpha, max_t, delta_t, n_samples,
                      n_trials, boundary_fun, boundary_params, random_state, return_option,
                      smooth_unif, kwargs)
+
+
+def full_ddm(v, a, z, t, sz, sv, st, deadline, s, delta_t=0.001, max_t=20, n_samples=20000,
+             n_trials=1, boundary_fun=None, boundary_params={}, random_state=None,  # noqa: B006
+             return_option="full", smooth_unif=False, n_threads=1, **kwargs):
+    """DDM with trial-to-trial variability in drift (sv, normal), start point (sz,
+    uniform) and non-decision time (st, uniform), flexible bounds
+    (src/cssm/ddm_models.pyx:2177-2497)."""
+    per = {"sz": sz, "sv": sv, "st": st}
+    f = {k: _f32(x, k) for k, x in dict(v=v, a=a, z=z, t=t, sz=sz, sv=sv, st=st, deadline=deadline, s=s).items()}
+    return _run_flex("full_ddm", v, a, z, t, deadline, s, None, max_t, delta_t, n_samples, n_trials,
+                     boundary_fun, boundary_params, random_state, return_option, smooth_unif, kwargs,
+                     per_trial=per, meta_params=f)
+
+
+def ddm_sdv(v, a, z, t, sv, deadline, s, delta_t=0.001, max_t=20, n_samples=20000, n_trials=1,
+            boundary_fun=None, boundary_params={}, random_state=None,  # noqa: B006
+            return_option="full", smooth_unif=False, n_threads=1, **kwargs):
+    """DDM with normally distributed drift variability sv, flexible bounds
+    (src/cssm/ddm_models.pyx:2500-2797)."""
+    f = {k: _f32(x, k) for k, x in dict(v=v, a=a, z=z, t=t, sv=sv, deadline=deadline, s=s).items()}
+    return _run_flex("ddm_sdv", v, a, z, t, deadline, s, None, max_t, delta_t, n_samples, n_trials,
+                     boundary_fun, boundary_params, random_state, return_option, smooth_unif, kwargs,
+                     per_trial={"sv": sv}, meta_params=f)
+
+
+def ornstein_uhlenbeck(v, z, g, t, deadline, s, delta_t=0.001, max_t=20, n_samples=20000,
+                       n_trials=1, boundary_fun=None, boundary_params={}, random_state=None,  # noqa: B006
+                       return_option="full", smooth_unif=False, n_threads=1, **kwargs):
+    """Ornstein-Uhlenbeck accumulator, drift v - g y, flexible bounds
+    (src/cssm/ornstein_models.pyx:47-330)."""
+    a = np.asarray(boundary_params.get("a", np.ones(int(n_trials))), dtype=np.float32)
+    f = {k: _f32(x, k) for k, x in dict(v=v, z=z, g=g, t=t, deadline=deadline, s=s).items()}
+    return _run_flex("ornstein_uhlenbeck", v, a, z, t, deadline, s, None, max_t, delta_t, n_samples,
+                     n_trials, boundary_fun, boundary_params, random_state, return_option, smooth_unif,
+                     kwargs, per_trial={"g": g}, meta_params=f)
 
 
 def ddm(v, a, z, t, deadline, s, max_t=20, delta_t=0.001, n_samples=20000, n_trials=10,

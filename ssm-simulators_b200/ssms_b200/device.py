@@ -21,6 +21,10 @@ from .tuning import launch_for
 MODEL_FLEX = "ddm_flexbound"
 MODEL_LEGACY = "ddm"
 MODEL_LEVY = "levy_flexbound"
+MODEL_SDV = "ddm_sdv"
+MODEL_FULL = "full_ddm"
+MODEL_OU = "ornstein_uhlenbeck"
+SINGLE_MODELS = (MODEL_FLEX, MODEL_LEGACY, MODEL_LEVY, MODEL_SDV, MODEL_FULL, MODEL_OU)
 
 
 @dataclass
@@ -36,7 +40,7 @@ def _opt_f32(x, n, name):
     return None if x is None else D.to_dev_f32(x, n, name)
 
 
-def simulate_single(model: str, *, v, z, t, deadline, s, a=None, alpha=None,
+def simulate_single(model: str, *, v, z, t, deadline, s, a=None, alpha=None, sv=None, sz=None, st=None, g=None,
                     n_trials: int, n_samples: int = 0, sample_offsets=None,
                     max_t: float = 20.0, max_t_per_trial=None, delta_t: float = 0.001,
                     bound_kind: int = _lib.BOUND_CONSTANT, bound_p1=None, bound_p2=None,
@@ -59,9 +63,10 @@ def simulate_single(model: str, *, v, z, t, deadline, s, a=None, alpha=None,
     zt = D.to_dev_f32(z, K, "z")
     tt = D.to_dev_f32(t, K, "t")
     dlt = D.to_dev_f32(deadline, K, "deadline")
-    st = D.to_dev_f32(s, K, "s")
+    s_t = D.to_dev_f32(s, K, "s")
     at = D.to_dev_f32(a if a is not None else np.ones(K, np.float32), K, "a")
     alt = _opt_f32(alpha, K, "alpha")
+    svt, szt, stt, gt = (_opt_f32(x, K, nm) for x, nm in ((sv, "sv"), (sz, "sz"), (st, "st"), (g, "g")))
     p1t = _opt_f32(bound_p1, K, "bound_p1")
     p2t = _opt_f32(bound_p2, K, "bound_p2")
     mtk = _opt_f32(max_t_per_trial, K, "max_t_per_trial")
@@ -93,7 +98,8 @@ def simulate_single(model: str, *, v, z, t, deadline, s, a=None, alpha=None,
     if noise_rows is not None:
         nrows = D.to_dev_f32(noise_rows)
         nlen = int(np.shape(noise_rows)[-1]) if not isinstance(noise_rows, torch.Tensor) else int(noise_rows.shape[-1])
-        nunif = D.to_dev_f32(noise_unif, total, "noise_unif")
+        # full_ddm takes three uniforms per trajectory (u_t, u_y, u_jitter)
+        nunif = D.to_dev_f32(noise_unif, total * (3 if model == MODEL_FULL else 1), "noise_unif")
         if nrows.numel() < total * nlen:
             raise ValueError("noise_rows must hold one row per trajectory")
     L = _lib.lib()
@@ -111,23 +117,42 @@ def simulate_single(model: str, *, v, z, t, deadline, s, a=None, alpha=None,
     )
     if model == MODEL_FLEX:
         status = L.ssm_ddm_flexbound(
-            D.ptr(vt), D.ptr(at), D.ptr(zt), D.ptr(tt), D.ptr(dlt), D.ptr(st), K, int(n_samples),
+            D.ptr(vt), D.ptr(at), D.ptr(zt), D.ptr(tt), D.ptr(dlt), D.ptr(s_t), K, int(n_samples),
             D.ptr(offs), float(np.float32(max_t)), D.ptr(mtk), float(np.float32(delta_t)),
             int(bound_kind), D.ptr(p1t), D.ptr(p2t), D.ptr(tab), tstride, tlen, *common_tail,
             ctypes.addressof(lopt), D.ptr(ws), ws.numel(), sp)
     elif model == MODEL_LEGACY:
         status = L.ssm_ddm(
-            D.ptr(vt), D.ptr(at), D.ptr(zt), D.ptr(tt), D.ptr(dlt), D.ptr(st), K, int(n_samples),
+            D.ptr(vt), D.ptr(at), D.ptr(zt), D.ptr(tt), D.ptr(dlt), D.ptr(s_t), K, int(n_samples),
             D.ptr(offs), float(np.float32(max_t)), float(np.float32(delta_t)), *common_tail,
             ctypes.addressof(lopt), D.ptr(ws), ws.numel(), sp)
     elif model == MODEL_LEVY:
         if alt is None:
             raise ValueError("levy_flexbound needs alpha")
         status = L.ssm_levy_flexbound(
-            D.ptr(vt), D.ptr(at), D.ptr(zt), D.ptr(alt), D.ptr(tt), D.ptr(dlt), D.ptr(st), K,
+            D.ptr(vt), D.ptr(at), D.ptr(zt), D.ptr(alt), D.ptr(tt), D.ptr(dlt), D.ptr(s_t), K,
             int(n_samples), D.ptr(offs), float(np.float32(max_t)), float(np.float32(delta_t)),
             int(bound_kind), D.ptr(p1t), D.ptr(p2t), D.ptr(tab), tstride, tlen, *common_tail,
             ctypes.addressof(lopt), D.ptr(ws), ws.numel(), sp)
+    elif model in (MODEL_SDV, MODEL_FULL, MODEL_OU):
+        bound_args = (K, int(n_samples), D.ptr(offs), float(np.float32(max_t)), float(np.float32(delta_t)),
+                      int(bound_kind), D.ptr(p1t), D.ptr(p2t), D.ptr(tab), tstride, tlen, *common_tail,
+                      ctypes.addressof(lopt), D.ptr(ws), ws.numel(), sp)
+        if model == MODEL_SDV:
+            if svt is None:
+                raise ValueError("ddm_sdv needs sv")
+            status = L.ssm_ddm_sdv(D.ptr(vt), D.ptr(at), D.ptr(zt), D.ptr(tt), D.ptr(svt), D.ptr(dlt),
+                                   D.ptr(s_t), *bound_args)
+        elif model == MODEL_FULL:
+            if svt is None or szt is None or stt is None:
+                raise ValueError("full_ddm needs sz, sv and st")
+            status = L.ssm_full_ddm(D.ptr(vt), D.ptr(at), D.ptr(zt), D.ptr(tt), D.ptr(szt), D.ptr(svt),
+                                    D.ptr(stt), D.ptr(dlt), D.ptr(s_t), *bound_args)
+        else:
+            if gt is None:
+                raise ValueError("ornstein_uhlenbeck needs g")
+            status = L.ssm_ornstein_uhlenbeck(D.ptr(vt), D.ptr(at), D.ptr(zt), D.ptr(gt), D.ptr(tt),
+                                              D.ptr(dlt), D.ptr(s_t), *bound_args)
     else:
         raise ValueError(f"unknown single-accumulator model {model!r}")
     _lib.check(status)

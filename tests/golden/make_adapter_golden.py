@@ -32,7 +32,7 @@ def _reference():
     sys.path.insert(0, str(ROOT / "oracle" / "_ref"))
     import cssm
 
-    for name in ("ddm_models", "race_models", "levy_models", "lba_models"):
+    for name in ("ddm_models", "race_models", "levy_models", "lba_models", "ornstein_models"):
         mod = __import__(f"cssm.{name}", fromlist=["x"])
         for k in dir(mod):
             if not k.startswith("_"):

@@ -1,0 +1,163 @@
+"""GPU parity for full_ddm, ddm_sdv and ornstein_uhlenbeck through the C ABI.
+
+* Noise injection: GPU and the CPU oracle (pinned to the reference's own
+  outputs, tests/test_oracle_golden.py) consume the same pre-drawn rows --
+  [drift normal, walk normals...] and [u_t, u_y, u_jitter] for full_ddm,
+  [drift normal, walk normals...] and [u_jitter] for ddm_sdv -- and step
+  counts, choices and rts must match bit for bit.
+* Device RNG: two-sample KS on rts per choice and choice probabilities within
+  3 Monte-Carlo standard errors against the reference stream (the oracle
+  driven by the reference's numpy generator).
+"""
+
+import zlib
+
+import numpy as np
+import pytest
+
+from ssms_b200 import boundary_functions as bf
+from ssms_b200 import cssm
+from ssms_b200 import device as dev
+
+from test_gpu_single import _bits, _compare_dist
+
+pytestmark = pytest.mark.gpu
+
+f32 = lambda x: np.asarray(x, dtype=np.float32)  # noqa: E731
+
+
+def _theta(rng, K):
+    return {"v": f32(rng.uniform(-2, 2, K)), "a": f32(rng.uniform(0.6, 2.0, K)), "z": f32(rng.uniform(0.3, 0.7, K)),
+            "t": f32(rng.uniform(0.1, 0.8, K)), "sz": f32(rng.uniform(0.0, 0.2, K)),
+            "sv": f32(rng.uniform(0.0, 1.5, K)), "st": f32(rng.uniform(0.0, 0.25, K)),
+            "g": f32(rng.uniform(-0.8, 1.5, K)), "theta": f32(rng.uniform(0.0, 1.0, K))}
+
+
+def _gpu(model, th, n, K, spec, *, rows=None, unif=None, smooth=True, max_t=3.0, seed=0, deadline=None):
+    out = dev.simulate_single(
+        model, v=th["v"], z=th["z"], t=th["t"], deadline=f32([999] * K) if deadline is None else deadline,
+        s=f32([1] * K), a=spec["a"], sv=th.get("sv"), sz=th.get("sz"), st=th.get("st"), g=th.get("g"),
+        n_trials=K, n_samples=n, max_t=max_t, delta_t=0.001, bound_kind=spec["kind"], bound_p1=spec["p1"],
+        bound_p2=spec["p2"], bound_table=spec["table"], seed=seed, smooth_unif=smooth, noise_rows=rows,
+        noise_unif=unif, want_steps=True)
+    return out.rts.cpu().numpy(), out.choices.cpu().numpy(), out.steps.cpu().numpy()
+
+
+def _oracle(oracle, model, th, n, K, fun, bp, *, rows=None, unif=None, smooth=True, max_t=3.0,
+            random_state=None, deadline=None):
+    dl = f32([999] * K) if deadline is None else deadline
+    if model == "ornstein_uhlenbeck":
+        return oracle.ornstein(th["v"], th["z"], th["g"], th["t"], dl, f32([1] * K), max_t=max_t, delta_t=0.001,
+                               n_samples=n, n_trials=K, boundary_fun=fun, boundary_params=bp, smooth_unif=smooth,
+                               rows=rows, unif=unif, random_state=random_state)
+    return oracle.ddm_variability(model, th["v"], th["z"], th["t"], th["sz"], th["sv"], th["st"], dl,
+                                  f32([1] * K), max_t=max_t, delta_t=0.001, n_samples=n, n_trials=K,
+                                  boundary_fun=fun, boundary_params=bp, smooth_unif=smooth, rows=rows,
+                                  unif=unif, random_state=random_state)
+
+
+CASES = [("full_ddm", "constant"), ("full_ddm", "angle"), ("full_ddm", "weibull_table"),
+         ("ddm_sdv", "constant"), ("ddm_sdv", "angle"), ("ornstein_uhlenbeck", "constant"),
+         ("ornstein_uhlenbeck", "angle")]
+
+
+@pytest.mark.parametrize("model,bname", CASES)
+@pytest.mark.parametrize("smooth", [True, False])
+def test_noise_injection_bit_exact(cuda, oracle, model, bname, smooth):
+    rng = np.random.default_rng(zlib.crc32(f"{model}/{bname}/{smooth}".encode()))
+    K, N, max_t = 5, 400, 3.0
+    th = _theta(rng, K)
+    th["alpha"], th["beta"] = f32(rng.uniform(1.0, 3.0, K)), f32(rng.uniform(0.8, 3.0, K))
+    if bname == "weibull_table":
+        fun, keys, force = bf.weibull_cdf, ["a", "alpha", "beta"], True
+    else:
+        fun, keys, force = bf.BOUNDARIES[bname][0], bf.BOUNDARIES[bname][1], False
+    bp = {k: th[k] for k in keys}
+    spec = bf.kernel_spec(fun, bp, K, bf.make_t_s(max_t, 0.001), force_table=force)
+    total = K * N
+    row_len = int(max_t / 0.001) + 80
+    rows = rng.standard_normal((total, row_len), dtype=np.float32)
+    unif = f32(rng.uniform(0, 1, total * (3 if model == "full_ddm" else 1)))
+    dl = f32(rng.uniform(0.5, 3.5, K))
+    dl[0] = 999.0
+    g_rt, g_ch, g_st = _gpu(model, th, N, K, spec, rows=rows, unif=unif, smooth=smooth, max_t=max_t, deadline=dl)
+    o_rt, o_ch, o_st, _ = _oracle(oracle, model, th, N, K, fun, bp, rows=rows, unif=unif, smooth=smooth,
+                                  max_t=max_t, deadline=dl)
+    np.testing.assert_array_equal(g_st, o_st)
+    np.testing.assert_array_equal(g_ch, o_ch)
+    np.testing.assert_array_equal(_bits(g_rt), _bits(o_rt))
+
+
+STAT_PANEL = [
+    ("full_ddm", "constant", dict(v=1.0, a=1.5, z=0.5, t=0.3, sz=0.15, sv=1.0, st=0.2)),
+    ("full_ddm", "angle", dict(v=-0.5, a=2.0, z=0.45, t=0.5, sz=0.05, sv=0.5, st=0.1, theta=0.5)),
+    ("ddm_sdv", "constant", dict(v=0.7, a=1.2, z=0.5, t=0.2, sv=1.5)),
+    ("ornstein_uhlenbeck", "constant", dict(v=0.8, a=1.5, z=0.5, t=0.3, g=0.8)),
+    ("ornstein_uhlenbeck", "angle", dict(v=-0.4, a=1.8, z=0.55, t=0.2, g=-0.5, theta=0.6)),
+]
+
+
+@pytest.mark.parametrize("case", range(len(STAT_PANEL)))
+def test_device_rng_matches_reference_distribution(cuda, oracle, case):
+    model, bname, p = STAT_PANEL[case]
+    N = 100_000
+    th = {k: f32([v]) for k, v in p.items()}
+    for k in ("sz", "sv", "st", "g"):
+        th.setdefault(k, f32([0.0]))
+    fun, keys = bf.BOUNDARIES[bname]
+    bp = {k: th[k] for k in keys}
+    spec = bf.kernel_spec(fun, bp, 1, bf.make_t_s(20.0, 0.001))
+    g_rt, g_ch, _ = _gpu(model, th, N, 1, spec, max_t=20.0, seed=77 + case)
+    r = _oracle(oracle, model, th, N, 1, fun, bp, max_t=20.0, random_state=99 + case)
+    _compare_dist(g_rt, g_ch, r[0], r[1], [-1, 1], alpha_ks=0.01 / len(STAT_PANEL))
+
+
+def test_cssm_contract(cuda):
+    """Shapes, dtypes and metadata keys as the reference's full_ddm / ddm_sdv / ornstein_uhlenbeck."""
+    K, N = 3, 50
+    one = f32([1.0] * K)
+    bp = {"a": f32([1.2] * K)}
+    out = cssm.full_ddm(f32([0.5] * K), bp["a"], f32([0.5] * K), f32([0.3] * K), f32([0.1] * K), f32([0.4] * K),
+                        f32([0.1] * K), f32([999] * K), one, n_samples=N, n_trials=K, boundary_fun=bf.constant,
+                        boundary_params=bp, random_state=3)
+    assert out["rts"].shape == (N, K, 1) and out["rts"].dtype == np.float32
+    assert out["choices"].dtype == np.int32 and set(np.unique(out["choices"])) <= {-1, 1}
+    m = out["metadata"]
+    assert m["simulator"] == "full_ddm" and m["trajectory"].shape == (20001, 1) and m["boundary"].shape == (20001,)
+    for k in ("v", "a", "z", "t", "sz", "sv", "st", "deadline", "s", "delta_t", "max_t", "n_threads"):
+        assert k in m, k
+    out = cssm.ddm_sdv(f32([0.5] * K), bp["a"], f32([0.5] * K), f32([0.3] * K), f32([0.4] * K), f32([999] * K), one,
+                       n_samples=N, n_trials=K, boundary_fun=bf.constant, boundary_params=bp, random_state=3,
+                       return_option="minimal")
+    assert out["metadata"]["simulator"] == "ddm_sdv" and "trajectory" not in out["metadata"]
+    out = cssm.ornstein_uhlenbeck(f32([0.5] * K), f32([0.5] * K), f32([0.3] * K), f32([0.3] * K), f32([999] * K),
+                                  one, n_samples=N, n_trials=K, boundary_fun=bf.constant, boundary_params=bp,
+                                  random_state=3)
+    assert out["metadata"]["simulator"] == "ornstein_uhlenbeck" and "g" in out["metadata"]
+    with pytest.raises(ValueError):
+        cssm.ornstein_uhlenbeck(f32([0.5]), f32([0.5]), f32([0.3]), f32([0.3]), f32([999]), f32([1]),
+                                n_samples=5, boundary_fun=bf.constant, boundary_params={"a": f32([1.0])},
+                                return_option="bogus")
+
+
+@pytest.mark.parametrize("model", ["full_ddm", "ornstein", "ornstein_angle"])
+def test_simulator_api_and_batched_sets(cuda, model):
+    """Simulator(model).simulate and the batched set path (SetBatch, the data
+    generator's simulator) run the new families and agree in distribution."""
+    from ssms_b200 import Simulator, model_config
+    from ssms_b200.batch_models import simulate_sets
+
+    cfg = model_config[model]
+    theta = dict(zip(cfg["params"], cfg["default_params"]))
+    out = Simulator(model).simulate(theta, n_samples=20000, random_state=5)
+    assert out["rts"].shape == (20000, 1) and out["metadata"]["model"] == model
+    prep = Simulator(model).prepare({k: np.full(2, v, np.float32) for k, v in theta.items()}, n_samples=20000,
+                                    random_state=6)
+    o = simulate_sets(cfg["simulator"].__name__, prep["theta"], prep["boundary"], 20000, max_t=20.0,
+                      delta_t=0.001, seed=6)
+    ch = o.choices.cpu().numpy().reshape(2, 20000)
+    p_api = np.mean(out["choices"][:, 0] == 1)
+    for k in range(2):
+        p_set = np.mean(ch[k] == 1)
+        se = np.sqrt(max(p_api * (1 - p_api), 1e-6) * 2 / 20000)
+        assert abs(p_set - p_api) < 4 * se, (p_set, p_api)
