@@ -460,7 +460,9 @@ MIX_BOUNDS = {
     "race_no_bias_angle_4": {**_V4, "a": (1.0, 3.0), "z": (0.0, 0.5), "t": (0.0, 2.0), "theta": (0.0, 1.45)},
     "levy": {"v": (-3.0, 3.0), "a": (0.3, 3.0), "z": (0.1, 0.9), "alpha": (1.0, 2.0), "t": (0.001, 2.0)},
 }
-MIX_CPU_ROWS_PER_CORE = {"lca_no_bias_4": 1, "race_no_bias_angle_4": 6, "levy": 6}
+MIX_CPU_ROWS_PER_CORE = {"lca_no_bias_4": 1, "race_no_bias_angle_4": 6, "levy": 6, "full_ddm": 6, "ornstein": 6}
+# further simulator families, 1024 parameter vectors from their configured bounds, 10000 samples
+WIDER = ("full_ddm", "ornstein")
 PLAIN_DDM = {"v": 1.0, "a": 1.5, "z": 0.5, "t": 0.2}
 PLAIN_SAMPLES = 100_000
 
@@ -476,7 +478,7 @@ def _constant_host(t, a):
 
 _HOST_BOUNDS = {"constant": _constant_host, "angle": _angle_host}
 _REF_MODULE = {"ddm_flexbound": "ddm_models", "levy_flexbound": "levy_models", "race_model": "race_models",
-               "lca": "race_models"}
+               "lca": "race_models", "full_ddm": "ddm_models", "ornstein_uhlenbeck": "ornstein_models"}
 
 
 def _cpu_sim_worker(job):
@@ -519,7 +521,14 @@ def run_other_workloads(args) -> dict:
     from ssms_b200.batch_models import SetBatch
 
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    from ssms_b200 import model_config
+
     cases = [(m, mix_workload(m, SEED + 100 + i), MIX_SAMPLES) for i, m in enumerate(MIX_BOUNDS)]
+    for i, m in enumerate(WIDER):
+        lo, hi = (np.asarray(b, np.float64) for b in model_config[m]["param_bounds"])
+        rng = np.random.default_rng(SEED + 200 + i)
+        cases.append((m, {p: rng.uniform(lo[j], hi[j], MIX_THETA).astype(np.float32)
+                          for j, p in enumerate(model_config[m]["params"])}, MIX_SAMPLES))
     cases.append(("ddm", {k: np.float32(v) for k, v in PLAIN_DDM.items()}, PLAIN_SAMPLES))
     res, cpu_jobs = {}, []
     for i, (model, theta, n) in enumerate(cases):
