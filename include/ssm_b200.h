@@ -187,6 +187,25 @@ int ssm_ornstein_uhlenbeck(const float *v, const float *a, const float *z, const
                            int64_t traj_len, const ssm_launch *launch, void *workspace,
                            size_t workspace_bytes, void *stream);
 
+/*
+ * ssm_ddm_flex -- replaces cssm.ddm_flex (src/cssm/ddm_models.pyx:884-1193):
+ * the flexible-bound DDM with a time-varying drift, y += v(t_ix) dt +
+ * sqrt(dt) s N(0,1).  drift_table holds each trial's drift function evaluated
+ * on the time grid t_ix = ix * dt (float32 [n_trials * drift_stride],
+ * drift_len entries per trial; later steps use the last entry); `v` is
+ * accepted for the reference's signature and unused, the drift function
+ * carries it.  Layout and noise conventions as ssm_ddm_flexbound.
+ */
+int ssm_ddm_flex(const float *v, const float *a, const float *z, const float *t, const float *deadline,
+                 const float *s, int64_t n_trials, int64_t n_samples, const int64_t *sample_offsets,
+                 float max_t, float delta_t, int bound_kind, const float *bound_p1,
+                 const float *bound_p2, const float *bound_table, int64_t table_stride,
+                 int64_t table_len, const float *drift_table, int64_t drift_stride, int64_t drift_len,
+                 uint64_t seed, int smooth_unif, const float *noise_rows, int64_t noise_row_len,
+                 const float *noise_unif, float *rts, int32_t *choices, int32_t *steps, float *traj,
+                 int64_t traj_len, const ssm_launch *launch, void *workspace,
+                 size_t workspace_bytes, void *stream);
+
 /* ---- multi-accumulator race / LCA --------------------------------------- */
 
 /* Bytes of scratch ssm_race_model / ssm_lca need. */

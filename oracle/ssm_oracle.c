@@ -275,6 +275,47 @@ int64_t oracle_ou_trial(int64_t k, int64_t n_samples, int64_t n_trials, float v,
 }
 
 /*
+ * One trial of ddm_flex (src/cssm/ddm_models.pyx:996-1043): the drift of step
+ * ix is the trial's drift table at ix (the drift function on the time grid),
+ * y += (v(t_ix) * dt) + sqrt_st * g.
+ */
+int64_t oracle_dflex_trial(int64_t k, int64_t n_samples, int64_t n_trials, float z, float t,
+                           float deadline, float sqrt_st, const float *bound, int64_t nb,
+                           const float *drift, int64_t nd, float max_t, float dt, int smooth,
+                           oracle_noise *nz, float *rts, int32_t *choices, int32_t *steps, float *traj,
+                           int64_t traj_len) {
+    const float dl = deadline_tmp(max_t, deadline, t);
+    int64_t total_steps = 0;
+    for (int64_t n = 0; n < n_samples; ++n) {
+        const int64_t w = n * n_trials + k;
+        /* (-1) * b0 + z * 2 * b0 with integer literals: float arithmetic */
+        float y = (-bound[0]) + ((z * 2.0f) * bound[0]);
+        float tp = 0.0f;
+        int64_t ix = 0;
+        const int rec = (traj != 0 && n == 0 && k == 0);
+        if (rec && traj_len > 0) traj[0] = y;
+        for (;;) {
+            const float b = bound[ix < nb ? ix : nb - 1];
+            if (!((y >= (-1.0 * (double)b)) && (y <= b) && (tp <= dl))) break;
+            const float gm = next_g(nz, w, ix, k);
+            y = (y + (drift[ix < nd ? ix : nd - 1] * dt)) + (sqrt_st * gm);
+            tp = tp + dt;
+            ix += 1;
+            if (rec && ix < traj_len) traj[ix] = y;
+        }
+        const float u = next_u(nz, w, k);
+        const float sm = smooth_jitter(smooth, tp, dl, dt, u);
+        float rt = (tp + t) + sm;
+        if (rt >= deadline || deadline <= 0) rt = -999.0f;
+        rts[w] = rt;
+        choices[w] = sign_f(y);
+        if (steps) steps[w] = (int32_t)ix;
+        total_steps += ix;
+    }
+    return total_steps;
+}
+
+/*
  * One trial of race_model (race_models.pyx:417-464) or lca
  * (race_models.pyx:825-879), selected by `lca`.  v, z, sqrt_st hold the
  * trial's np particle values; increments are consumed particle-major within a

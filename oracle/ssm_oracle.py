@@ -72,6 +72,9 @@ def lib():
         L.oracle_ou_trial.restype = I64
         L.oracle_ou_trial.argtypes = [I64, I64, I64, F, F, F, F, F, F, P, I64, F, F, I, NP, P, P, P, P,
                                       I64]
+        L.oracle_dflex_trial.restype = I64
+        L.oracle_dflex_trial.argtypes = [I64, I64, I64, F, F, F, F, P, I64, P, I64, F, F, I, NP, P, P, P, P,
+                                         I64]
         L.oracle_lba_f32.restype = None
         L.oracle_lba_f32.argtypes = [I64, I64, I, P, P, P, P, P, P, P]
         _lib = L
@@ -273,6 +276,34 @@ def ornstein(v, z, g, t, deadline, s, *, max_t, delta_t, n_samples, n_trials, bo
         L.oracle_ou_trial(k, n_samples, n_trials, v[k], z[k], g[k], t[k], deadline[k], scales[k],
                           _p(tab), tab.shape[0], f32(max_t), f32(delta_t), int(bool(smooth_unif)),
                           C.byref(nz), _p(rts), _p(chs), _p(steps), _p(traj), traj_len)
+    if rows is not None and nz.overrun:
+        raise ValueError("noise rows too short for the simulated trajectories")
+    del keep
+    return rts, chs, steps, traj
+
+
+def ddm_flex(z, t, deadline, s, *, max_t, delta_t, n_samples, n_trials, boundary_fun, boundary_params,
+             drift_fun, drift_params, smooth_unif, random_state=None, rows=None, unif=None, traj_len=0):
+    """ddm_flex (stream or row mode): the drift table of each trial is
+    drift_fun(t=t_s, **params_k) cast to float32, as the reference computes it."""
+    L = lib()
+    z, t, deadline, s = (np.asarray(x, np.float32) for x in (z, t, deadline, s))
+    nd = num_draws(max_t, delta_t)
+    t_s = t_grid(max_t, delta_t)
+    if rows is None:
+        strm = _Stream(random_state, _normal_init(nd), _normal_refill)
+        nz, keep = strm.noise, strm
+    else:
+        nz, keep = _rows_noise(rows, unif)
+    rts, chs, steps = _outputs(n_samples, n_trials)
+    traj = np.full(traj_len, -999, np.float32) if traj_len else None
+    scales = (sqrt_dt(delta_t) * s).astype(np.float32)
+    for k, tab in enumerate(_bound_tables(boundary_fun, boundary_params, n_trials, t_s)):
+        params_k = {key: np.asarray(val)[k] for key, val in drift_params.items()}
+        drift = np.ascontiguousarray(np.asarray(drift_fun(t=t_s, **params_k)).astype(np.float32))
+        L.oracle_dflex_trial(k, n_samples, n_trials, z[k], t[k], deadline[k], scales[k], _p(tab), tab.shape[0],
+                             _p(drift), drift.shape[0], f32(max_t), f32(delta_t), int(bool(smooth_unif)),
+                             C.byref(nz), _p(rts), _p(chs), _p(steps), _p(traj), traj_len)
     if rows is not None and nz.overrun:
         raise ValueError("noise rows too short for the simulated trajectories")
     del keep

@@ -34,8 +34,9 @@ namespace ssm {
 
 // M_SDV: ddm_sdv (drift v + sv N(0,1) per trajectory); M_FULL: full_ddm (and
 // start point + U(-sz, sz), non-decision time + U(-st, st)); M_OU:
-// ornstein_uhlenbeck (drift v - g y).
-enum Model { M_FLEX = 0, M_LEGACY = 1, M_LEVY = 2, M_SDV = 3, M_FULL = 4, M_OU = 5 };
+// ornstein_uhlenbeck (drift v - g y); M_DFLEX: ddm_flex (drift v(t) from a
+// per-trial table the host evaluates from the drift function).
+enum Model { M_FLEX = 0, M_LEGACY = 1, M_LEVY = 2, M_SDV = 3, M_FULL = 4, M_OU = 5, M_DFLEX = 6 };
 
 struct alignas(16) TrialRow {
     float drift;     // v * dt ; SDV/FULL: v
@@ -70,6 +71,8 @@ struct SingleParams {
     int chunk;
     const float *table;
     int64_t tstride, tlen;
+    const float *dtable;     // DFLEX: drift v(t_ix) per trial, row stride dstride, dlen entries
+    int64_t dstride, dlen;
     const float *noise;      // injected increments: row w holds nlen floats
     int64_t nlen;
     const float *nunif;      // injected jitter uniforms, one per trajectory
@@ -136,8 +139,9 @@ __global__ void k_prep(const PrepArgs A) {
     r.c2 = -1.3862944f * r.scale * r.scale;
     if (A.model == M_LEGACY) {
         r.y0 = __fmul_rn(A.z[k], r.a);  // ddm_models.pyx:451
-    } else if (A.model == M_OU) {
-        // (-1) * b0 + z * 2 * b0 with integer literals: float arithmetic (ornstein_models.pyx:167)
+    } else if (A.model == M_OU || A.model == M_DFLEX) {
+        // (-1) * b0 + z * 2 * b0 with integer literals: float arithmetic
+        // (ornstein_models.pyx:167, ddm_models.pyx:1014)
         const float b0 = (A.bound == SSM_BOUND_TABLE) ? A.table[k * A.tstride] : r.a;
         r.y0 = __fadd_rn(-b0, __fmul_rn(__fmul_rn(A.z[k], 2.0f), b0));
     } else {
@@ -302,7 +306,7 @@ __device__ __forceinline__ void draw_block(const SingleParams &p, const Lane &L,
             g[2 * h + 3] = fmaf(r.scale, cms_stable(c.z, c.w, r), r.drift);
         }
     } else {
-        const float drift = DrawnDrift<MODEL>::value ? L.dinc : r.drift;
+        const float drift = DrawnDrift<MODEL>::value ? L.dinc : (MODEL == M_DFLEX ? 0.f : r.drift);
         const uint4 b0 = philox10(make_uint4(2u * L.blk, L.n, L.k + p.k_base, 0u), p.key);
         const uint4 b1 = philox10(make_uint4(2u * L.blk + 1u, L.n, L.k + p.k_base, 0u), p.key);
         bm_increment(b0.x, b0.y, r.c2, drift, g[0], g[1]);
@@ -323,7 +327,8 @@ __device__ __forceinline__ bool step_block(const SingleParams &p, Lane &L, const
         raise_error(p.hdr, SSM_ERR_DEVICE, (int)L.w);
         return false;
     }
-    constexpr bool INT_IX = NOISE || RECORD || BOUND == SSM_BOUND_TABLE;
+    constexpr bool INT_IX = NOISE || RECORD || BOUND == SSM_BOUND_TABLE || MODEL == M_DFLEX;
+    const float *drow = (MODEL == M_DFLEX) ? p.dtable + (int64_t)L.k * p.dstride : nullptr;
     bool live = true;
 #pragma unroll
     for (int q = 0; q < BLK; ++q) {
@@ -344,6 +349,10 @@ __device__ __forceinline__ bool step_block(const SingleParams &p, Lane &L, const
                     // (y + (v - g y) dt) + scale*g (ornstein_models.pyx:177)
                     const float lk = __fmul_rn(__fsub_rn(r.alpha, __fmul_rn(r.inv_alpha, L.y)), p.dt);
                     L.y = __fadd_rn(__fadd_rn(L.y, lk), __fmul_rn(r.scale, g[q]));
+                } else if (MODEL == M_DFLEX) {
+                    // (y + v(t_ix) dt) + scale*g (ddm_models.pyx:1025)
+                    const float dv = __ldg(drow + ((L.ix < p.dlen) ? L.ix : p.dlen - 1));
+                    L.y = __fadd_rn(__fadd_rn(L.y, __fmul_rn(dv, p.dt)), __fmul_rn(r.scale, g[q]));
                 } else {
                     // (y + v*dt) + scale*g: the association the reference build uses
                     const float dr = DrawnDrift<MODEL>::value ? L.dinc : r.drift;
@@ -352,6 +361,8 @@ __device__ __forceinline__ bool step_block(const SingleParams &p, Lane &L, const
                 L.tp = __fadd_rn(L.tp, p.dt);
             } else {
                 if (MODEL == M_OU) L.y = fmaf(L.y, r.expo, g[q]);  // y (1 - g dt) + v dt + noise
+                else if (MODEL == M_DFLEX)                          // y + v(t_ix) dt + noise
+                    L.y += fmaf(__ldg(drow + ((L.ix < p.dlen) ? L.ix : p.dlen - 1)), p.dt, g[q]);
                 else L.y += g[q];
                 L.tp += p.dt;
             }
@@ -574,6 +585,8 @@ struct SingleCall {
     int model;
     const float *v, *a, *z, *alpha, *t, *deadline, *s;
     const float *sv, *sz, *st, *g;
+    const float *dtable;
+    int64_t dstride, dlen;
     int64_t n_trials, n_samples;
     const int64_t *offsets;
     float max_t;
@@ -609,6 +622,8 @@ static int run_single(const SingleCall &c) {
     SSM_REQUIRE((c.model != M_SDV && c.model != M_FULL) || c.sv, "sv is required");
     SSM_REQUIRE(c.model != M_FULL || (c.sz && c.st), "sz and st are required");
     SSM_REQUIRE(c.model != M_OU || c.g, "g is required for the Ornstein-Uhlenbeck model");
+    SSM_REQUIRE(c.model != M_DFLEX || (c.dtable && c.dlen >= 1 && c.dstride >= c.dlen),
+                "ddm_flex needs drift_table with drift_stride >= drift_len >= 1");
     if (c.model != M_LEGACY) {
         SSM_REQUIRE(c.bound >= SSM_BOUND_TABLE && c.bound <= SSM_BOUND_WEIBULL, "unknown boundary kind %d", c.bound);
         SSM_REQUIRE(c.bound != SSM_BOUND_LINEAR || c.p1, "linear boundary needs bound_p1");
@@ -647,6 +662,7 @@ static int run_single(const SingleCall &c) {
     p.total = c.offsets ? -1 : c.n_trials * c.n_samples;
     p.k_base = (uint32_t)((c.launch && c.launch->first_trial > 0) ? c.launch->first_trial : 0);
     p.ustride = (c.model == M_FULL) ? 3 : 1;
+    p.dtable = c.dtable; p.dstride = c.dstride; p.dlen = c.dlen;
     p.dt = c.dt;
     p.smooth = c.smooth ? 1 : 0;
     p.chunk = (c.launch && c.launch->chunk >= 32) ? c.launch->chunk : 64;
@@ -668,6 +684,7 @@ static int run_single(const SingleCall &c) {
         case M_SDV: return Launcher::dispatch<M_SDV>(c.bound, noise, p, c.launch, st);
         case M_FULL: return Launcher::dispatch<M_FULL>(c.bound, noise, p, c.launch, st);
         case M_OU: return Launcher::dispatch<M_OU>(c.bound, noise, p, c.launch, st);
+        case M_DFLEX: return Launcher::dispatch<M_DFLEX>(c.bound, noise, p, c.launch, st);
         default: return Launcher::dispatch<M_LEVY>(c.bound, noise, p, c.launch, st);
     }
 }
@@ -688,7 +705,7 @@ int ssm_ddm_flexbound(const float *v, const float *a, const float *z, const floa
                       int32_t *choices, int32_t *steps, float *traj, int64_t traj_len,
                       const ssm_launch *launch, void *workspace, size_t workspace_bytes,
                       void *stream) {
-    ssm::SingleCall c{ssm::M_FLEX, v, a, z, nullptr, t, deadline, s, nullptr, nullptr, nullptr, nullptr,
+    ssm::SingleCall c{ssm::M_FLEX, v, a, z, nullptr, t, deadline, s, nullptr, nullptr, nullptr, nullptr, nullptr, 0, 0,
                       n_trials, n_samples,
                       sample_offsets, max_t, max_t_per_trial, delta_t, bound_kind, bound_p1,
                       bound_p2, bound_table, table_stride, table_len, seed, smooth_unif,
@@ -704,7 +721,7 @@ int ssm_ddm(const float *v, const float *a, const float *z, const float *t, cons
             const float *noise_unif, float *rts, int32_t *choices, int32_t *steps, float *traj,
             int64_t traj_len, const ssm_launch *launch, void *workspace, size_t workspace_bytes,
             void *stream) {
-    ssm::SingleCall c{ssm::M_LEGACY, v, a, z, nullptr, t, deadline, s, nullptr, nullptr, nullptr, nullptr,
+    ssm::SingleCall c{ssm::M_LEGACY, v, a, z, nullptr, t, deadline, s, nullptr, nullptr, nullptr, nullptr, nullptr, 0, 0,
                       n_trials, n_samples,
                       sample_offsets, max_t, nullptr, delta_t, SSM_BOUND_CONSTANT, nullptr, nullptr,
                       nullptr, 0, 0, seed, smooth_unif, noise_rows, noise_row_len, noise_unif,
@@ -723,7 +740,7 @@ int ssm_levy_flexbound(const float *v, const float *a, const float *z, const flo
                        int32_t *choices, int32_t *steps, float *traj, int64_t traj_len,
                        const ssm_launch *launch, void *workspace, size_t workspace_bytes,
                        void *stream) {
-    ssm::SingleCall c{ssm::M_LEVY, v, a, z, alpha, t, deadline, s, nullptr, nullptr, nullptr, nullptr,
+    ssm::SingleCall c{ssm::M_LEVY, v, a, z, alpha, t, deadline, s, nullptr, nullptr, nullptr, nullptr, nullptr, 0, 0,
                       n_trials, n_samples,
                       sample_offsets, max_t, nullptr, delta_t, bound_kind, bound_p1, bound_p2,
                       bound_table, table_stride, table_len, seed, smooth_unif, noise_rows,
@@ -740,7 +757,7 @@ int ssm_ddm_sdv(const float *v, const float *a, const float *z, const float *t, 
                 const float *noise_rows, int64_t noise_row_len, const float *noise_unif, float *rts,
                 int32_t *choices, int32_t *steps, float *traj, int64_t traj_len,
                 const ssm_launch *launch, void *workspace, size_t workspace_bytes, void *stream) {
-    ssm::SingleCall c{ssm::M_SDV, v, a, z, nullptr, t, deadline, s, sv, nullptr, nullptr, nullptr,
+    ssm::SingleCall c{ssm::M_SDV, v, a, z, nullptr, t, deadline, s, sv, nullptr, nullptr, nullptr, nullptr, 0, 0,
                       n_trials, n_samples, sample_offsets, max_t, nullptr, delta_t, bound_kind,
                       bound_p1, bound_p2, bound_table, table_stride, table_len, seed, smooth_unif,
                       noise_rows, noise_row_len, noise_unif, rts, choices, steps, traj, traj_len,
@@ -757,7 +774,7 @@ int ssm_full_ddm(const float *v, const float *a, const float *z, const float *t,
                  const float *noise_unif, float *rts, int32_t *choices, int32_t *steps, float *traj,
                  int64_t traj_len, const ssm_launch *launch, void *workspace,
                  size_t workspace_bytes, void *stream) {
-    ssm::SingleCall c{ssm::M_FULL, v, a, z, nullptr, t, deadline, s, sv, sz, st, nullptr,
+    ssm::SingleCall c{ssm::M_FULL, v, a, z, nullptr, t, deadline, s, sv, sz, st, nullptr, nullptr, 0, 0,
                       n_trials, n_samples, sample_offsets, max_t, nullptr, delta_t, bound_kind,
                       bound_p1, bound_p2, bound_table, table_stride, table_len, seed, smooth_unif,
                       noise_rows, noise_row_len, noise_unif, rts, choices, steps, traj, traj_len,
@@ -775,11 +792,28 @@ int ssm_ornstein_uhlenbeck(const float *v, const float *a, const float *z, const
                            float *rts, int32_t *choices, int32_t *steps, float *traj,
                            int64_t traj_len, const ssm_launch *launch, void *workspace,
                            size_t workspace_bytes, void *stream) {
-    ssm::SingleCall c{ssm::M_OU, v, a, z, nullptr, t, deadline, s, nullptr, nullptr, nullptr, g,
+    ssm::SingleCall c{ssm::M_OU, v, a, z, nullptr, t, deadline, s, nullptr, nullptr, nullptr, g, nullptr, 0, 0,
                       n_trials, n_samples, sample_offsets, max_t, nullptr, delta_t, bound_kind,
                       bound_p1, bound_p2, bound_table, table_stride, table_len, seed, smooth_unif,
                       noise_rows, noise_row_len, noise_unif, rts, choices, steps, traj, traj_len,
                       launch, workspace, workspace_bytes, stream};
+    return ssm::run_single(c);
+}
+
+int ssm_ddm_flex(const float *v, const float *a, const float *z, const float *t, const float *deadline,
+                 const float *s, int64_t n_trials, int64_t n_samples, const int64_t *sample_offsets,
+                 float max_t, float delta_t, int bound_kind, const float *bound_p1,
+                 const float *bound_p2, const float *bound_table, int64_t table_stride,
+                 int64_t table_len, const float *drift_table, int64_t drift_stride, int64_t drift_len,
+                 uint64_t seed, int smooth_unif, const float *noise_rows, int64_t noise_row_len,
+                 const float *noise_unif, float *rts, int32_t *choices, int32_t *steps, float *traj,
+                 int64_t traj_len, const ssm_launch *launch, void *workspace,
+                 size_t workspace_bytes, void *stream) {
+    ssm::SingleCall c{ssm::M_DFLEX, v, a, z, nullptr, t, deadline, s, nullptr, nullptr, nullptr, nullptr,
+                      drift_table, drift_stride, drift_len, n_trials, n_samples, sample_offsets, max_t,
+                      nullptr, delta_t, bound_kind, bound_p1, bound_p2, bound_table, table_stride,
+                      table_len, seed, smooth_unif, noise_rows, noise_row_len, noise_unif, rts, choices,
+                      steps, traj, traj_len, launch, workspace, workspace_bytes, stream};
     return ssm::run_single(c);
 }
 

@@ -17,8 +17,9 @@ import torch
 from . import _device as D
 from . import boundary_functions as bf
 from . import device as dev
+from . import drift_functions as dfn
 
-SINGLE = ("ddm_flexbound", "levy_flexbound", "ddm", "full_ddm", "ddm_sdv", "ornstein_uhlenbeck")
+SINGLE = ("ddm_flexbound", "levy_flexbound", "ddm", "full_ddm", "ddm_sdv", "ornstein_uhlenbeck", "ddm_flex")
 _PER_TRIAL = {"full_ddm": ("sz", "sv", "st"), "ddm_sdv": ("sv",), "ornstein_uhlenbeck": ("g",)}
 RACE = ("race_model", "lca")
 
@@ -41,7 +42,8 @@ class SetBatch:
     """
 
     def __init__(self, sim_name: str, kwargs: dict, boundary: dict, n_samples: int, *,
-                 max_t: float, delta_t: float, smooth_unif: bool = True, n_samples_per_set=None):
+                 max_t: float, delta_t: float, smooth_unif: bool = True, n_samples_per_set=None,
+                 drift: dict | None = None):
         D.require_cuda()
         K = int(np.asarray(kwargs["v"]).shape[0])
         ns = (np.full(K, int(n_samples), np.int64) if n_samples_per_set is None
@@ -68,6 +70,11 @@ class SetBatch:
             self.deadline, self.s = _dev(_col(kwargs["deadline"], K), K), _dev(_col(kwargs["s"], K), K)
             self.alpha = _dev(_col(kwargs["alpha"], K), K) if sim_name == "levy_flexbound" else None
             self.extra = {k: _dev(_col(kwargs[k], K), K, k) for k in _PER_TRIAL.get(sim_name, ())}
+            if sim_name == "ddm_flex":
+                if not drift:
+                    raise ValueError("ddm_flex needs the drift dict (drift_fun, drift_params)")
+                tab = dfn.drift_table(drift["drift_fun"], drift["drift_params"], K, bf.make_t_s(max_t, delta_t))
+                self.extra["drift_table"] = D.to_dev_f32(tab).reshape(tab.shape)
         elif sim_name in RACE:
             v = np.asarray(kwargs["v"], np.float32)
             self.n_acc = int(v.shape[1])
@@ -119,8 +126,9 @@ class SetBatch:
 
 def simulate_sets(sim_name: str, kwargs: dict, boundary: dict, n_samples: int, *,
                   max_t: float, delta_t: float, seed: int, smooth_unif: bool = True,
-                  n_samples_per_set=None, want_steps: bool = False) -> dev.SimOutput:
+                  n_samples_per_set=None, want_steps: bool = False, drift: dict | None = None) -> dev.SimOutput:
     """Simulate K parameter sets (K = len of the per-trial arrays) with
     n_samples each (or n_samples_per_set[k]) in the set-major ragged layout."""
     return SetBatch(sim_name, kwargs, boundary, n_samples, max_t=max_t, delta_t=delta_t,
-                    smooth_unif=smooth_unif, n_samples_per_set=n_samples_per_set).run(seed, want_steps)
+                    smooth_unif=smooth_unif, n_samples_per_set=n_samples_per_set,
+                    drift=drift).run(seed, want_steps)

@@ -24,6 +24,7 @@ import numpy as np
 
 from .. import boundary_functions as bf
 from .. import cssm
+from .. import drift_functions as dfn
 from ..transforms import (ColumnStackParameters, DeleteParameters, ExpandDimension,
                           RenameParameter, SetValue, SetZeroArray, SwapIfLessConstraint,
                           TileColumns)
@@ -37,6 +38,7 @@ _SIMULATORS = {
     "ddm_flexbound": cssm.ddm_flexbound, "ddm": cssm.ddm, "race_model": cssm.race_model,
     "lca": cssm.lca, "levy_flexbound": cssm.levy_flexbound, "lba_vanilla": cssm.lba_vanilla,
     "full_ddm": cssm.full_ddm, "ddm_sdv": cssm.ddm_sdv, "ornstein_uhlenbeck": cssm.ornstein_uhlenbeck,
+    "ddm_flex": cssm.ddm_flex,
 }
 
 
@@ -82,6 +84,9 @@ def _build(name: str) -> dict:
         "simulator": _SIMULATORS[e["simulator"]],
         "parameter_transforms": {"sampling": sampling, "simulation": simulation},
     }
+    if e.get("drift_name"):
+        cfg["drift_name"] = e["drift_name"]
+        cfg["drift_fun"] = dfn.DRIFTS[e["drift_name"]][0]
     cfg["param_bounds_dict"] = {p: (lo, hi) for p, lo, hi in
                                 zip(cfg["params"], cfg["param_bounds"][0], cfg["param_bounds"][1])}
     return cfg
@@ -128,6 +133,41 @@ def register_boundary(name, function, params):
     _BOUNDARY_REGISTRY.register(name, function, params)
 
 
+class DriftRegistry:
+    """Name -> {"fun", "params"} (the reference's drift registry)."""
+
+    def __init__(self):
+        self._d = {name: {"fun": fun, "params": list(params)} for name, (fun, params) in dfn.DRIFTS.items()}
+
+    def register(self, name, function, params):
+        if name in self._d:
+            raise ValueError(f"Drift '{name}' is already registered. "
+                             f"Use a different name or unregister the existing drift first.")
+        self._d[name] = {"fun": function, "params": list(params)}
+
+    def get(self, name):
+        if name not in self._d:
+            raise KeyError(f"Drift '{name}' is not registered. Available drifts: {sorted(self._d)}")
+        return dict(self._d[name])
+
+    def is_registered(self, name):
+        return name in self._d
+
+    def list_drifts(self):
+        return sorted(self._d)
+
+
+_DRIFT_REGISTRY = DriftRegistry()
+
+
+def get_drift_registry() -> DriftRegistry:
+    return _DRIFT_REGISTRY
+
+
+def register_drift(name, function, params):
+    _DRIFT_REGISTRY.register(name, function, params)
+
+
 class ModelConfigBuilder:
     @staticmethod
     def from_model(model_name: str, **overrides) -> dict:
@@ -169,4 +209,4 @@ class ModelConfigBuilder:
 
 
 __all__ = ["model_config", "get_model_config", "ModelConfigBuilder", "get_boundary_registry",
-           "register_boundary", "DEADLINE_PARAM_CONFIG"]
+           "register_boundary", "get_drift_registry", "register_drift", "DEADLINE_PARAM_CONFIG"]

@@ -22,7 +22,7 @@ from pathlib import Path
 HERE = Path(__file__).resolve().parent
 REPO = HERE.parents[2]
 SIMULATORS = {"ddm_flexbound", "ddm", "race_model", "lca", "levy_flexbound", "lba_vanilla", "full_ddm",
-              "ddm_sdv", "ornstein_uhlenbeck"}
+              "ddm_sdv", "ornstein_uhlenbeck", "ddm_flex"}
 
 
 def _import_reference(root: Path):
@@ -75,6 +75,7 @@ def main() -> None:
             "nchoices": int(cfg["nchoices"]),
             "choices": [int(c) for c in cfg.get("choices", list(range(int(cfg["nchoices"]))))],
             "n_particles": int(cfg["n_particles"]), "simulator": sim,
+            "drift_name": cfg.get("drift_name"),
         }
     (HERE / "model_table.json").write_text(json.dumps(table, indent=1))
     print(f"wrote {len(table)} models to {HERE / 'model_table.json'}")

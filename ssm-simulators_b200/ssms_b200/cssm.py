@@ -15,6 +15,7 @@ import numpy as np
 from . import _lib
 from . import boundary_functions as bf
 from . import device as dev
+from . import drift_functions as dfn
 
 DTYPE = np.float32
 
@@ -59,7 +60,7 @@ def _traj_host(traj_t, n):
 
 def _run_flex(model, v, a, z, t, deadline, s, levy_alpha, max_t, delta_t, n_samples, n_trials,
               boundary_fun, boundary_params, random_state, return_option, smooth_unif, extra,
-              per_trial=None, meta_params=None):
+              per_trial=None, meta_params=None, drift_table=None):
     """Shared driver of the flexible-bound single-accumulator simulators.
     ``per_trial``: extra float32 per-trial arrays of the model (sv, sz, st, g);
     ``meta_params``: the parameter entries of the full metadata, in the
@@ -80,7 +81,7 @@ def _run_flex(model, v, a, z, t, deadline, s, levy_alpha, max_t, delta_t, n_samp
     per_trial = {k: _f32(x, k) for k, x in (per_trial or {}).items()}
     out = dev.simulate_single(
         model, v=v, z=z, t=t, deadline=deadline, s=s, a=spec["a"],
-        alpha=alpha, n_trials=n_trials, **per_trial,
+        alpha=alpha, n_trials=n_trials, drift_table=drift_table, **per_trial,
         n_samples=n_samples, max_t=max_t, delta_t=delta_t, bound_kind=spec["kind"],
         bound_p1=spec["p1"], bound_p2=spec["p2"], bound_table=spec["table"],
         seed=_seed(random_state), smooth_unif=smooth_unif,
@@ -164,6 +165,29 @@ def ornstein_uhlenbeck(v, z, g, t, deadline, s, delta_t=0.001, max_t=20, n_sampl
     return _run_flex("ornstein_uhlenbeck", v, a, z, t, deadline, s, None, max_t, delta_t, n_samples,
                      n_trials, boundary_fun, boundary_params, random_state, return_option, smooth_unif,
                      kwargs, per_trial={"g": g}, meta_params=f)
+
+
+def ddm_flex(v, a, z, t, deadline, s, delta_t=0.001, max_t=20, n_samples=20000, n_trials=1,
+             boundary_fun=None, drift_fun=None, boundary_params={}, drift_params={},  # noqa: B006
+             random_state=None, return_option="full", smooth_unif=False, n_threads=1, **kwargs):
+    """DDM with flexible bounds and a time-varying drift v(t) = drift_fun(t,
+    **drift_params) (src/cssm/ddm_models.pyx:884-1193).  The drift function is
+    evaluated per trial on the time grid (the reference's own procedure) into
+    the table the kernel reads; ``v`` is carried by the drift function."""
+    _check_return_option(return_option)
+    if drift_fun is None:
+        raise TypeError("drift_fun is required")
+    n_trials = int(n_trials)
+    table = dfn.drift_table(drift_fun, drift_params, n_trials, bf.make_t_s(max_t, delta_t))
+    out = _run_flex("ddm_flex", v, a, z, t, deadline, s, None, max_t, delta_t, n_samples, n_trials,
+                    boundary_fun, boundary_params, random_state, return_option, smooth_unif, kwargs,
+                    drift_table=table)
+    meta = out["metadata"]
+    meta["drift_fun_type"] = boundary_fun.__name__  # as the reference records it
+    if return_option == "full":
+        meta.update(drift_params)
+        meta["drift"] = table[-1].copy() if n_trials > 0 else np.zeros(table.shape[1], np.float32)
+    return out
 
 
 def ddm(v, a, z, t, deadline, s, max_t=20, delta_t=0.001, n_samples=20000, n_trials=10,

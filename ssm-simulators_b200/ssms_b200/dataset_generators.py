@@ -367,7 +367,7 @@ class BatchedKdePipeline:
         K = prep["n_trials"]
         sim_name = self.model_config["simulator"].__name__
         out = simulate_sets(sim_name, prep["theta"], prep["boundary"], N, max_t=max_t, delta_t=dt,
-                            seed=seed, smooth_unif=sc.get("smooth_unif", True))
+                            seed=seed, smooth_unif=sc.get("smooth_unif", True), drift=prep["drift"])
         rts, chs = out.rts, out.choices
         soff = torch.arange(0, (K + 1) * N, N, dtype=torch.int64, device="cuda")
         pc = list(self.model_config["choices"])

@@ -24,7 +24,8 @@ MODEL_LEVY = "levy_flexbound"
 MODEL_SDV = "ddm_sdv"
 MODEL_FULL = "full_ddm"
 MODEL_OU = "ornstein_uhlenbeck"
-SINGLE_MODELS = (MODEL_FLEX, MODEL_LEGACY, MODEL_LEVY, MODEL_SDV, MODEL_FULL, MODEL_OU)
+MODEL_DFLEX = "ddm_flex"
+SINGLE_MODELS = (MODEL_FLEX, MODEL_LEGACY, MODEL_LEVY, MODEL_SDV, MODEL_FULL, MODEL_OU, MODEL_DFLEX)
 
 
 @dataclass
@@ -41,6 +42,7 @@ def _opt_f32(x, n, name):
 
 
 def simulate_single(model: str, *, v, z, t, deadline, s, a=None, alpha=None, sv=None, sz=None, st=None, g=None,
+                    drift_table=None,
                     n_trials: int, n_samples: int = 0, sample_offsets=None,
                     max_t: float = 20.0, max_t_per_trial=None, delta_t: float = 0.001,
                     bound_kind: int = _lib.BOUND_CONSTANT, bound_p1=None, bound_p2=None,
@@ -134,6 +136,18 @@ def simulate_single(model: str, *, v, z, t, deadline, s, a=None, alpha=None, sv=
             int(n_samples), D.ptr(offs), float(np.float32(max_t)), float(np.float32(delta_t)),
             int(bound_kind), D.ptr(p1t), D.ptr(p2t), D.ptr(tab), tstride, tlen, *common_tail,
             ctypes.addressof(lopt), D.ptr(ws), ws.numel(), sp)
+    elif model == MODEL_DFLEX:
+        if drift_table is None:
+            raise ValueError("ddm_flex needs drift_table (float32 [n_trials, len])")
+        dtab = D.to_dev_f32(drift_table).reshape(-1)
+        dlen = int(drift_table.shape[-1])
+        if dlen < 1 or dtab.numel() < K * dlen:
+            raise ValueError("drift_table must be float32 [n_trials, len]")
+        status = L.ssm_ddm_flex(
+            D.ptr(vt), D.ptr(at), D.ptr(zt), D.ptr(tt), D.ptr(dlt), D.ptr(s_t), K, int(n_samples), D.ptr(offs),
+            float(np.float32(max_t)), float(np.float32(delta_t)), int(bound_kind), D.ptr(p1t), D.ptr(p2t),
+            D.ptr(tab), tstride, tlen, D.ptr(dtab), dlen, dlen, *common_tail, ctypes.addressof(lopt),
+            D.ptr(ws), ws.numel(), sp)
     elif model in (MODEL_SDV, MODEL_FULL, MODEL_OU):
         bound_args = (K, int(n_samples), D.ptr(offs), float(np.float32(max_t)), float(np.float32(delta_t)),
                       int(bound_kind), D.ptr(p1t), D.ptr(p2t), D.ptr(tab), tstride, tlen, *common_tail,

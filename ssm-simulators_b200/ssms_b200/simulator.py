@@ -20,7 +20,7 @@ from threading import Lock
 
 import numpy as np
 
-from .config import ModelConfigBuilder, get_boundary_registry
+from .config import ModelConfigBuilder, get_boundary_registry, get_drift_registry
 from .transforms import apply_all
 
 OMISSION_SENTINEL: float = -999.0
@@ -118,6 +118,20 @@ def make_boundary_dict(config: dict, theta: dict) -> dict:
     return {"boundary_params": {p: v for p, v in theta.items() if p in names}, "boundary_fun": fun}
 
 
+def make_drift_dict(config: dict, theta: dict) -> dict:
+    """drift_fun and the drift's parameters taken from theta (simulator.py:342-375);
+    a callable drift with its own ``drift_params`` list is used as given."""
+    if callable(config.get("drift")) and config.get("drift_params") and not get_drift_registry().is_registered(
+            config.get("drift_name", "")):
+        names, fun = config["drift_params"], config["drift"]
+    elif "drift_name" in config:
+        info = get_drift_registry().get(config["drift_name"])
+        names, fun = info["params"], info["fun"]
+    else:
+        return {}
+    return {"drift_fun": fun, "drift_params": {p: v for p, v in theta.items() if p in names}}
+
+
 def validate_ssm_parameters(model: str, theta: dict) -> None:
     """The reference's parameter checks (simulator.py:500-581) for the models here."""
     if model == "lba_3_vs_constraint":
@@ -169,9 +183,6 @@ class Simulator:
 
     def __init__(self, model=None, boundary=None, drift=None, simulator_function=None,
                  parameter_adapter=None, parameter_adaptations=None, **config_overrides):
-        if drift is not None:
-            raise ValueError("drift functions belong to the ddm_flex simulator family, which this "
-                             "package does not implement")
         self._parameter_adapter = parameter_adapter
         self._custom_adaptations = list(parameter_adaptations or [])
         if isinstance(model, dict):
@@ -188,6 +199,8 @@ class Simulator:
             config["simulator"] = simulator_function
         if boundary is not None:
             self._apply_boundary(config, boundary)
+        if drift is not None:
+            self._apply_drift(config, drift)
         for field in ("params", "nchoices", "simulator"):
             if field not in config:
                 raise ValueError(f"Configuration missing required field: '{field}'")
@@ -218,6 +231,30 @@ class Simulator:
         for p in config.get("params", []):
             if p not in params:
                 raise ValueError(f"Simulator function '{fn.__name__}' is missing required model parameter '{p}'")
+
+    @staticmethod
+    def _apply_drift(config, drift):
+        """A drift by registry name or a callable taking t first (simulator_class.py:404-446)."""
+        if isinstance(drift, str):
+            reg = get_drift_registry()
+            if not reg.is_registered(drift):
+                raise ValueError(f"Unknown drift '{drift}'. Available drifts: {reg.list_drifts()}")
+            info = reg.get(drift)
+            config["drift_name"], config["drift"] = drift, info["fun"]
+            config.setdefault("drift_params", info["params"])
+        elif callable(drift):
+            names = list(inspect.signature(drift).parameters)
+            if not names or names[0] != "t":
+                raise ValueError(f"Drift function '{getattr(drift, '__name__', drift)}' must accept 't' as "
+                                 "first positional argument")
+            config["drift"] = drift
+            config["drift_name"] = getattr(drift, "__name__", "custom")
+            if "drift_params" not in config:
+                warnings.warn("Custom drift function provided without 'drift_params'. "
+                              "You may need to specify drift parameter names.", UserWarning)
+                config["drift_params"] = []
+        else:
+            raise ValueError("drift must be a string name or callable function")
 
     @staticmethod
     def _apply_boundary(config, boundary):
@@ -268,9 +305,10 @@ class Simulator:
         for tr in self._custom_adaptations:
             theta = tr.apply(theta, cfg, n_trials)
         boundary_dict = make_boundary_dict(cfg, theta) if ("boundary_name" in cfg or "boundary" in cfg) else {}
+        drift_dict = make_drift_dict(cfg, theta) if ("drift_name" in cfg or "drift" in cfg) else {}
         validate_ssm_parameters(model_name, theta)
         return {"config": cfg, "model_name": model_name, "n_trials": n_trials, "theta": theta,
-                "boundary": boundary_dict, "sim_params": sim_params}
+                "boundary": boundary_dict, "drift": drift_dict, "sim_params": sim_params}
 
     def simulate(self, theta, n_samples: int = 1000, delta_t: float = 0.001, max_t: float = 20,
                  no_noise: bool = False, sigma_noise=None, smooth_unif: bool = True,
@@ -282,7 +320,7 @@ class Simulator:
                             n_threads=n_threads)
         cfg, model_name, n_trials = prep["config"], prep["model_name"], prep["n_trials"]
         theta, boundary_dict, sim_params = prep["theta"], prep["boundary"], prep["sim_params"]
-        x = cfg["simulator"](**theta, **boundary_dict, **sim_params, **(extra_fields or {}))
+        x = cfg["simulator"](**theta, **boundary_dict, **prep["drift"], **sim_params, **(extra_fields or {}))
         if not isinstance(x, dict):
             raise TypeError(f"Simulator returned {type(x).__name__}, expected dict")
         if n_trials == 1:

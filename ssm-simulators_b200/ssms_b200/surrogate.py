@@ -354,7 +354,7 @@ def kde_loglik(model: str, theta, rt, choice, *, n_samples: int = 100_000, delta
                        max_t=max_t, random_state=seed % (2 ** 31))
     K = prep["n_trials"]
     o = simulate_sets(cfg["simulator"].__name__, prep["theta"], prep["boundary"], n_samples, max_t=max_t,
-                      delta_t=delta_t, seed=seed)
+                      delta_t=delta_t, seed=seed, drift=prep["drift"])
     soff = torch.arange(0, (K + 1) * n_samples, n_samples, dtype=torch.int64, device="cuda")
     pc = list(cfg["choices"])
     kb = KdeBatch(o.rts, o.choices, soff, pc)

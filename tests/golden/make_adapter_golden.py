@@ -74,6 +74,12 @@ def main():
         for k, v in rec.items():
             if k == "boundary_fun":
                 meta[f"{name}|boundary_fun"] = v.__name__
+            elif k == "drift_fun":
+                meta[f"{name}|drift_fun"] = table[name]["drift_name"]
+            elif k == "drift_params":
+                for dk, dv in v.items():
+                    arrays[f"{name}|dp|{dk}"] = np.asarray(dv)
+                meta[f"{name}|dp_keys"] = sorted(v)
             elif k == "boundary_params":
                 for bk, bv in v.items():
                     arrays[f"{name}|bp|{bk}"] = np.asarray(bv)

@@ -4,6 +4,8 @@ oracle/build_ref.py): inputs plus rts, choices and the recorded trajectory of
 small fixed-seed cases, stored as .npz fixtures in this directory.
 
 Usage:  python oracle/build_ref.py && python tests/golden/make_golden_var.py
+        python tests/golden/make_golden_var.py --flex [REFERENCE_ROOT]   (ddm_flex cases; the
+        reference's drift functions are loaded from its source tree)
 """
 
 from __future__ import annotations
@@ -70,5 +72,63 @@ def main():
     _case("ornstein_angle", "ornstein_uhlenbeck", bf.angle, ["a", "theta"], th, 500, 35, False)
 
 
-if __name__ == "__main__":
+if __name__ == "__main__" and "--flex" not in sys.argv:
     main()
+
+
+def _reference_drifts():
+    """The reference's drift functions, loaded from its source file."""
+    import importlib.util
+
+    ref = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    spec = importlib.util.spec_from_file_location("ref_drift_functions",
+                                                  ref / "ssms" / "basic_simulators" / "drift_functions.py")
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def main_flex():
+    from cssm.ddm_models import ddm_flex
+
+    df = _reference_drifts()
+    cases = [
+        ("ddm_flex_constant", bf.constant, ["a"], df.constant, ["v"],
+         {"v": f32([1.0, -0.7, 0.3]), "a": f32([1.5, 1.0, 2.0]), "z": f32([0.5, 0.4, 0.6]),
+          "t": f32([0.3, 0.5, 0.2])}, True),
+        ("ddm_flex_gamma_angle", bf.angle, ["a", "theta"], df.gamma_drift, ["v", "shape", "scale", "c"],
+         {"v": f32([0.5, -0.3]), "a": f32([1.6, 1.2]), "z": f32([0.5, 0.45]), "t": f32([0.2, 0.4]),
+          "theta": f32([0.3, 0.7]), "shape": f32([2.5, 3.0]), "scale": f32([0.05, 0.2]), "c": f32([1.5, -1.0])},
+         False),
+        ("ddm_flex_conflict_ds", bf.constant, ["a"], df.conflict_ds_drift,
+         ["v", "tinit", "dinit", "tslope", "dslope", "tfixedp", "tcoh", "dcoh"],
+         {"v": f32([0.0, 0.2]), "a": f32([2.0, 1.5]), "z": f32([0.5, 0.5]), "t": f32([0.3, 0.2]),
+          "tinit": f32([2.0, 1.0]), "dinit": f32([2.0, 3.0]), "tslope": f32([2.0, 1.0]), "dslope": f32([2.0, 4.0]),
+          "tfixedp": f32([3.0, 2.0]), "tcoh": f32([0.5, 0.8]), "dcoh": f32([-0.5, 0.3])}, True),
+        ("ddm_flex_attend", bf.constant, ["a"], df.attend_drift, ["v", "ptarget", "pouter", "pinner", "r", "sda"],
+         {"v": f32([0.0, 0.1]), "a": f32([1.2, 1.6]), "z": f32([0.5, 0.55]), "t": f32([0.25, 0.35]),
+          "ptarget": f32([0.8, -0.5]), "pouter": f32([-0.4, 0.6]), "pinner": f32([0.3, -0.2]), "r": f32([1.0, 3.0]),
+          "sda": f32([2.0, 1.5])}, True),
+        ("ddm_flex_stimflexrel1", bf.constant, ["a"], df.conflict_stimflexrel1_drift,
+         ["v", "vt", "vd", "tcoh", "dcoh", "tonset", "donset"],
+         {"v": f32([0.0, 0.3]), "a": f32([1.8, 1.4]), "z": f32([0.5, 0.5]), "t": f32([0.2, 0.3]),
+          "vt": f32([2.0, 1.0]), "vd": f32([2.0, 1.5]), "tcoh": f32([0.5, 0.8]), "dcoh": f32([-0.5, 0.2]),
+          "tonset": f32([0.2, 0.0]), "donset": f32([0.0, 0.4])}, False),
+    ]
+    for i, (name, bfun, bkeys, dfun, dkeys, th, smooth) in enumerate(cases):
+        K = th["z"].shape[0]
+        dl, s = f32([999] * K), f32([1.0] * K)
+        out = ddm_flex(th["v"], th["a"], th["z"], th["t"], dl, s, max_t=20.0, delta_t=0.001, n_samples=500,
+                       n_trials=K, boundary_fun=bfun, drift_fun=dfun,
+                       boundary_params={k: th[k] for k in bkeys}, drift_params={k: th[k] for k in dkeys},
+                       random_state=40 + i, smooth_unif=smooth)
+        _save(name, model="ddm_flex", boundary=bfun.__name__, bkeys=np.array(bkeys),
+              drift=getattr(dfun, "__name__", None) or name.replace("ddm_flex_", ""), dkeys=np.array(dkeys),
+              seed=40 + i, smooth=smooth, max_t=20.0, dt=0.001, n=500, deadline=dl, s=s,
+              **{f"theta_{k}": v for k, v in th.items()}, rts=out["rts"], choices=out["choices"].astype(np.int8),
+              trajectory=out["metadata"]["trajectory"], boundary0=out["metadata"]["boundary"])
+
+
+if __name__ == "__main__" and "--flex" in sys.argv:
+    sys.argv.remove("--flex")
+    main_flex()

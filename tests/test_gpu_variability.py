@@ -161,3 +161,90 @@ def test_simulator_api_and_batched_sets(cuda, model):
         p_set = np.mean(ch[k] == 1)
         se = np.sqrt(max(p_api * (1 - p_api), 1e-6) * 2 / 20000)
         assert abs(p_set - p_api) < 4 * se, (p_set, p_api)
+
+
+# ------------------------------------------------------------------ ddm_flex (drift functions)
+def _flex_theta(rng, K):
+    th = {"v": f32(rng.uniform(-1, 1, K)), "a": f32(rng.uniform(0.8, 2.0, K)), "z": f32(rng.uniform(0.35, 0.65, K)),
+          "t": f32(rng.uniform(0.1, 0.6, K)), "theta": f32(rng.uniform(0.0, 0.9, K)),
+          "shape": f32(rng.uniform(2.0, 3.5, K)), "scale": f32(rng.uniform(0.05, 0.3, K)), "c": f32(rng.uniform(-1.5, 1.5, K)),
+          "tinit": f32(rng.uniform(0, 3, K)), "dinit": f32(rng.uniform(0, 3, K)), "tslope": f32(rng.uniform(0.5, 4, K)),
+          "dslope": f32(rng.uniform(0.5, 4, K)), "tfixedp": f32(rng.uniform(0, 3, K)), "tcoh": f32(rng.uniform(-1, 1, K)),
+          "dcoh": f32(rng.uniform(-1, 1, K)), "ptarget": f32(rng.uniform(-1, 1, K)), "pouter": f32(rng.uniform(-1, 1, K)),
+          "pinner": f32(rng.uniform(-1, 1, K)), "r": f32(rng.uniform(0.5, 3, K)), "sda": f32(rng.uniform(1, 3, K))}
+    return th
+
+
+FLEX_CASES = [("constant", "constant"), ("gamma_drift", "angle"), ("conflict_ds_drift", "constant"),
+              ("attend_drift", "angle"), ("attend_drift_simple", "constant")]
+
+
+@pytest.mark.parametrize("drift,bname", FLEX_CASES)
+def test_ddm_flex_noise_injection_bit_exact(cuda, oracle, drift, bname):
+    from ssms_b200 import drift_functions as dfn
+
+    rng = np.random.default_rng(zlib.crc32(f"flex/{drift}/{bname}".encode()))
+    K, N, max_t = 4, 400, 3.0
+    th = _flex_theta(rng, K)
+    fun, keys = bf.BOUNDARIES[bname]
+    bp = {k: th[k] for k in keys}
+    dfun, dkeys = dfn.DRIFTS[drift]
+    dp = {k: th[k] for k in dkeys}
+    t_s = bf.make_t_s(max_t, 0.001)
+    spec = bf.kernel_spec(fun, bp, K, t_s)
+    table = dfn.drift_table(dfun, dp, K, t_s)
+    total = K * N
+    rows = rng.standard_normal((total, int(max_t / 0.001) + 80), dtype=np.float32)
+    unif = f32(rng.uniform(0, 1, total))
+    out = dev.simulate_single("ddm_flex", v=th["v"], z=th["z"], t=th["t"], deadline=f32([999] * K), s=f32([1] * K),
+                              a=spec["a"], drift_table=table, n_trials=K, n_samples=N, max_t=max_t, delta_t=0.001,
+                              bound_kind=spec["kind"], bound_p1=spec["p1"], bound_p2=spec["p2"],
+                              bound_table=spec["table"], smooth_unif=True, noise_rows=rows, noise_unif=unif,
+                              want_steps=True)
+    o_rt, o_ch, o_st, _ = oracle.ddm_flex(th["z"], th["t"], f32([999] * K), f32([1] * K), max_t=max_t, delta_t=0.001,
+                                          n_samples=N, n_trials=K, boundary_fun=fun, boundary_params=bp,
+                                          drift_fun=dfun, drift_params=dp, smooth_unif=True, rows=rows, unif=unif)
+    np.testing.assert_array_equal(out.steps.cpu().numpy(), o_st)
+    np.testing.assert_array_equal(out.choices.cpu().numpy(), o_ch)
+    np.testing.assert_array_equal(_bits(out.rts.cpu().numpy()), _bits(o_rt))
+
+
+@pytest.mark.parametrize("drift,bname", [("gamma_drift", "constant"), ("conflict_ds_drift", "angle")])
+def test_ddm_flex_device_rng_matches_reference_distribution(cuda, oracle, drift, bname):
+    from ssms_b200 import drift_functions as dfn
+
+    rng = np.random.default_rng(5)
+    th = {k: v[:1] for k, v in _flex_theta(rng, 1).items()}
+    fun, keys = bf.BOUNDARIES[bname]
+    bp = {k: th[k] for k in keys}
+    dfun, dkeys = dfn.DRIFTS[drift]
+    dp = {k: th[k] for k in dkeys}
+    N = 100_000
+    out = cssm.ddm_flex(th["v"], th["a"], th["z"], th["t"], f32([999]), f32([1]), n_samples=N, n_trials=1,
+                        boundary_fun=fun, boundary_params=bp, drift_fun=dfun, drift_params=dp, random_state=11,
+                        smooth_unif=True, return_option="minimal")
+    r = oracle.ddm_flex(th["z"], th["t"], f32([999]), f32([1]), max_t=20.0, delta_t=0.001, n_samples=N, n_trials=1,
+                        boundary_fun=fun, boundary_params=bp, drift_fun=dfun, drift_params=dp, smooth_unif=True,
+                        random_state=12)
+    _compare_dist(out["rts"].reshape(-1), out["choices"].reshape(-1), r[0], r[1], [-1, 1], alpha_ks=0.005)
+
+
+@pytest.mark.parametrize("model", ["conflict_ds", "gamma_drift_angle", "shrink_spot", "conflict_stimflexrel1"])
+def test_ddm_flex_models_through_simulator_and_sets(cuda, model):
+    from ssms_b200 import Simulator, model_config
+    from ssms_b200.batch_models import simulate_sets
+
+    cfg = model_config[model]
+    theta = dict(zip(cfg["params"], cfg["default_params"]))
+    out = Simulator(model).simulate(theta, n_samples=20000, random_state=5)
+    assert out["rts"].shape == (20000, 1) and out["metadata"]["simulator"] == "ddm_flex"
+    assert out["metadata"]["drift"].shape == (20001,)
+    prep = Simulator(model).prepare({k: np.full(2, v, np.float32) for k, v in theta.items()}, n_samples=20000,
+                                    random_state=6)
+    o = simulate_sets("ddm_flex", prep["theta"], prep["boundary"], 20000, max_t=20.0, delta_t=0.001, seed=6,
+                      drift=prep["drift"])
+    ch = o.choices.cpu().numpy().reshape(2, 20000)
+    p_api = np.mean(out["choices"][:, 0] == 1)
+    for k in range(2):
+        se = np.sqrt(max(p_api * (1 - p_api), 1e-6) * 2 / 20000)
+        assert abs(np.mean(ch[k] == 1) - p_api) < 4 * se

@@ -34,7 +34,7 @@ def _recording_config(name):
 
 def test_all_reference_models_with_built_simulators_are_configured():
     assert set(MODELS) == set(model_config)
-    assert len(MODELS) == 40
+    assert len(MODELS) == 54
 
 
 @pytest.mark.parametrize("name", MODELS)
@@ -53,6 +53,15 @@ def test_simulator_hands_the_reference_arguments(name):
     assert sorted(rec["boundary_params"]) == META[f"{name}|bp_keys"]
     for bk in META[f"{name}|bp_keys"]:
         np.testing.assert_array_equal(rec["boundary_params"][bk], ARR[f"{name}|bp|{bk}"])
+    if f"{name}|dp_keys" in META:  # ddm_flex models: the drift function and its parameters
+        from ssms_b200 import drift_functions as dfn
+
+        assert rec["drift_fun"] is dfn.DRIFTS[META[f"{name}|drift_fun"]][0]
+        assert sorted(rec["drift_params"]) == META[f"{name}|dp_keys"]
+        for dk in META[f"{name}|dp_keys"]:
+            np.testing.assert_array_equal(rec["drift_params"][dk], ARR[f"{name}|dp|{dk}"])
+    else:
+        assert "drift_fun" not in rec
     for key in ("n_samples", "n_trials", "max_t", "delta_t", "random_state", "return_option",
                 "smooth_unif", "n_threads", "nact"):
         if f"{name}|{key}" in META:

@@ -129,3 +129,30 @@ def test_ornstein_matches_reference(oracle, name):
     np.testing.assert_array_equal(_bits(rts), _bits(g["rts"].reshape(-1)))
     np.testing.assert_array_equal(chs, g["choices"].reshape(-1).astype(np.int32))
     np.testing.assert_array_equal(_bits(traj), _bits(g["trajectory"][:, 0]))
+
+
+FLEX_DRIFTS = {"ddm_flex_constant": "constant", "ddm_flex_gamma_angle": "gamma_drift",
+               "ddm_flex_conflict_ds": "conflict_ds_drift", "ddm_flex_attend": "attend_drift",
+               "ddm_flex_stimflexrel1": "conflict_stimflexrel1_drift"}
+
+
+@pytest.mark.parametrize("name", sorted(FLEX_DRIFTS))
+def test_ddm_flex_matches_reference(oracle, name):
+    """ddm_flex with the drift table evaluated by this package's drift functions:
+    the reference's rts, choices and trajectory bit for bit, which also pins
+    the drift functions to the reference's."""
+    from ssms_b200 import drift_functions as dfn
+
+    g = _load(name)
+    theta = {k[len("theta_"):]: g[k] for k in g if k.startswith("theta_")}
+    n, K = int(g["n"]), theta["z"].shape[0]
+    fun, dkeys = dfn.DRIFTS[FLEX_DRIFTS[name]]
+    rts, chs, steps, traj = oracle.ddm_flex(
+        theta["z"], theta["t"], g["deadline"], g["s"], max_t=float(g["max_t"]), delta_t=float(g["dt"]),
+        n_samples=n, n_trials=K, boundary_fun=BOUNDS[str(g["boundary"])],
+        boundary_params={k: theta[k] for k in [str(x) for x in g["bkeys"]]}, drift_fun=fun,
+        drift_params={k: theta[k] for k in [str(x) for x in g["dkeys"]]}, smooth_unif=bool(g["smooth"]),
+        random_state=int(g["seed"]), traj_len=g["trajectory"].shape[0])
+    np.testing.assert_array_equal(_bits(rts), _bits(g["rts"].reshape(-1)))
+    np.testing.assert_array_equal(chs, g["choices"].reshape(-1).astype(np.int32))
+    np.testing.assert_array_equal(_bits(traj), _bits(g["trajectory"][:, 0]))
