@@ -247,6 +247,26 @@ int ssm_lca(const float *v, const float *z, const float *g, const float *b, cons
             void *stream);
 
 /*
+ * ssm_racing_diffusion -- replaces cssm.racing_diffusion_model
+ * (src/cssm/race_models.pyx:925-1300): n_particles Wiener accumulators
+ * starting at U(0, A) race to one threshold b without a lower barrier; the
+ * first one (in index order) at or above b wins, and the step that reaches it
+ * does not advance the time.  v: float32 [n_trials, n_particles]; b, A, t, s:
+ * one value per trial.  Choices 0..n_particles-1, -1 with rt -999 when no
+ * accumulator wins before the deadline.  Noise injection: row w holds the
+ * increments step-major (step * n_particles + j); noise_unif holds
+ * n_particles + 1 values per trajectory, the start uniforms then the jitter
+ * uniform.  Workspace: ssm_race_workspace_bytes.
+ */
+int ssm_racing_diffusion(const float *v, const float *b, const float *A, const float *t, const float *s,
+                         const float *deadline, int64_t n_trials, int64_t n_samples, int n_particles,
+                         const int64_t *sample_offsets, float max_t, float delta_t, uint64_t seed,
+                         int smooth_unif, const float *noise_rows, int64_t noise_row_len,
+                         const float *noise_unif, float *rts, int32_t *choices, int32_t *steps,
+                         float *traj, int64_t traj_len, const ssm_launch *launch, void *workspace,
+                         size_t workspace_bytes, void *stream);
+
+/*
  * ssm_lba_vanilla -- replaces cssm.lba_vanilla (src/cssm/lba_models.pyx:36-139):
  * per sample x_j = (a - U(0, z)) / |N(v_j, sd_j)|, choice = argmin_j x_j,
  * rt = min_j x_j + t, rt = -999 when rt >= deadline.  v, sd: float32[n_trials *

@@ -316,6 +316,68 @@ int64_t oracle_dflex_trial(int64_t k, int64_t n_samples, int64_t n_trials, float
 }
 
 /*
+ * One trial of racing_diffusion_model (src/cssm/race_models.pyx:1205-1266):
+ * np accumulators start at U(0, A) (the reference draws these with C rand(),
+ * rand() / RAND_MAX in float), each step updates them in index order,
+ * x_j += v_j dt + sqrt_st g, and the first one at or above b ends the walk
+ * before the time is advanced.  No lower boundary.  Row mode: increments
+ * step-major (step * np + j); uniform row w = [starts..., u_smooth].
+ */
+#include <stdlib.h>
+int64_t oracle_rdm_trial(int64_t k, int64_t n_samples, int64_t n_trials, int np_, const float *v,
+                         float b, float A, float t, float deadline, float sqrt_st, float max_t,
+                         float dt, int smooth, oracle_noise *nz, float *rts, int32_t *choices,
+                         int32_t *steps, float *traj, int64_t traj_len) {
+    float x[64];
+    const float dl = deadline_tmp(max_t, deadline, t);
+    int64_t total_steps = 0;
+    for (int64_t n = 0; n < n_samples; ++n) {
+        const int64_t w = n * n_trials + k;
+        for (int j = 0; j < np_; ++j) {
+            float u;
+            if (nz->rows) u = nz->urows[w * (np_ + 1) + j];
+            else u = ((float)rand()) / RAND_MAX;
+            x[j] = u * A;
+        }
+        float tp = 0.0f;
+        int64_t ix = 0;
+        int winner = -1;
+        const int rec = (traj != 0 && n == 0 && k == 0);
+        if (rec)
+            for (int j = 0; j < np_ && j < traj_len; ++j) traj[j] = x[j];
+        while (winner < 0 && tp <= dl) {
+            for (int j = 0; j < np_; ++j) {
+                const float g = next_g(nz, w, ix * np_ + j, k);
+                x[j] = (x[j] + (v[j] * dt)) + (sqrt_st * g);
+                if (x[j] >= b) {
+                    winner = j;
+                    break;
+                }
+            }
+            if (winner >= 0) break;
+            tp = tp + dt;
+            ix += 1;
+            if (rec && (ix + 1) * np_ <= traj_len)
+                for (int j = 0; j < np_; ++j) traj[ix * np_ + j] = x[j];
+        }
+        const float u = nz->rows ? nz->urows[w * (np_ + 1) + np_] : next_u(nz, w, k);
+        const float sm = smooth_jitter(smooth, tp, dl, dt, u);
+        float rt = (tp + t) + sm;
+        int ch = winner;
+        if (rt >= deadline || deadline <= 0) rt = -999.0f;
+        if (rt == -999.0f || winner < 0) {
+            rt = -999.0f;
+            ch = -1;
+        }
+        rts[w] = rt;
+        choices[w] = ch;
+        if (steps) steps[w] = (int32_t)ix;
+        total_steps += ix;
+    }
+    return total_steps;
+}
+
+/*
  * One trial of race_model (race_models.pyx:417-464) or lca
  * (race_models.pyx:825-879), selected by `lca`.  v, z, sqrt_st hold the
  * trial's np particle values; increments are consumed particle-major within a

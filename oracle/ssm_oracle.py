@@ -75,6 +75,8 @@ def lib():
         L.oracle_dflex_trial.restype = I64
         L.oracle_dflex_trial.argtypes = [I64, I64, I64, F, F, F, F, P, I64, P, I64, F, F, I, NP, P, P, P, P,
                                          I64]
+        L.oracle_rdm_trial.restype = I64
+        L.oracle_rdm_trial.argtypes = [I64, I64, I64, I, P, F, F, F, F, F, F, F, I, NP, P, P, P, P, I64]
         L.oracle_lba_f32.restype = None
         L.oracle_lba_f32.argtypes = [I64, I64, I, P, P, P, P, P, P, P]
         _lib = L
@@ -304,6 +306,36 @@ def ddm_flex(z, t, deadline, s, *, max_t, delta_t, n_samples, n_trials, boundary
         L.oracle_dflex_trial(k, n_samples, n_trials, z[k], t[k], deadline[k], scales[k], _p(tab), tab.shape[0],
                              _p(drift), drift.shape[0], f32(max_t), f32(delta_t), int(bool(smooth_unif)),
                              C.byref(nz), _p(rts), _p(chs), _p(steps), _p(traj), traj_len)
+    if rows is not None and nz.overrun:
+        raise ValueError("noise rows too short for the simulated trajectories")
+    del keep
+    return rts, chs, steps, traj
+
+
+def rdm(v, b, A, t, s, deadline, *, max_t, delta_t, n_samples, n_trials, smooth_unif, random_state=None,
+        rows=None, unif=None, traj_len=0):
+    """racing_diffusion_model (stream or row mode).  v: float32 [n_trials, np];
+    b, A, t, s: one value per trial.  Stream mode seeds C rand() with
+    random_state (the reference's start points) and numpy with the same seed."""
+    L = lib()
+    v = np.ascontiguousarray(np.asarray(v, np.float32))
+    b, A, t, s, deadline = (np.asarray(x, np.float32).reshape(n_trials, -1)[:, 0] for x in (b, A, t, s, deadline))
+    npart = v.shape[1]
+    nd = num_draws(max_t, delta_t, 1) * npart
+    if rows is None:
+        C.CDLL(None).srand(C.c_uint(int(random_state) & 0xFFFFFFFF))
+        strm = _Stream(random_state, _normal_init(nd), _normal_refill)
+        nz, keep = strm.noise, strm
+    else:
+        nz, keep = _rows_noise(rows, unif)
+    rts, chs, steps = _outputs(n_samples, n_trials)
+    traj = np.full(traj_len, -999, np.float32) if traj_len else None
+    sq = (sqrt_dt(delta_t) * s).astype(np.float32)
+    for k in range(n_trials):
+        vk = np.ascontiguousarray(v[k])
+        L.oracle_rdm_trial(k, n_samples, n_trials, npart, _p(vk), b[k], A[k], t[k], deadline[k], sq[k], f32(max_t),
+                           f32(delta_t), int(bool(smooth_unif)), C.byref(nz), _p(rts), _p(chs), _p(steps), _p(traj),
+                           traj_len)
     if rows is not None and nz.overrun:
         raise ValueError("noise rows too short for the simulated trajectories")
     del keep

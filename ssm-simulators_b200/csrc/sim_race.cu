@@ -17,6 +17,12 @@ namespace ssm {
 
 constexpr int RACE_MAX_NP = 16;
 
+// Simulator families sharing this kernel: the race model, the LCA and the
+// racing diffusion model (racing_diffusion_model, race_models.pyx:1150-1266:
+// starts U(0, A), no lower barrier, the first accumulator at or above b wins
+// and the step that reaches it does not advance the time).
+enum RaceFamily { FAM_RACE = 0, FAM_LCA = 1, FAM_RDM = 2 };
+
 // Per-trial header (64 B) followed by v[np], sq[np] (= sqrt(dt)*s), z[np]
 // padded to a multiple of 4 floats.
 struct alignas(16) RaceHead {
@@ -55,6 +61,7 @@ struct RaceParams {
 
 struct RacePrep {
     const float *v, *z, *t, *s, *deadline, *a, *p1, *p2, *g, *b, *table;
+    int per_trial_zs;  // rdm: z (the start range A) and s hold one value per trial
     int64_t n_trials, tstride, row_floats;
     int np, bound;
     float dt, sqrt_dt, max_t;
@@ -88,8 +95,9 @@ __global__ void k_race_prep(const RacePrep A) {
     float *v = row + 16, *sq = v + A.np, *z = sq + A.np;
     for (int j = 0; j < A.np; ++j) {
         v[j] = A.v[k * A.np + j];
-        sq[j] = __fmul_rn(A.sqrt_dt, A.s[k * A.np + j]);  // delta_t_sqrt * s (race_models.pyx:385)
-        z[j] = A.z[k * A.np + j];
+        const int64_t i = A.per_trial_zs ? k : k * A.np + j;
+        sq[j] = __fmul_rn(A.sqrt_dt, A.s[i]);  // delta_t_sqrt * s (race_models.pyx:385)
+        z[j] = A.z[i];
     }
 }
 
@@ -122,12 +130,13 @@ struct RaceLane {
     int ix;
     float ixf, tp;  // race: float32 time accumulator
     double tpd;     // lca: double time accumulator (Cython infers double, race_models.pyx:838)
+    int win;        // rdm: index of the winning accumulator (-1 while racing)
     float x[NP];
 };
 
 // One Euler step of every accumulator.  Returns false when the loop condition
 // failed before the step (the walk is over).
-template <int NP, bool LCA, int BOUND, bool NOISE, bool RECORD>
+template <int NP, int FAM, int BOUND, bool NOISE, bool RECORD>
 __device__ __forceinline__ bool race_step(const RaceParams &p, RaceLane<NP> &L, const RaceHead &h,
                                           const float *v, const float *sq, int np, uint32_t &ctr) {
     if (L.ixf >= h.capf) {
@@ -136,9 +145,12 @@ __device__ __forceinline__ bool race_step(const RaceParams &p, RaceLane<NP> &L, 
     }
     const float bnd = race_bound<BOUND, NOISE>(h, L.ixf, L.ix, p, L.k);
     bool finished = false;
+    if (FAM != FAM_RDM) {  // race / LCA test the bound before the step; RDM after each update
 #pragma unroll
-    for (int j = 0; j < NP; ++j)
-        if (j < np) finished |= (L.x[j] > bnd);
+        for (int j = 0; j < NP; ++j)
+            if (j < np) finished |= (L.x[j] > bnd);
+    }
+    constexpr bool LCA = (FAM == FAM_LCA);
     const bool in_time = LCA ? (L.tpd <= (double)h.dl_tmp) : (L.tp <= h.dl_tmp);
     if (finished || !in_time) return false;
     float gsn[NP];
@@ -189,6 +201,25 @@ __device__ __forceinline__ bool race_step(const RaceParams &p, RaceLane<NP> &L, 
             }
         }
         L.tpd = NOISE ? __dadd_rn(L.tpd, (double)p.dt) : L.tpd + (double)p.dt;
+    } else if (FAM == FAM_RDM) {
+        // no lower barrier; the first accumulator (in index order) at or above b
+        // wins and its step does not advance the time (race_models.pyx:1227-1244)
+        int win = -1;
+#pragma unroll
+        for (int j = 0; j < NP; ++j) {
+            if (j < np) {
+                float xj;
+                if (NOISE) xj = __fadd_rn(__fadd_rn(L.x[j], __fmul_rn(v[j], p.dt)), __fmul_rn(sq[j], gsn[j]));
+                else xj = fmaf(sq[j], gsn[j], L.x[j] + v[j] * p.dt);
+                L.x[j] = xj;
+                if (win < 0 && xj >= bnd) win = j;
+            }
+        }
+        if (win >= 0) {
+            L.win = win;
+            return false;
+        }
+        L.tp = NOISE ? __fadd_rn(L.tp, p.dt) : L.tp + p.dt;
     } else {
 #pragma unroll
         for (int j = 0; j < NP; ++j) {
@@ -209,13 +240,14 @@ __device__ __forceinline__ bool race_step(const RaceParams &p, RaceLane<NP> &L, 
     return true;
 }
 
-template <int NP, bool LCA, bool NOISE>
+template <int NP, int FAM, bool NOISE>
 __device__ __forceinline__ void race_finalize(const RaceParams &p, const RaceLane<NP> &L,
                                               const RaceHead &h, int np) {
     float u;
-    if (NOISE) u = __ldg(p.nunif + L.w);
+    if (NOISE) u = __ldg(p.nunif + ((FAM == FAM_RDM) ? L.w * (np + 1) + np : L.w));
     else u = uniform_co(philox10(make_uint4(0xFFFFFFFFu, L.n, L.k + p.k_base, 1u), p.key).x);
     // compute_smooth_unif receives the time as a C float (_utils.pyx:668-695)
+    constexpr bool LCA = (FAM == FAM_LCA);
     const float tpf = LCA ? __double2float_rn(L.tpd) : L.tp;
     float sm = 0.f;
     if (p.smooth) {
@@ -226,6 +258,13 @@ __device__ __forceinline__ void race_finalize(const RaceParams &p, const RaceLan
     if (LCA) rt = __double2float_rn(__dadd_rn(__dadd_rn(L.tpd, (double)h.t), (double)sm));
     else rt = __fadd_rn(__fadd_rn(L.tp, h.t), sm);
     if (rt >= h.deadline || h.deadline <= 0.f) rt = -999.f;  // enforce_deadline
+    if (FAM == FAM_RDM) {  // no decision or an omission: rt -999, choice -1
+        const bool omit = (rt == -999.f) || (L.win < 0);
+        p.rts[L.w] = omit ? -999.f : rt;
+        p.choices[L.w] = omit ? -1 : L.win;
+        if (p.steps) p.steps[L.w] = L.ix;
+        return;
+    }
     int best = 0;
     float bv = L.x[0];
 #pragma unroll
@@ -255,7 +294,7 @@ __device__ __forceinline__ int64_t race_find(const int64_t *off, int64_t K, int6
     return k;
 }
 
-template <int NP>
+template <int NP, int FAM, bool NOISE>
 __device__ __forceinline__ void race_init(const RaceParams &p, RaceLane<NP> &L, RaceHead &h,
                                           int64_t w, int64_t &hint, int np) {
     int64_t k, n;
@@ -274,18 +313,37 @@ __device__ __forceinline__ void race_init(const RaceParams &p, RaceLane<NP> &L, 
 #pragma unroll
     for (int i = 0; i < 4; ++i) dst[i] = __ldg(src + i);
     const float *z = row + 16 + 2 * np;
-#pragma unroll
-    for (int j = 0; j < NP; ++j) L.x[j] = (j < np) ? __fmul_rn(__ldg(z + j), h.y0scale) : 0.f;
     L.w = w;
     L.k = (uint32_t)k;
     L.n = (uint32_t)n;
+    L.win = -1;
+    if (FAM == FAM_RDM) {
+        // starts U(0, A): z holds A; injected uniforms, or the trajectory's own stream
+#pragma unroll
+        for (int j0 = 0; j0 < NP; j0 += 4) {
+            uint4 r = make_uint4(0u, 0u, 0u, 0u);
+            if (!NOISE && j0 < np) r = philox10(make_uint4(0xFFFFFFFEu, L.n, L.k + p.k_base, 2u + (uint32_t)j0), p.key);
+            const uint32_t wd[4] = {r.x, r.y, r.z, r.w};
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int j = j0 + q;
+                if (j < NP) {
+                    const float u = NOISE ? ((j < np) ? __ldg(p.nunif + L.w * (np + 1) + j) : 0.f) : uniform_co(wd[q]);
+                    L.x[j] = (j < np) ? __fmul_rn(u, __ldg(z + j)) : 0.f;
+                }
+            }
+        }
+    } else {
+#pragma unroll
+        for (int j = 0; j < NP; ++j) L.x[j] = (j < np) ? __fmul_rn(__ldg(z + j), h.y0scale) : 0.f;
+    }
     L.ix = 0;
     L.ixf = 0.f;
     L.tp = 0.f;
     L.tpd = 0.0;
 }
 
-template <int NP, bool LCA, int BOUND, bool NOISE>
+template <int NP, int FAM, int BOUND, bool NOISE>
 __global__ void __launch_bounds__(256) k_race(const __grid_constant__ RaceParams p) {
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
@@ -294,7 +352,7 @@ __global__ void __launch_bounds__(256) k_race(const __grid_constant__ RaceParams
     const int np = (NP == RACE_MAX_NP) ? p.np : NP;
     RaceLane<NP> L;
     RaceHead h;
-    L.w = 0; L.k = L.n = 0; L.ix = 0; L.ixf = L.tp = 0.f; L.tpd = 0.0;
+    L.w = 0; L.k = L.n = 0; L.ix = 0; L.ixf = L.tp = 0.f; L.tpd = 0.0; L.win = -1;
 #pragma unroll
     for (int j = 0; j < NP; ++j) L.x[j] = 0.f;
     uint32_t ctr = 0;
@@ -316,7 +374,7 @@ __global__ void __launch_bounds__(256) k_race(const __grid_constant__ RaceParams
                 const int rank = __popc(need & lt_mask);
                 const int64_t w = (rank < avail) ? q_next + rank : base + (rank - avail);
                 if (w < total) {
-                    race_init<NP>(p, L, h, w, hint, np);
+                    race_init<NP, FAM, NOISE>(p, L, h, w, hint, np);
                     ctr = 0;
                     active = true;
                 }
@@ -342,16 +400,16 @@ __global__ void __launch_bounds__(256) k_race(const __grid_constant__ RaceParams
             bool live = true;
 #pragma unroll 1
             for (int s = 0; s < 4 && live; ++s)
-                live = race_step<NP, LCA, BOUND, NOISE, false>(p, L, h, vr, sr, np, ctr);
+                live = race_step<NP, FAM, BOUND, NOISE, false>(p, L, h, vr, sr, np, ctr);
             if (!live) {
-                race_finalize<NP, LCA, NOISE>(p, L, h, np);
+                race_finalize<NP, FAM, NOISE>(p, L, h, np);
                 active = false;
             }
         }
     }
 }
 
-template <int NP, bool LCA, int BOUND, bool NOISE>
+template <int NP, int FAM, int BOUND, bool NOISE>
 __global__ void k_race_record(const __grid_constant__ RaceParams p) {
     const int np = (NP == RACE_MAX_NP) ? p.np : NP;
     for (int64_t i = threadIdx.x; i < p.traj_len; i += blockDim.x) p.traj[i] = -999.f;
@@ -360,7 +418,7 @@ __global__ void k_race_record(const __grid_constant__ RaceParams p) {
     RaceLane<NP> L;
     RaceHead h;
     int64_t hint = 0;
-    race_init<NP>(p, L, h, 0, hint, np);
+    race_init<NP, FAM, NOISE>(p, L, h, 0, hint, np);
     for (int j = 0; j < np && j < NP && j < p.traj_len; ++j) p.traj[j] = L.x[j];
     const float *row = p.rows + (int64_t)L.k * p.row_floats;
     float vr[NP], sr[NP];
@@ -369,13 +427,13 @@ __global__ void k_race_record(const __grid_constant__ RaceParams p) {
         sr[j] = (j < np) ? row[16 + np + j] : 0.f;
     }
     uint32_t ctr = 0;
-    while (race_step<NP, LCA, BOUND, NOISE, true>(p, L, h, vr, sr, np, ctr)) {
+    while (race_step<NP, FAM, BOUND, NOISE, true>(p, L, h, vr, sr, np, ctr)) {
     }
 }
 
-template <int NP, bool LCA, int BOUND, bool NOISE>
+template <int NP, int FAM, int BOUND, bool NOISE>
 static int race_launch(const RaceParams &p, const ssm_launch *opt, cudaStream_t st) {
-    auto kern = k_race<NP, LCA, BOUND, NOISE>;
+    auto kern = k_race<NP, FAM, BOUND, NOISE>;
     int threads = (opt && opt->block_threads > 0) ? opt->block_threads : 256;
     if (threads > 256 || threads % 32) {
         set_error("block_threads must be a multiple of 32 and at most 256");
@@ -388,44 +446,44 @@ static int race_launch(const RaceParams &p, const ssm_launch *opt, cudaStream_t 
     kern<<<sm_count() * per_sm, threads, 0, st>>>(p);
     SSM_CUDA(cudaGetLastError());
     if (p.traj && p.traj_len > 0) {
-        k_race_record<NP, LCA, BOUND, NOISE><<<1, 128, 0, st>>>(p);
+        k_race_record<NP, FAM, BOUND, NOISE><<<1, 128, 0, st>>>(p);
         SSM_CUDA(cudaGetLastError());
     }
     return SSM_OK;
 }
 
-template <int NP, bool LCA>
+template <int NP, int FAM>
 static int race_dispatch_bound(int bound, bool noise, const RaceParams &p, const ssm_launch *opt,
                                cudaStream_t st) {
     if (noise) {  // exact mode: any boundary shape arrives as a host table or in closed form
         switch (bound) {
-            case SSM_BOUND_TABLE: return race_launch<NP, LCA, SSM_BOUND_TABLE, true>(p, opt, st);
-            case SSM_BOUND_CONSTANT: return race_launch<NP, LCA, SSM_BOUND_CONSTANT, true>(p, opt, st);
-            case SSM_BOUND_LINEAR: return race_launch<NP, LCA, SSM_BOUND_LINEAR, true>(p, opt, st);
+            case SSM_BOUND_TABLE: return race_launch<NP, FAM, SSM_BOUND_TABLE, true>(p, opt, st);
+            case SSM_BOUND_CONSTANT: return race_launch<NP, FAM, SSM_BOUND_CONSTANT, true>(p, opt, st);
+            case SSM_BOUND_LINEAR: return race_launch<NP, FAM, SSM_BOUND_LINEAR, true>(p, opt, st);
             default: break;
         }
         set_error("noise injection supports table, constant and linear boundaries");
         return SSM_ERR_ARG;
     }
     switch (bound) {
-        case SSM_BOUND_TABLE: return race_launch<NP, LCA, SSM_BOUND_TABLE, false>(p, opt, st);
-        case SSM_BOUND_CONSTANT: return race_launch<NP, LCA, SSM_BOUND_CONSTANT, false>(p, opt, st);
-        case SSM_BOUND_LINEAR: return race_launch<NP, LCA, SSM_BOUND_LINEAR, false>(p, opt, st);
-        case SSM_BOUND_WEIBULL: return race_launch<NP, LCA, SSM_BOUND_WEIBULL, false>(p, opt, st);
+        case SSM_BOUND_TABLE: return race_launch<NP, FAM, SSM_BOUND_TABLE, false>(p, opt, st);
+        case SSM_BOUND_CONSTANT: return race_launch<NP, FAM, SSM_BOUND_CONSTANT, false>(p, opt, st);
+        case SSM_BOUND_LINEAR: return race_launch<NP, FAM, SSM_BOUND_LINEAR, false>(p, opt, st);
+        case SSM_BOUND_WEIBULL: return race_launch<NP, FAM, SSM_BOUND_WEIBULL, false>(p, opt, st);
         default: break;
     }
     set_error("unknown boundary kind %d", bound);
     return SSM_ERR_ARG;
 }
 
-template <bool LCA>
+template <int FAM>
 static int race_dispatch(int np, int bound, bool noise, const RaceParams &p, const ssm_launch *opt,
                          cudaStream_t st) {
     switch (np) {
-        case 2: return race_dispatch_bound<2, LCA>(bound, noise, p, opt, st);
-        case 3: return race_dispatch_bound<3, LCA>(bound, noise, p, opt, st);
-        case 4: return race_dispatch_bound<4, LCA>(bound, noise, p, opt, st);
-        default: return race_dispatch_bound<RACE_MAX_NP, LCA>(bound, noise, p, opt, st);
+        case 2: return race_dispatch_bound<2, FAM>(bound, noise, p, opt, st);
+        case 3: return race_dispatch_bound<3, FAM>(bound, noise, p, opt, st);
+        case 4: return race_dispatch_bound<4, FAM>(bound, noise, p, opt, st);
+        default: return race_dispatch_bound<RACE_MAX_NP, FAM>(bound, noise, p, opt, st);
     }
 }
 
@@ -435,7 +493,7 @@ static size_t race_ws_bytes(int64_t n_trials, int np) {
     return (b + 255) & ~(size_t)255;
 }
 
-static int run_race(bool lca, const float *v, const float *z, const float *t, const float *s,
+static int run_race(int fam, const float *v, const float *z, const float *t, const float *s,
                     const float *deadline, const float *g, const float *b, int64_t n_trials,
                     int64_t n_samples, int np, const int64_t *offsets, float max_t, float dt,
                     int bound, const float *a, const float *p1, const float *p2,
@@ -449,7 +507,7 @@ static int run_race(bool lca, const float *v, const float *z, const float *t, co
     SSM_REQUIRE(isfinite(max_t) && (double)max_t / (double)dt <= 8388608.0,
                 "max_t must be finite with max_t / delta_t <= 2^23");
     SSM_REQUIRE(n_trials == 0 || (v && z && t && s && deadline), "v, z, t, s, deadline are required");
-    SSM_REQUIRE(!lca || n_trials == 0 || (g && b), "lca needs g and b");
+    SSM_REQUIRE(fam != FAM_LCA || n_trials == 0 || (g && b), "lca needs g and b");
     SSM_REQUIRE((rts && choices) || (!offsets && n_trials * n_samples == 0), "rts and choices outputs are required");
     SSM_REQUIRE(bound >= SSM_BOUND_TABLE && bound <= SSM_BOUND_WEIBULL, "unknown boundary kind %d", bound);
     SSM_REQUIRE(bound == SSM_BOUND_TABLE || n_trials == 0 || a, "boundary height a is required");
@@ -474,6 +532,7 @@ static int run_race(bool lca, const float *v, const float *z, const float *t, co
     A.g = g; A.b = b; A.table = table; A.n_trials = n_trials; A.tstride = tstride;
     A.row_floats = race_row_floats(np); A.np = np; A.bound = bound; A.dt = dt;
     A.sqrt_dt = (float)sqrt((double)dt); A.max_t = max_t; A.rows = rows;
+    A.per_trial_zs = (fam == FAM_RDM) ? 1 : 0;
     k_race_prep<<<(unsigned)((n_trials + 127) / 128), 128, 0, st>>>(A);
     SSM_CUDA(cudaGetLastError());
     RaceParams p;
@@ -486,8 +545,11 @@ static int run_race(bool lca, const float *v, const float *z, const float *t, co
     p.noise = noise; p.nlen = nlen; p.nunif = nunif;
     p.rts = rts; p.choices = choices; p.steps = steps; p.hdr = hdr;
     p.traj = traj; p.traj_len = traj_len;
-    return lca ? race_dispatch<true>(np, bound, noise != nullptr, p, launch, st)
-               : race_dispatch<false>(np, bound, noise != nullptr, p, launch, st);
+    switch (fam) {
+        case FAM_LCA: return race_dispatch<FAM_LCA>(np, bound, noise != nullptr, p, launch, st);
+        case FAM_RDM: return race_dispatch<FAM_RDM>(np, bound, noise != nullptr, p, launch, st);
+        default: return race_dispatch<FAM_RACE>(np, bound, noise != nullptr, p, launch, st);
+    }
 }
 
 }  // namespace ssm
@@ -507,7 +569,7 @@ int ssm_race_model(const float *v, const float *z, const float *t, const float *
                    const float *noise_unif, float *rts, int32_t *choices, int32_t *steps,
                    float *traj, int64_t traj_len, const ssm_launch *launch, void *workspace,
                    size_t workspace_bytes, void *stream) {
-    return ssm::run_race(false, v, z, t, s, deadline, nullptr, nullptr, n_trials, n_samples,
+    return ssm::run_race(ssm::FAM_RACE, v, z, t, s, deadline, nullptr, nullptr, n_trials, n_samples,
                          n_particles, sample_offsets, max_t, delta_t, bound_kind, a, bound_p1,
                          bound_p2, bound_table, table_stride, table_len, seed, smooth_unif,
                          noise_rows, noise_row_len, noise_unif, rts, choices, steps, traj,
@@ -523,11 +585,26 @@ int ssm_lca(const float *v, const float *z, const float *g, const float *b, cons
             const float *noise_unif, float *rts, int32_t *choices, int32_t *steps, float *traj,
             int64_t traj_len, const ssm_launch *launch, void *workspace, size_t workspace_bytes,
             void *stream) {
-    return ssm::run_race(true, v, z, t, s, deadline, g, b, n_trials, n_samples, n_particles,
+    return ssm::run_race(ssm::FAM_LCA, v, z, t, s, deadline, g, b, n_trials, n_samples, n_particles,
                          sample_offsets, max_t, delta_t, bound_kind, a, bound_p1, bound_p2,
                          bound_table, table_stride, table_len, seed, smooth_unif, noise_rows,
                          noise_row_len, noise_unif, rts, choices, steps, traj, traj_len, launch,
                          workspace, workspace_bytes, stream);
+}
+
+int ssm_racing_diffusion(const float *v, const float *b, const float *A, const float *t, const float *s,
+                         const float *deadline, int64_t n_trials, int64_t n_samples, int n_particles,
+                         const int64_t *sample_offsets, float max_t, float delta_t, uint64_t seed,
+                         int smooth_unif, const float *noise_rows, int64_t noise_row_len,
+                         const float *noise_unif, float *rts, int32_t *choices, int32_t *steps,
+                         float *traj, int64_t traj_len, const ssm_launch *launch, void *workspace,
+                         size_t workspace_bytes, void *stream) {
+    SSM_REQUIRE(n_trials == 0 || (b && A), "b and A are required");
+    return ssm::run_race(ssm::FAM_RDM, v, A, t, s, deadline, nullptr, nullptr, n_trials, n_samples,
+                         n_particles, sample_offsets, max_t, delta_t, SSM_BOUND_CONSTANT, b, nullptr,
+                         nullptr, nullptr, 0, 0, seed, smooth_unif, noise_rows, noise_row_len,
+                         noise_unif, rts, choices, steps, traj, traj_len, launch, workspace,
+                         workspace_bytes, stream);
 }
 
 }  // extern "C"

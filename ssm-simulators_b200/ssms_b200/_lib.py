@@ -82,6 +82,8 @@ _SIGNATURES: dict[str, tuple] = {
     "ssm_lca": (_I, [_P, _P, _P, _P, _P, _P, _P, _I64, _I64, _I, _P, _F, _F, _I, _P, _P, _P, _P,
                      _I64, _I64, _U64, _I, _P, _I64, _P, _P, _P, _P, _P, _I64, _P, _P,
                      C.c_size_t, _P]),
+    "ssm_racing_diffusion": (_I, [_P, _P, _P, _P, _P, _P, _I64, _I64, _I, _P, _F, _F, _U64, _I, _P, _I64, _P, _P,
+                                  _P, _P, _P, _I64, _P, _P, C.c_size_t, _P]),
     "ssm_lba_vanilla": (_I, [_P, _P, _P, _P, _P, _P, _I64, _I64, _I, _P, _U64, _P, _P, _P, _P, _P]),
     "ssm_kde_fit": (_I, [_P, _P, _I64, _P, _P, _I, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
     "ssm_kde_eval_workspace_bytes": (C.c_size_t, [_I64, _I, _I64]),

@@ -38,7 +38,7 @@ _SIMULATORS = {
     "ddm_flexbound": cssm.ddm_flexbound, "ddm": cssm.ddm, "race_model": cssm.race_model,
     "lca": cssm.lca, "levy_flexbound": cssm.levy_flexbound, "lba_vanilla": cssm.lba_vanilla,
     "full_ddm": cssm.full_ddm, "ddm_sdv": cssm.ddm_sdv, "ornstein_uhlenbeck": cssm.ornstein_uhlenbeck,
-    "ddm_flex": cssm.ddm_flex,
+    "ddm_flex": cssm.ddm_flex, "racing_diffusion_model": cssm.racing_diffusion_model,
 }
 
 
@@ -66,6 +66,9 @@ def _family_transforms(name: str, entry: dict) -> tuple[list, list]:
             DeleteParameters(["A", "b"]),
             SetValue("t", lambda k: np.zeros(k, dtype=np.float32)),
         ]
+    m = re.match(r"^racing_diffusion_(\d)$", name)
+    if m:
+        return [], [ColumnStackParameters(vs, "v", delete_sources=False), ExpandDimension(["t", "A", "b"])]
     if name == "lba_3_vs_constraint":
         return [], [ColumnStackParameters(vs, "v"), ExpandDimension(["a", "z"]),
                     SetValue("t", lambda k: np.zeros(k, dtype=np.float32))]

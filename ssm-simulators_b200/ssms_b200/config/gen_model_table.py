@@ -22,7 +22,7 @@ from pathlib import Path
 HERE = Path(__file__).resolve().parent
 REPO = HERE.parents[2]
 SIMULATORS = {"ddm_flexbound", "ddm", "race_model", "lca", "levy_flexbound", "lba_vanilla", "full_ddm",
-              "ddm_sdv", "ornstein_uhlenbeck", "ddm_flex"}
+              "ddm_sdv", "ornstein_uhlenbeck", "ddm_flex", "racing_diffusion_model"}
 
 
 def _import_reference(root: Path):

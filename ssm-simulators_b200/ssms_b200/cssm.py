@@ -291,6 +291,41 @@ def lca(v, z, g, b, t, s, deadline, delta_t=0.001, max_t=20, n_samples=2000, n_t
                      kwargs)
 
 
+def racing_diffusion_model(v, b, A, t, s, deadline, delta_t=0.001, max_t=20, n_samples=2000, n_trials=1,
+                           random_state=None, return_option="full", smooth_unif=False, n_threads=1, **kwargs):
+    """Racing diffusion model: first-past-the-post race of Wiener accumulators
+    from U(0, A) starts to one threshold b (src/cssm/race_models.pyx:925-1300).
+    The reference draws the start points from C rand(); here they come from the
+    trajectory's Philox stream like every other draw."""
+    _check_return_option(return_option)
+    n_trials, n_samples = int(n_trials), int(n_samples)
+    v = np.ascontiguousarray(_f32(v, "v"))
+    b, A, t, s = (_f32(x, nm) for x, nm in ((b, "b"), (A, "A"), (t, "t"), (s, "s")))
+    deadline = _f32(deadline, "deadline")
+    n_part = v.shape[1]
+    col = lambda x: np.ascontiguousarray(x.reshape(n_trials, -1)[:, 0]) if n_trials else x.reshape(-1)  # noqa: E731
+    full = return_option == "full"
+    n_rows = int(np.float32(np.float32(max_t) / np.float32(delta_t))) + 1
+    out = dev.simulate_rdm(v=v, b=col(b), A=col(A), t=col(t), s=col(s), deadline=deadline, n_trials=n_trials,
+                           n_samples=n_samples, max_t=max_t, delta_t=delta_t, seed=_seed(random_state),
+                           smooth_unif=smooth_unif,
+                           traj_len=n_rows * n_part if (full and n_trials and n_samples) else 0)
+    rts = out.rts.cpu().numpy().reshape(n_samples, n_trials, 1)
+    choices = out.choices.cpu().numpy().reshape(n_samples, n_trials, 1)
+    minimal = _minimal_meta("rdm_simulator", list(np.arange(0, n_part, 1)), n_samples, n_trials)
+    if not full:
+        return {"rts": rts, "choices": choices, "metadata": minimal}
+    meta = dict(minimal)
+    meta.update({"v": v, "b": b, "A": A, "t": t, "deadline": deadline, "s": s})
+    meta.update({"delta_t": float(np.float32(delta_t)), "max_t": float(np.float32(max_t)), "n_threads": 1})
+    traj = np.full((n_rows, n_part), -999, dtype=DTYPE)
+    if out.traj is not None:
+        traj.reshape(-1)[:] = out.traj.cpu().numpy()[: n_rows * n_part]
+    meta["trajectory"] = traj
+    meta.update(_param_dict(v, "v", n_part))
+    return {"rts": rts, "choices": choices, "metadata": meta}
+
+
 def lba_vanilla(v, a, z, deadline, sd, t, nact=3, n_samples=2000, n_trials=1, max_t=20,
                 **kwargs):
     """Linear ballistic accumulator, closed form (src/cssm/lba_models.pyx:36-139).

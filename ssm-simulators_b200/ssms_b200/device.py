@@ -265,6 +265,51 @@ def simulate_race(model: str, *, v, z, t, s, deadline, n_trials: int, n_samples:
     return SimOutput(rts=rts, choices=chs, steps=steps, traj=traj, workspace=ws)
 
 
+def simulate_rdm(*, v, b, A, t, s, deadline, n_trials: int, n_samples: int = 0, sample_offsets=None,
+                 max_t: float = 20.0, delta_t: float = 0.001, seed: int = 0, smooth_unif: bool = False,
+                 noise_rows=None, noise_unif=None, want_steps: bool = False, traj_len: int = 0, total=None,
+                 launch=None, stream: torch.cuda.Stream | None = None, ws_tag: int = 0) -> SimOutput:
+    """racing_diffusion_model on the GPU.  v: [n_trials, n_particles]; b, A, t, s,
+    deadline: one value per trial."""
+    dev = D.require_cuda()
+    K = int(n_trials)
+    n_part = int(v.shape[-1]) if isinstance(v, torch.Tensor) else int(np.shape(v)[-1])
+    vt = D.to_dev_f32(v, K * n_part, "v")
+    bt, At, tt, st_, dlt = (D.to_dev_f32(x, K, nm) for x, nm in
+                            ((b, "b"), (A, "A"), (t, "t"), (s, "s"), (deadline, "deadline")))
+    offs = _offsets(sample_offsets, K, dev)
+    if total is None:
+        total = int(offs[-1].item()) if offs is not None else K * int(n_samples)
+    rts = torch.empty(total, dtype=torch.float32, device=dev)
+    chs = torch.empty(total, dtype=torch.int32, device=dev)
+    steps = torch.empty(total, dtype=torch.int32, device=dev) if want_steps else None
+    traj = torch.empty(int(traj_len), dtype=torch.float32, device=dev) if traj_len > 0 else None
+    nrows = nunif = None
+    nlen = 0
+    if noise_rows is not None:
+        nrows = D.to_dev_f32(noise_rows)
+        nlen = int(noise_rows.shape[-1])
+        nunif = D.to_dev_f32(noise_unif, total * (n_part + 1), "noise_unif")
+        if nrows.numel() < total * nlen:
+            raise ValueError("noise_rows must hold one row per trajectory")
+    L = _lib.lib()
+    ws = D.workspace(L.ssm_race_workspace_bytes(K, n_part), tag=ws_tag, stream=stream)
+    if K == 0 or total == 0:
+        if traj is not None:
+            traj.fill_(-999.0)
+        return SimOutput(rts=rts, choices=chs, steps=steps, traj=traj, workspace=ws)
+    lopt = launch if launch is not None else launch_for("racing_diffusion_model")
+    sp = D.stream_ptr(stream)
+    _lib.check(L.ssm_racing_diffusion(
+        D.ptr(vt), D.ptr(bt), D.ptr(At), D.ptr(tt), D.ptr(st_), D.ptr(dlt), K, int(n_samples), n_part, D.ptr(offs),
+        float(np.float32(max_t)), float(np.float32(delta_t)), _lib.U64_cast(seed), int(bool(smooth_unif)),
+        D.ptr(nrows), nlen, D.ptr(nunif), D.ptr(rts), D.ptr(chs), D.ptr(steps), D.ptr(traj), int(traj_len),
+        ctypes.addressof(lopt), D.ptr(ws), ws.numel(), sp))
+    if noise_rows is not None:
+        _lib.check(L.ssm_check_status(D.ptr(ws), sp))
+    return SimOutput(rts=rts, choices=chs, steps=steps, traj=traj, workspace=ws)
+
+
 def simulate_lba(*, v, a, z, deadline, sd, t, n_trials: int, n_samples: int = 0,
                  sample_offsets=None, seed: int = 0, noise_u=None, noise_g=None, total=None,
                  stream: torch.cuda.Stream | None = None) -> SimOutput:

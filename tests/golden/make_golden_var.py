@@ -6,6 +6,7 @@ small fixed-seed cases, stored as .npz fixtures in this directory.
 Usage:  python oracle/build_ref.py && python tests/golden/make_golden_var.py
         python tests/golden/make_golden_var.py --flex [REFERENCE_ROOT]   (ddm_flex cases; the
         reference's drift functions are loaded from its source tree)
+        python tests/golden/make_golden_var.py --rdm    (racing_diffusion_model cases)
 """
 
 from __future__ import annotations
@@ -72,7 +73,7 @@ def main():
     _case("ornstein_angle", "ornstein_uhlenbeck", bf.angle, ["a", "theta"], th, 500, 35, False)
 
 
-if __name__ == "__main__" and "--flex" not in sys.argv:
+if __name__ == "__main__" and "--flex" not in sys.argv and "--rdm" not in sys.argv:
     main()
 
 
@@ -132,3 +133,23 @@ def main_flex():
 if __name__ == "__main__" and "--flex" in sys.argv:
     sys.argv.remove("--flex")
     main_flex()
+
+
+def main_rdm():
+    from cssm.race_models import racing_diffusion_model
+
+    f2 = lambda x: f32(x).reshape(-1, 1)  # noqa: E731
+    cases = [("rdm3", f32([[1.0, 0.8, 0.5], [0.3, 1.5, 0.9]]), f2([1.5, 1.2]), f2([0.5, 0.3]), f2([0.3, 0.5]),
+              f32([999.0, 1.6]), 500, 51, True),
+             ("rdm4", f32([[0.5, 0.6, 0.7, 0.8]]), f2([2.0]), f2([0.8]), f2([0.2]), f32([999.0]), 500, 52, False)]
+    for name, v, b, A, t, dl, n, seed, smooth in cases:
+        K = v.shape[0]
+        s = f2([1.0] * K)
+        out = racing_diffusion_model(v, b, A, t, s, dl, delta_t=0.001, max_t=20.0, n_samples=n, n_trials=K,
+                                     random_state=seed, smooth_unif=smooth)
+        _save(name, v=v, b=b, A=A, t=t, s=s, deadline=dl, n=n, seed=seed, smooth=smooth, rts=out["rts"],
+              choices=out["choices"].astype(np.int8), trajectory=out["metadata"]["trajectory"])
+
+
+if __name__ == "__main__" and "--rdm" in sys.argv:
+    main_rdm()

@@ -168,3 +168,56 @@ def test_cssm_race_lca_lba_contract(cuda):
     assert lb["rts"].shape == (N, K, 1)
     assert {"v_0", "v_1", "v_2", "a", "z", "sd", "t", "deadline", "max_t"} <= set(lb["metadata"])
     assert set(np.unique(lb["choices"])) <= {0, 1, 2}
+
+
+# ------------------------------------------------------------------ racing diffusion model
+@pytest.mark.parametrize("npart,smooth", [(2, True), (3, False), (4, True), (6, True)])
+def test_racing_diffusion_noise_injection_bit_exact(cuda, oracle, npart, smooth):
+    rng = np.random.default_rng(300 + npart)
+    K, N, max_t = 5, 300, 3.0
+    v = f32(rng.uniform(0, 2.5, (K, npart)))
+    b, A = f32(rng.uniform(0.5, 2.0, K)), f32(rng.uniform(0.0, 0.5, K))
+    t, s = f32(rng.uniform(0, 1, K)), f32(rng.uniform(0.7, 1.3, K))
+    dl = f32(rng.uniform(1.0, 4.0, K))
+    dl[0] = 999.0
+    total = K * N
+    rows = rng.standard_normal((total, (int(max_t / 0.001) + 20) * npart), dtype=np.float32)
+    unif = f32(rng.uniform(0, 1, total * (npart + 1)))
+    out = dev.simulate_rdm(v=v, b=b, A=A, t=t, s=s, deadline=dl, n_trials=K, n_samples=N, max_t=max_t, delta_t=0.001,
+                           smooth_unif=smooth, noise_rows=rows, noise_unif=unif, want_steps=True)
+    o_rt, o_ch, o_st, _ = oracle.rdm(v, b, A, t, s, dl, max_t=max_t, delta_t=0.001, n_samples=N, n_trials=K,
+                                     smooth_unif=smooth, rows=rows, unif=unif)
+    np.testing.assert_array_equal(out.steps.cpu().numpy(), o_st)
+    np.testing.assert_array_equal(out.choices.cpu().numpy(), o_ch)
+    np.testing.assert_array_equal(_bits(out.rts.cpu().numpy()), _bits(o_rt))
+
+
+@pytest.mark.parametrize("case", [0, 1])
+def test_racing_diffusion_device_rng_matches_reference(cuda, oracle, case):
+    v = [f32([[1.0, 0.8, 0.5]]), f32([[0.4, 0.5, 0.6, 1.2]])][case]
+    b, A, t = f32([[1.5], [2.0]][case]), f32([[0.5], [0.3]][case]), f32([[0.3], [0.2]][case])
+    N = 100_000
+    out = cssm.racing_diffusion_model(v, b.reshape(1, 1), A.reshape(1, 1), t.reshape(1, 1), f32([[1.0]]), f32([999]),
+                                      n_samples=N, n_trials=1, random_state=21 + case, smooth_unif=True,
+                                      return_option="minimal")
+    r = oracle.rdm(v, b, A, t, f32([1.0]), f32([999]), max_t=20.0, delta_t=0.001, n_samples=N, n_trials=1,
+                   smooth_unif=True, random_state=77 + case)
+    choices = list(range(v.shape[1]))
+    g_rt, g_ch = out["rts"].reshape(-1), out["choices"].reshape(-1)
+    for c in choices:
+        p1, p2 = np.mean(g_ch == c), np.mean(r[1] == c)
+        se = np.sqrt(max(0.5 * (p1 + p2) * (1 - 0.5 * (p1 + p2)), 1e-12) * 2 / N)
+        assert abs(p1 - p2) <= 3 * se + 1e-12, (c, p1, p2)
+        a_, b_ = g_rt[g_ch == c], r[0][r[1] == c]
+        if len(a_) > 50 and len(b_) > 50:
+            assert stats.ks_2samp(a_, b_).pvalue > 0.0025, c
+
+
+def test_racing_diffusion_through_simulator(cuda):
+    from ssms_b200 import Simulator, model_config
+
+    cfg = model_config["racing_diffusion_3"]
+    theta = dict(zip(cfg["params"], cfg["default_params"]))
+    out = Simulator("racing_diffusion_3").simulate(theta, n_samples=5000, random_state=4)
+    assert out["rts"].shape == (5000, 1) and set(np.unique(out["choices"])) <= {-1, 0, 1, 2}
+    assert out["metadata"]["simulator"] == "rdm_simulator" and out["metadata"]["trajectory"].shape == (20001, 3)

@@ -34,7 +34,7 @@ def _recording_config(name):
 
 def test_all_reference_models_with_built_simulators_are_configured():
     assert set(MODELS) == set(model_config)
-    assert len(MODELS) == 54
+    assert len(MODELS) == 55
 
 
 @pytest.mark.parametrize("name", MODELS)

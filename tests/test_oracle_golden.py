@@ -156,3 +156,15 @@ def test_ddm_flex_matches_reference(oracle, name):
     np.testing.assert_array_equal(_bits(rts), _bits(g["rts"].reshape(-1)))
     np.testing.assert_array_equal(chs, g["choices"].reshape(-1).astype(np.int32))
     np.testing.assert_array_equal(_bits(traj), _bits(g["trajectory"][:, 0]))
+
+
+@pytest.mark.parametrize("name", ["rdm3", "rdm4"])
+def test_racing_diffusion_matches_reference(oracle, name):
+    g = _load(name)
+    K = g["v"].shape[0]
+    rts, chs, _, traj = oracle.rdm(g["v"], g["b"], g["A"], g["t"], g["s"], g["deadline"], max_t=20.0, delta_t=0.001,
+                                   n_samples=int(g["n"]), n_trials=K, smooth_unif=bool(g["smooth"]),
+                                   random_state=int(g["seed"]), traj_len=g["trajectory"].size)
+    np.testing.assert_array_equal(_bits(rts), _bits(g["rts"].reshape(-1)))
+    np.testing.assert_array_equal(chs, g["choices"].reshape(-1).astype(np.int32))
+    np.testing.assert_array_equal(_bits(traj), _bits(g["trajectory"].reshape(-1)))
