@@ -361,6 +361,24 @@ int ssm_set_summary(const float *rts, const int32_t *choices, int64_t n_sets,
                     float *hist_b, void *stream);
 
 /*
+ * ssm_simulator_summary -- the derived outputs of simulator()
+ * (ssms/basic_simulators/simulator.py:806-863) and its pooled rt histograms
+ * (bin_simulator_output, simulator.py:435-497) for an output in the reference
+ * layout (index n * n_trials + k): per trial, choice counts [n_trials,
+ * n_choices], choice counts among non-omitted samples, omission counts (rt ==
+ * -999) and no-go counts (choice != the largest choice value, or omitted);
+ * pooled over all trials, per-choice histograms [nbins, n_choices] of the
+ * non-omitted rts with numpy.histogram's rule on the float64 bin edges
+ * (nbins + 1 of them; the last may be +inf).  Counters are int64 and cleared
+ * by the call.
+ */
+int ssm_simulator_summary(const float *rts, const int32_t *choices, int64_t n_samples, int64_t n_trials,
+                          const int32_t *choice_values, int n_choices, const double *edges_a, int nbins_a,
+                          const double *edges_b, int nbins_b, int64_t *choice_counts, int64_t *kept_counts,
+                          int64_t *omission_counts, int64_t *nogo_counts, int64_t *hist_a, int64_t *hist_b,
+                          void *stream);
+
+/*
  * ssm_ddm_flexbound_static -- no counterpart in the reference.  The same
  * simulation as ssm_ddm_flexbound for callers that cannot allocate device
  * memory (for example code running inside an allocator-free host plugin, or a

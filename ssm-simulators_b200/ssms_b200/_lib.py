@@ -91,6 +91,7 @@ _SIGNATURES: dict[str, tuple] = {
                           C.c_double, _P, C.c_size_t, _P, _P]),
     "ssm_kde_sample": (_I, [_P, _P, _P, _I64, _I, _P, _P, _P, _U64, C.c_double, C.c_double,
                             C.c_double, _P, _P]),
+    "ssm_simulator_summary": (_I, [_P, _P, _I64, _I64, _P, _I, _P, _I, _P, _I, _P, _P, _P, _P, _P, _P, _P]),
     "ssm_set_summary": (_I, [_P, _P, _I64, _P, _P, _I, C.c_double, _P, _P, _P, _I, _P, _I, _P, _P]),
     "ssm_kde_records": (_I, [_P, _I, _I64, _I, _P, _P, _P, _P, _I64, _I64, _F, _U64, _P, _P]),
     "ssm_ddm_nf_loglik": (_I, [_P, _P, _P, _P, _P, _P, _P, _I64, _I, C.c_double, _P, _P, _P]),

@@ -357,25 +357,53 @@ def simulator(theta, model: str = "angle", n_samples: int = 1000, delta_t: float
     x = sim.simulate(theta, n_samples=n_samples, delta_t=delta_t, max_t=max_t, no_noise=no_noise,
                      sigma_noise=sigma_noise, smooth_unif=smooth_unif, random_state=random_state,
                      return_option=return_option, n_threads=n_threads, extra_fields=extra_fields)
-    rts = x["rts"].reshape(n_samples, n_trials, 1)
-    chs = x["choices"].reshape(n_samples, n_trials, 1)
-    pc = x["metadata"]["possible_choices"]
-    x["choice_p"] = np.zeros((n_trials, len(pc)))
-    x["choice_p_no_omission"] = np.zeros((n_trials, len(pc)))
-    x["omission_p"] = np.zeros((n_trials, 1))
-    x["nogo_p"] = np.zeros((n_trials, 1))
-    x["go_p"] = np.zeros((n_trials, 1))
-    for k in range(n_trials):
-        r, c = rts[:, k, :], chs[:, k, :]
-        kept = r != OMISSION_SENTINEL
-        n_keep = int(kept.sum())
-        for i, ch in enumerate(pc):
-            x["choice_p"][k, i] = (c == ch).sum() / r.shape[0]
-            x["choice_p_no_omission"][k, i] = ((c[kept] == ch).sum() / n_keep) if n_keep > 0 else OMISSION_SENTINEL
-        x["omission_p"][k, 0] = (r == OMISSION_SENTINEL).sum() / r.shape[0]
-        x["nogo_p"][k, 0] = ((c != max(pc)) | (r == OMISSION_SENTINEL)).sum() / r.shape[0]
-        x["go_p"][k, 0] = 1 - x["nogo_p"][k, 0]
+    pc = list(x["metadata"]["possible_choices"])
+    counts = summarize_output(x["rts"], x["choices"], n_samples, n_trials, pc, x["metadata"]["max_t"])
+    x["choice_p"] = counts["choice"] / n_samples
+    kept = (n_samples - counts["omission"]).reshape(n_trials, 1)  # samples with rt != -999
+    with np.errstate(invalid="ignore", divide="ignore"):
+        x["choice_p_no_omission"] = np.where(kept > 0, counts["kept"] / np.maximum(kept, 1), OMISSION_SENTINEL)
+    x["omission_p"] = (counts["omission"] / n_samples).reshape(n_trials, 1)
+    x["nogo_p"] = (counts["nogo"] / n_samples).reshape(n_trials, 1)
+    x["go_p"] = 1 - x["nogo_p"]
     x["metadata"]["model"] = model
-    x["binned_128"] = np.expand_dims(bin_simulator_output(x, nbins=128, max_t=-1, freq_cnt=True), axis=0)
-    x["binned_256"] = np.expand_dims(bin_simulator_output(x, nbins=256, max_t=-1, freq_cnt=True), axis=0)
+    x["binned_128"] = np.expand_dims(counts["binned_128"], axis=0)
+    x["binned_256"] = np.expand_dims(counts["binned_256"], axis=0)
     return x
+
+
+def _hist_edges(nbins: int, max_t: float) -> np.ndarray:
+    """bin_simulator_output's edges: linspace(0, max_t, nbins) and +inf."""
+    edges = np.zeros(nbins + 1)
+    edges[:nbins] = np.linspace(0, max_t, nbins)
+    edges[nbins] = np.inf
+    return edges
+
+
+def summarize_output(rts, choices, n_samples: int, n_trials: int, possible_choices, max_t: float) -> dict:
+    """simulator()'s derived counts in one GPU pass (libssm_b200's
+    ssm_simulator_summary) over rts/choices in the reference layout: per trial
+    choice counts [K, C], choice counts without omissions, omission and no-go
+    counts; pooled 128- and 256-bin rt histograms [nbins, C] (float64 counts,
+    bin_simulator_output with freq_cnt=True)."""
+    import torch
+
+    from . import _device as Dv
+    from . import _lib
+
+    dev = Dv.require_cuda()
+    C = len(possible_choices)
+    r = torch.from_numpy(np.ascontiguousarray(np.asarray(rts, np.float32).reshape(-1))).to(dev)
+    c = torch.from_numpy(np.ascontiguousarray(np.asarray(choices).astype(np.int32).reshape(-1))).to(dev)
+    cv = torch.from_numpy(np.asarray(possible_choices, np.int32)).to(dev)
+    ea = torch.from_numpy(_hist_edges(128, float(max_t))).to(dev)
+    eb = torch.from_numpy(_hist_edges(256, float(max_t))).to(dev)
+    i64 = lambda *shape: torch.empty(*shape, dtype=torch.int64, device=dev)  # noqa: E731
+    cc, kc, om, ng, ha, hb = i64(n_trials * C), i64(n_trials * C), i64(n_trials), i64(n_trials), i64(128 * C), i64(256 * C)
+    _lib.check(_lib.lib().ssm_simulator_summary(
+        Dv.ptr(r), Dv.ptr(c), int(n_samples), int(n_trials), Dv.ptr(cv), C, Dv.ptr(ea), 128, Dv.ptr(eb), 256,
+        Dv.ptr(cc), Dv.ptr(kc), Dv.ptr(om), Dv.ptr(ng), Dv.ptr(ha), Dv.ptr(hb), Dv.stream_ptr()))
+    h = lambda t, *shape: t.cpu().numpy().reshape(*shape)  # noqa: E731
+    return {"choice": h(cc, n_trials, C).astype(np.float64), "kept": h(kc, n_trials, C).astype(np.float64),
+            "omission": h(om, n_trials).astype(np.float64), "nogo": h(ng, n_trials).astype(np.float64),
+            "binned_128": h(ha, 128, C).astype(np.float64), "binned_256": h(hb, 256, C).astype(np.float64)}

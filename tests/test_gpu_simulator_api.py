@@ -70,3 +70,34 @@ def test_deadline_model_marks_omissions(cuda):
                                              n_samples=5000, random_state=8)
     rts = out["rts"][:, 0]
     assert np.any(rts == -999) and np.all(rts[rts != -999] < 0.8)
+
+
+def test_simulator_summary_matches_host_definition(cuda):
+    """The device summary behind simulator() equals the reference's host loops
+    (simulator.py:806-863) and bin_simulator_output (:435-497) on outputs with
+    omissions, out-of-set choices and rts past max_t."""
+    from ssms_b200.simulator import bin_simulator_output, summarize_output
+
+    rng = np.random.default_rng(9)
+    N, K, max_t = 3000, 7, 5.0
+    rts = rng.uniform(0, 7, (N, K, 1)).astype(np.float32)
+    chs = rng.choice([-1, 1], (N, K, 1)).astype(np.int32)
+    rts[rng.random((N, K, 1)) < 0.1] = -999.0
+    rts[:, 3, :] = -999.0  # a trial with omissions only
+    chs[rng.random((N, K, 1)) < 0.02] = 5  # a value outside the possible choices
+    pc = [-1, 1]
+    got = summarize_output(rts, chs, N, K, pc, max_t)
+    for k in range(K):
+        r, c = rts[:, k, :], chs[:, k, :]
+        kept = r != -999
+        for i, ch in enumerate(pc):
+            assert got["choice"][k, i] == (c == ch).sum()
+            assert got["kept"][k, i] == (c[kept] == ch).sum()
+        assert got["omission"][k] == (r == -999).sum()
+        assert got["nogo"][k] == ((c != max(pc)) | (r == -999)).sum()
+    out = {"rts": rts, "choices": chs, "metadata": {"max_t": max_t, "possible_choices": pc, "n_samples": N}}
+    np.testing.assert_array_equal(got["binned_128"], bin_simulator_output(out, nbins=128, max_t=-1, freq_cnt=True))
+    np.testing.assert_array_equal(got["binned_256"], bin_simulator_output(out, nbins=256, max_t=-1, freq_cnt=True))
+    x = simulator({"v": [0.5, -0.5], "a": 1.5, "z": 0.5, "t": 0.3, "theta": 0.2}, model="angle", n_samples=500,
+                  random_state=4)
+    assert np.all(x["choice_p_no_omission"] >= 0)

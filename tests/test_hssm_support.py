@@ -56,10 +56,10 @@ def test_seed_range_and_simulator_validation():
 def test_rng_fn_draws_posterior_predictive_samples(cuda):
     fun = H.get_simulator_fun_internal("ddm")
     rng = np.random.default_rng(1)
-    # 4 posterior draws x 5 data trials, 3 replicas each
+    # 4 posterior draws x 5 data trials; size counts data trials x replicas -> 3 replicas
     v = rng.uniform(-1, 1, (4, 5)).astype(np.float32)
     args = [v, np.array(1.5, np.float32), np.array(0.5, np.float32), np.array(0.3, np.float32)]
-    out = H.rng_fn(args, 60, rng, fun, 2)
+    out = H.rng_fn(args, 15, rng, fun, 2)
     assert out.shape == (4, 5, 3, 2)
     rts, chs = out[..., 0], out[..., 1]
     assert np.all((rts > 0.3) | (rts == -999)) and set(np.unique(chs)) <= {-1.0, 1.0}
