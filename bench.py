@@ -460,9 +460,10 @@ MIX_BOUNDS = {
     "race_no_bias_angle_4": {**_V4, "a": (1.0, 3.0), "z": (0.0, 0.5), "t": (0.0, 2.0), "theta": (0.0, 1.45)},
     "levy": {"v": (-3.0, 3.0), "a": (0.3, 3.0), "z": (0.1, 0.9), "alpha": (1.0, 2.0), "t": (0.001, 2.0)},
 }
-MIX_CPU_ROWS_PER_CORE = {"lca_no_bias_4": 1, "race_no_bias_angle_4": 6, "levy": 6, "full_ddm": 6, "ornstein": 6}
+MIX_CPU_ROWS_PER_CORE = {"lca_no_bias_4": 1, "race_no_bias_angle_4": 6, "levy": 6, "full_ddm": 6, "ornstein": 6,
+                         "conflict_ds": 6, "racing_diffusion_3": 4}
 # further simulator families, 1024 parameter vectors from their configured bounds, 10000 samples
-WIDER = ("full_ddm", "ornstein")
+WIDER = ("full_ddm", "ornstein", "conflict_ds", "racing_diffusion_3")
 PLAIN_DDM = {"v": 1.0, "a": 1.5, "z": 0.5, "t": 0.2}
 PLAIN_SAMPLES = 100_000
 
@@ -478,7 +479,8 @@ def _constant_host(t, a):
 
 _HOST_BOUNDS = {"constant": _constant_host, "angle": _angle_host}
 _REF_MODULE = {"ddm_flexbound": "ddm_models", "levy_flexbound": "levy_models", "race_model": "race_models",
-               "lca": "race_models", "full_ddm": "ddm_models", "ornstein_uhlenbeck": "ornstein_models"}
+               "lca": "race_models", "full_ddm": "ddm_models", "ornstein_uhlenbeck": "ornstein_models",
+               "ddm_flex": "ddm_models", "racing_diffusion_model": "race_models"}
 
 
 def _cpu_sim_worker(job):
@@ -486,12 +488,22 @@ def _cpu_sim_worker(job):
     sim_name, calls = job
     sys.path.insert(0, str(Path(__file__).resolve().parent / "oracle" / "_ref"))
     import importlib
+    import importlib.util
 
     fn = getattr(importlib.import_module("cssm." + _REF_MODULE[sim_name]), sim_name)
     done = 0
-    for kw, bname, bparams, n, seed in calls:
+    for kw, bname, bparams, n, seed, drift in calls:
+        extra = {}
+        if drift is not None:  # ddm_flex: the drift function by name, from this package's host module
+            spec = importlib.util.spec_from_file_location(
+                "bench_drifts", Path(__file__).resolve().parent / "ssm-simulators_b200" / "ssms_b200" /
+                "drift_functions.py")
+            mod = importlib.util.module_from_spec(spec)
+            spec.loader.exec_module(mod)
+            extra = {"drift_fun": mod.DRIFTS[drift[0]][0], "drift_params": drift[1]}
         fn(**kw, boundary_fun=_HOST_BOUNDS[bname], boundary_params=bparams, max_t=20.0, delta_t=0.001,
-           n_samples=int(n), n_trials=1, random_state=int(seed), return_option="minimal", smooth_unif=True)
+           n_samples=int(n), n_trials=1, random_state=int(seed), return_option="minimal", smooth_unif=True,
+           **extra)
         done += int(n)
     return done
 
@@ -503,7 +515,11 @@ def _row_calls(prep: dict, rows: int, n: int, seed0: int) -> list:
               if np.ndim(v) >= 1}
         bp = {key: np.ascontiguousarray(np.asarray(v)[k:k + 1])
               for key, v in prep["boundary"]["boundary_params"].items()}
-        calls.append((kw, prep["boundary"]["boundary_fun"].__name__, bp, n, seed0 + k))
+        drift = None
+        if prep.get("drift"):
+            drift = (prep["config"]["drift_name"],
+                     {key: np.ascontiguousarray(np.asarray(v)[k:k + 1]) for key, v in prep["drift"]["drift_params"].items()})
+        calls.append((kw, prep["boundary"]["boundary_fun"].__name__, bp, n, seed0 + k, drift))
     return calls
 
 
@@ -535,7 +551,7 @@ def run_other_workloads(args) -> dict:
         sim = Simulator(model)
         prep = sim.prepare(theta, n_samples=n, random_state=SEED + i)
         name = prep["config"]["simulator"].__name__
-        sb = SetBatch(name, prep["theta"], prep["boundary"], n, max_t=20.0, delta_t=0.001)
+        sb = SetBatch(name, prep["theta"], prep["boundary"], n, max_t=20.0, delta_t=0.001, drift=prep["drift"])
         o = sb.run(SEED, want_steps=True)
         steps = int(o.steps.to(torch.int64).sum().item())
         for w in range(args.warmup):
@@ -579,14 +595,14 @@ def run_other_workloads(args) -> dict:
     try:
         for label, name, prep, n in cpu_jobs:
             if label == "plain_ddm":  # one parameter set: the samples are split over the cores
-                (kw, bn, bp, _, _), = _row_calls(prep, 1, n, 0)
+                (kw, bn, bp, _, _, dr), = _row_calls(prep, 1, n, 0)
                 per = [n // cores + (1 if c < n % cores else 0) for c in range(cores)]
-                jobs = [(name, [(kw, bn, bp, m, SEED + 300 + c)]) for c, m in enumerate(per)]
+                jobs = [(name, [(kw, bn, bp, m, SEED + 300 + c, dr)]) for c, m in enumerate(per)]
             else:
                 calls = _row_calls(prep, MIX_CPU_ROWS_PER_CORE[label] * cores, n, SEED + 300)
                 jobs = [(name, [c]) for c in calls]
-            kw, bn, bp, _, _ = jobs[0][1][0]
-            pool.map(_cpu_sim_worker, [(name, [(kw, bn, bp, 10, 1)])] * cores)  # warm the workers
+            kw, bn, bp, _, _, dr = jobs[0][1][0]
+            pool.map(_cpu_sim_worker, [(name, [(kw, bn, bp, 10, 1, dr)])] * cores)  # warm the workers
             t0 = time.perf_counter()
             done = sum(pool.imap_unordered(_cpu_sim_worker, jobs, chunksize=1))
             sec = time.perf_counter() - t0

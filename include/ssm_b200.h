@@ -53,6 +53,7 @@ typedef struct ssm_launch {
     int block_threads;     /* 0 = library default (autotuned value if set) */
     int blocks_per_sm;     /* 0 = as many as fit                            */
     int chunk;             /* trajectories a warp claims per queue access; 0 = default */
+    int refill_min;        /* ended walks a warp collects before restarting lanes (1-32); 0 = default */
     /* Index that trial 0 of this call has in the random streams (0 = none).
      * A batch simulated as several calls over consecutive trial windows --
      * each with its per-trial pointers advanced to the window, first_trial =

@@ -47,6 +47,7 @@ struct RaceParams {
     int np;
     float dt;
     int smooth, chunk;
+    int refill_min;           // ended walks a warp collects before it restarts lanes
     const float *table;
     int64_t tstride, tlen;
     const float *noise;
@@ -356,11 +357,19 @@ __global__ void __launch_bounds__(256) k_race(const __grid_constant__ RaceParams
 #pragma unroll
     for (int j = 0; j < NP; ++j) L.x[j] = 0.f;
     uint32_t ctr = 0;
-    bool active = false, exhausted = false;
+    bool active = false, pending = false, exhausted = false;
     int64_t q_next = 0, q_end = 0, hint = 0;
     for (;;) {
+        // ended walks are written and their lanes restarted refill_min at a
+        // time (one divergent pass for several lanes); all at once when the
+        // queue is empty
         const unsigned need = __ballot_sync(FULL, !active);
-        if (need != 0u && !exhausted) {
+        const bool pass = exhausted ? (__ballot_sync(FULL, pending) != 0u) : (__popc(need) >= p.refill_min);
+        if (pass && pending) {
+            race_finalize<NP, FAM, NOISE>(p, L, h, np);
+            pending = false;
+        }
+        if (pass && !exhausted) {
             const int cnt = __popc(need);
             const int64_t avail = q_end - q_next;
             int64_t base = 0;
@@ -402,8 +411,8 @@ __global__ void __launch_bounds__(256) k_race(const __grid_constant__ RaceParams
             for (int s = 0; s < 4 && live; ++s)
                 live = race_step<NP, FAM, BOUND, NOISE, false>(p, L, h, vr, sr, np, ctr);
             if (!live) {
-                race_finalize<NP, FAM, NOISE>(p, L, h, np);
                 active = false;
+                pending = true;
             }
         }
     }
@@ -541,6 +550,7 @@ static int run_race(int fam, const float *v, const float *z, const float *t, con
     p.n_trials = n_trials; p.total = total; p.np = np; p.dt = dt; p.smooth = smooth ? 1 : 0;
     p.k_base = (uint32_t)((launch && launch->first_trial > 0) ? launch->first_trial : 0);
     p.chunk = (launch && launch->chunk >= 32) ? launch->chunk : 64;
+    p.refill_min = (launch && launch->refill_min > 0) ? min(launch->refill_min, 32) : SSM_REFILL_MIN_RACE;
     p.table = table; p.tstride = tstride; p.tlen = tlen;
     p.noise = noise; p.nlen = nlen; p.nunif = nunif;
     p.rts = rts; p.choices = choices; p.steps = steps; p.hdr = hdr;

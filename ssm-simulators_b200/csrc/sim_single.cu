@@ -7,10 +7,11 @@
 //    a 64-byte TrialRow with every derived float computed once, in the same
 //    IEEE operation order the reference uses (src/cssm/ddm_models.pyx:700-744).
 //  * The main kernel runs one grid of resident CTAs.  Each warp claims
-//    trajectories from a global work counter in chunks; whenever lanes finish
-//    (ballot), the warp hands them the next trajectories of its chunk
-//    (popc rank), so lanes never idle while work remains and divergence
-//    between fast and slow trajectories costs at most one 4-step block.
+//    trajectories from a global work counter in chunks; once refill_min of
+//    its lanes have ended their walks (ballot), it writes their results and
+//    hands them the next trajectories of its chunk (popc rank) in one
+//    divergent pass, so that pass is paid once per several trajectories and
+//    an ended lane idles for a few blocks at most.
 //  * Steps run in blocks of eight: two independent Philox4x32-10 calls yield
 //    eight 32-bit words = four Box-Muller pairs = the block's increments,
 //    already scaled to drift + s sqrt(dt) N(0,1); the steps themselves are
@@ -29,6 +30,7 @@
 #ifndef SSM_MIN_CTAS
 #define SSM_MIN_CTAS 4
 #endif
+
 
 namespace ssm {
 
@@ -69,10 +71,12 @@ struct SingleParams {
     float dt;
     int smooth;
     int chunk;
+    int refill_min;          // ended walks a warp collects before it restarts lanes
     const float *table;
     int64_t tstride, tlen;
     const float *dtable;     // DFLEX: drift v(t_ix) per trial, row stride dstride, dlen entries
     int64_t dstride, dlen;
+    int dvec;                // rows 16-byte aligned: a block's 8 drifts are two float4 loads
     const float *noise;      // injected increments: row w holds nlen floats
     int64_t nlen;
     const float *nunif;      // injected jitter uniforms, one per trajectory
@@ -329,6 +333,21 @@ __device__ __forceinline__ bool step_block(const SingleParams &p, Lane &L, const
     }
     constexpr bool INT_IX = NOISE || RECORD || BOUND == SSM_BOUND_TABLE || MODEL == M_DFLEX;
     const float *drow = (MODEL == M_DFLEX) ? p.dtable + (int64_t)L.k * p.dstride : nullptr;
+    // device RNG: the block's drifts v(t_ix .. t_ix+7) are read before the
+    // steps, off the dependency chain (a live walk starts every block at a
+    // multiple of 8 steps); past the table's end the last entry repeats
+    float dvq[BLK];
+    if (MODEL == M_DFLEX && !NOISE) {
+        if (p.dvec && (L.ix & 3) == 0 && L.ix + BLK <= p.dlen) {
+            const float4 *d4 = reinterpret_cast<const float4 *>(drow + L.ix);
+            const float4 a = __ldg(d4), b = __ldg(d4 + 1);
+            dvq[0] = a.x; dvq[1] = a.y; dvq[2] = a.z; dvq[3] = a.w;
+            dvq[4] = b.x; dvq[5] = b.y; dvq[6] = b.z; dvq[7] = b.w;
+        } else {
+#pragma unroll
+            for (int q = 0; q < BLK; ++q) dvq[q] = __ldg(drow + ((L.ix + q < p.dlen) ? L.ix + q : p.dlen - 1));
+        }
+    }
     bool live = true;
 #pragma unroll
     for (int q = 0; q < BLK; ++q) {
@@ -362,7 +381,7 @@ __device__ __forceinline__ bool step_block(const SingleParams &p, Lane &L, const
             } else {
                 if (MODEL == M_OU) L.y = fmaf(L.y, r.expo, g[q]);  // y (1 - g dt) + v dt + noise
                 else if (MODEL == M_DFLEX)                          // y + v(t_ix) dt + noise
-                    L.y += fmaf(__ldg(drow + ((L.ix < p.dlen) ? L.ix : p.dlen - 1)), p.dt, g[q]);
+                    L.y += fmaf(dvq[q], p.dt, g[q]);
                 else L.y += g[q];
                 L.tp += p.dt;
             }
@@ -460,12 +479,22 @@ __global__ void __launch_bounds__(256, SSM_MIN_CTAS) k_single(const __grid_const
     TrialRow r;
     L.w = 0; L.k = L.n = L.blk = 0; L.ix = 0; L.y = L.tp = L.ixf = L.dinc = 0.f;
     bool active = false;
+    bool pending = false;  // walk ended, result not yet written
     bool exhausted = false;
     int64_t q_next = 0, q_end = 0, hint = 0;
 
     for (;;) {
+        // Lanes whose walk ended wait (predicated off) until refill_min of
+        // them have: finishing and restarting lanes runs divergently, with the
+        // rest of the warp idle, so it is done for several lanes in one pass.
+        // Once the queue is empty, pending results are written at once.
         const unsigned need = __ballot_sync(FULL, !active);
-        if (need != 0u && !exhausted) {
+        const bool pass = exhausted ? (__ballot_sync(FULL, pending) != 0u) : (__popc(need) >= p.refill_min);
+        if (pass && pending) {
+            finalize<MODEL, NOISE>(p, L);
+            pending = false;
+        }
+        if (pass && !exhausted) {
             const int cnt = __popc(need);
             const int64_t avail = q_end - q_next;
             int64_t base = 0;
@@ -497,8 +526,8 @@ __global__ void __launch_bounds__(256, SSM_MIN_CTAS) k_single(const __grid_const
             const bool live = step_block<MODEL, BOUND, NOISE, false>(p, L, r, g);
             L.blk += 1;
             if (!live) {
-                finalize<MODEL, NOISE>(p, L);
                 active = false;
+                pending = true;
             }
         }
     }
@@ -663,9 +692,11 @@ static int run_single(const SingleCall &c) {
     p.k_base = (uint32_t)((c.launch && c.launch->first_trial > 0) ? c.launch->first_trial : 0);
     p.ustride = (c.model == M_FULL) ? 3 : 1;
     p.dtable = c.dtable; p.dstride = c.dstride; p.dlen = c.dlen;
+    p.dvec = (c.dtable && ((uintptr_t)c.dtable & 15u) == 0 && (c.dstride & 3) == 0) ? 1 : 0;
     p.dt = c.dt;
     p.smooth = c.smooth ? 1 : 0;
     p.chunk = (c.launch && c.launch->chunk >= 32) ? c.launch->chunk : 64;
+    p.refill_min = (c.launch && c.launch->refill_min > 0) ? min(c.launch->refill_min, 32) : SSM_REFILL_MIN;
     p.table = c.table; p.tstride = c.tstride; p.tlen = c.tlen;
     p.noise = c.noise; p.nlen = c.nlen; p.nunif = c.nunif;
     p.rts = c.rts; p.choices = c.choices; p.steps = c.steps;

@@ -27,11 +27,11 @@ BOUND_WEIBULL = 3
 
 
 class SsmLaunch(C.Structure):
-    """Mirror of ``ssm_launch`` (block size, CTAs per SM, warp chunk, random-stream index of
-    the call's first trial)."""
+    """Mirror of ``ssm_launch`` (block size, CTAs per SM, warp chunk, ended walks a warp
+    collects before restarting lanes, random-stream index of the call's first trial)."""
 
     _fields_ = [("block_threads", C.c_int), ("blocks_per_sm", C.c_int), ("chunk", C.c_int),
-                ("first_trial", C.c_int64)]
+                ("refill_min", C.c_int), ("first_trial", C.c_int64)]
 
 
 class SsmError(RuntimeError):

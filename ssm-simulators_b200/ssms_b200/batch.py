@@ -165,7 +165,8 @@ class BatchedSimulator:
             k0, k1 = int(bounds[i]), int(bounds[i + 1])
             o0, o1 = int(self.offsets_host[k0]), int(self.offsets_host[k1])
             st = cs0 if i % 2 == 0 else cs1
-            lopt = _lib.SsmLaunch(base.block_threads, base.blocks_per_sm, base.chunk, k0)
+            lopt = _lib.SsmLaunch(block_threads=base.block_threads, blocks_per_sm=base.blocks_per_sm,
+                                  chunk=base.chunk, refill_min=base.refill_min, first_trial=k0)
             with torch.cuda.stream(st):
                 dev.simulate_single(
                     self.family, v=self.v[k0:k1], z=self.z[k0:k1], t=self.t[k0:k1],

@@ -74,7 +74,7 @@ class SetBatch:
                 if not drift:
                     raise ValueError("ddm_flex needs the drift dict (drift_fun, drift_params)")
                 tab = dfn.drift_table(drift["drift_fun"], drift["drift_params"], K, bf.make_t_s(max_t, delta_t))
-                self.extra["drift_table"] = D.to_dev_f32(tab).reshape(tab.shape)
+                self.extra["drift_table"] = dev.padded_drift_table(tab)
         elif sim_name in RACE:
             v = np.asarray(kwargs["v"], np.float32)
             self.n_acc = int(v.shape[1])
@@ -85,6 +85,13 @@ class SetBatch:
             self.g = _dev(_col(kwargs["g"], K), K) if lca else None
             self.b = _dev(_col(kwargs["b"], K), K) if lca else None
             self.v_shape = v.shape
+        elif sim_name == "racing_diffusion_model":
+            v = np.asarray(kwargs["v"], np.float32)
+            self.n_acc = int(v.shape[1])
+            self.v_shape = v.shape
+            self.v = _dev(v)
+            self.b, self.A, self.t, self.s = (_dev(_col(kwargs[k], K), K, k) for k in ("b", "A", "t", "s"))
+            self.deadline = _dev(_col(kwargs["deadline"], K), K)
         elif sim_name == "lba_vanilla":
             v = np.asarray(kwargs["v"], np.float32)
             sd = np.asarray(kwargs["sd"], np.float32).reshape(K, -1)
@@ -98,7 +105,7 @@ class SetBatch:
         else:
             raise ValueError(f"no batched device path for simulator {sim_name!r}")
 
-    def run(self, seed: int, want_steps: bool = False) -> dev.SimOutput:
+    def run(self, seed: int, want_steps: bool = False, launch=None) -> dev.SimOutput:
         K, total = self.K, self.total
         if self.sim_name in SINGLE:
             rts = torch.empty(total, dtype=torch.float32, device="cuda")
@@ -108,14 +115,19 @@ class SetBatch:
                 a=self.a, alpha=self.alpha, n_trials=K, sample_offsets=self.offsets,
                 max_t=self.max_t, delta_t=self.delta_t, bound_kind=self.kind, bound_p1=self.p1,
                 bound_p2=self.p2, bound_table=self._table(), seed=seed, smooth_unif=self.smooth,
-                want_steps=want_steps, out_rts=rts, out_choices=chs, **self.extra)
+                want_steps=want_steps, out_rts=rts, out_choices=chs, launch=launch, **self.extra)
         if self.sim_name in RACE:
             return dev.simulate_race(
                 self.sim_name, v=self.v.reshape(self.v_shape), z=self.z, t=self.t, s=self.s,
                 deadline=self.deadline, n_trials=K, sample_offsets=self.offsets, g=self.g, b=self.b,
                 max_t=self.max_t, delta_t=self.delta_t, bound_kind=self.kind, a=self.a,
                 bound_p1=self.p1, bound_p2=self.p2, bound_table=self._table(), seed=seed,
-                smooth_unif=self.smooth, want_steps=want_steps, total=total)
+                smooth_unif=self.smooth, want_steps=want_steps, total=total, launch=launch)
+        if self.sim_name == "racing_diffusion_model":
+            return dev.simulate_rdm(v=self.v.reshape(self.v_shape), b=self.b, A=self.A, t=self.t, s=self.s,
+                                    deadline=self.deadline, n_trials=K, sample_offsets=self.offsets,
+                                    max_t=self.max_t, delta_t=self.delta_t, seed=seed, smooth_unif=self.smooth,
+                                    want_steps=want_steps, total=total, launch=launch)
         return dev.simulate_lba(v=self.v.reshape(self.v_shape), a=self.a, z=self.z,
                                 deadline=self.deadline, sd=self.sd, t=self.t, n_trials=K,
                                 sample_offsets=self.offsets, seed=seed, total=total)

@@ -41,6 +41,25 @@ def _opt_f32(x, n, name):
     return None if x is None else D.to_dev_f32(x, n, name)
 
 
+def _device_rows(t) -> bool:
+    return (isinstance(t, torch.Tensor) and t.is_cuda and t.dtype == torch.float32 and t.dim() == 2
+            and t.stride(1) == 1)
+
+
+def padded_drift_table(table) -> torch.Tensor:
+    """A ddm_flex drift table [n_trials, len] on the device with rows padded to
+    a multiple of 8 floats (the view [:, :len] of that buffer is returned), so
+    the kernel reads a block's eight drifts as two aligned float4 loads."""
+    shape = tuple(table.shape)
+    if len(shape) != 2:
+        raise ValueError("drift_table must be float32 [n_trials, len]")
+    K, n = int(shape[0]), int(shape[1])
+    src = D.to_dev_f32(table).reshape(K, n)
+    buf = torch.zeros((K, (n + 7) // 8 * 8), dtype=torch.float32, device=src.device)
+    buf[:, :n].copy_(src)
+    return buf[:, :n]
+
+
 def simulate_single(model: str, *, v, z, t, deadline, s, a=None, alpha=None, sv=None, sz=None, st=None, g=None,
                     drift_table=None,
                     n_trials: int, n_samples: int = 0, sample_offsets=None,
@@ -139,14 +158,16 @@ def simulate_single(model: str, *, v, z, t, deadline, s, a=None, alpha=None, sv=
     elif model == MODEL_DFLEX:
         if drift_table is None:
             raise ValueError("ddm_flex needs drift_table (float32 [n_trials, len])")
-        dtab = D.to_dev_f32(drift_table).reshape(-1)
-        dlen = int(drift_table.shape[-1])
-        if dlen < 1 or dtab.numel() < K * dlen:
+        # a device table is used as it is (any row stride); host tables are
+        # uploaded with rows padded for the kernel's vector loads
+        dtab = drift_table if _device_rows(drift_table) else padded_drift_table(drift_table)
+        dlen, dstride = int(dtab.shape[-1]), int(dtab.stride(0))
+        if dtab.dim() != 2 or dlen < 1 or int(dtab.shape[0]) < K:
             raise ValueError("drift_table must be float32 [n_trials, len]")
         status = L.ssm_ddm_flex(
             D.ptr(vt), D.ptr(at), D.ptr(zt), D.ptr(tt), D.ptr(dlt), D.ptr(s_t), K, int(n_samples), D.ptr(offs),
             float(np.float32(max_t)), float(np.float32(delta_t)), int(bound_kind), D.ptr(p1t), D.ptr(p2t),
-            D.ptr(tab), tstride, tlen, D.ptr(dtab), dlen, dlen, *common_tail, ctypes.addressof(lopt),
+            D.ptr(tab), tstride, tlen, int(dtab.data_ptr()), dstride, dlen, *common_tail, ctypes.addressof(lopt),
             D.ptr(ws), ws.numel(), sp)
     elif model in (MODEL_SDV, MODEL_FULL, MODEL_OU):
         bound_args = (K, int(n_samples), D.ptr(offs), float(np.float32(max_t)), float(np.float32(delta_t)),

@@ -38,23 +38,26 @@ def _load() -> dict[str, dict]:
     return _cache
 
 
-# (block_threads, blocks_per_sm, chunk): CTA size, CTAs per SM (0 = as many as
-# fit) and the warp's claim size
-DEFAULT_CANDIDATES = [(bt, bps, ch) for bt in (128, 256) for bps in (0, 3) for ch in (32, 64, 128, 256)]
+# (block_threads, blocks_per_sm, chunk[, refill_min]): CTA size, CTAs per SM
+# (0 = as many as fit), the warp's claim size and the ended walks a warp
+# collects before restarting lanes (0 = library default)
+DEFAULT_CANDIDATES = [(bt, bps, ch, rm) for bt in (128, 256) for bps in (0, 3) for ch in (64, 128, 256)
+                      for rm in (0, 2, 6)]
 
 
 def launch_for(model: str) -> _lib.SsmLaunch:
     cfg = _load().get(model, {})
-    return _lib.SsmLaunch(int(cfg.get("block_threads", 0)), int(cfg.get("blocks_per_sm", 0)),
-                          int(cfg.get("chunk", 0)))
+    return _lib.SsmLaunch(block_threads=int(cfg.get("block_threads", 0)),
+                          blocks_per_sm=int(cfg.get("blocks_per_sm", 0)), chunk=int(cfg.get("chunk", 0)),
+                          refill_min=int(cfg.get("refill_min", 0)))
 
 
-def set_launch(model: str, block_threads: int, blocks_per_sm: int, chunk: int,
+def set_launch(model: str, block_threads: int, blocks_per_sm: int, chunk: int, refill_min: int = 0,
                persist: bool = False) -> None:
     with _lock:
         d = _load()
         d[model] = {"block_threads": int(block_threads), "blocks_per_sm": int(blocks_per_sm),
-                    "chunk": int(chunk)}
+                    "chunk": int(chunk), "refill_min": int(refill_min)}
         if persist:
             _PATH.write_text(json.dumps(d, indent=1, sort_keys=True))
 
@@ -68,8 +71,9 @@ def autotune(model: str, run, candidates=None, repeats: int = 2, persist: bool =
     if candidates is None:
         candidates = DEFAULT_CANDIDATES
     timings = []
-    for bt, bps, ch in candidates:
-        opt = _lib.SsmLaunch(bt, bps, ch)
+    for cand in candidates:
+        bt, bps, ch, rm = (tuple(cand) + (0,))[:4]
+        opt = _lib.SsmLaunch(block_threads=bt, blocks_per_sm=bps, chunk=ch, refill_min=rm)
         run(opt)  # warm-up
         torch.cuda.synchronize()
         best = float("inf")
@@ -81,10 +85,11 @@ def autotune(model: str, run, candidates=None, repeats: int = 2, persist: bool =
             e1.record()
             e1.synchronize()
             best = min(best, e0.elapsed_time(e1))
-        timings.append(((bt, bps, ch), best))
-    (bt, bps, ch), _ = min(timings, key=lambda x: x[1])
-    set_launch(model, bt, bps, ch, persist=persist)
-    return {"best": {"block_threads": bt, "blocks_per_sm": bps, "chunk": ch},
+        timings.append((tuple(cand), best))
+    cand, _ = min(timings, key=lambda x: x[1])
+    bt, bps, ch, rm = (tuple(cand) + (0,))[:4]
+    set_launch(model, bt, bps, ch, rm, persist=persist)
+    return {"best": {"block_threads": bt, "blocks_per_sm": bps, "chunk": ch, "refill_min": rm},
             "timings": timings, "when": time.time()}
 
 

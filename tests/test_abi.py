@@ -55,3 +55,29 @@ def test_argument_errors_are_reported_without_a_launch():
     assert b"required" in lib.ssm_last_error()
     with pytest.raises(ValueError):
         _lib.check(st)
+
+
+def test_launch_struct_layout_matches_the_header(tmp_path):
+    """ctypes' SsmLaunch has the size and field offsets the C compiler gives ssm_launch."""
+    import shutil
+    import subprocess
+
+    import pytest
+
+    from ssms_b200 import _lib
+
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    fields = [f for f, _ in _lib.SsmLaunch._fields_]
+    src = tmp_path / "layout.c"
+    src.write_text("#include <stddef.h>\n#include <stdio.h>\n#include \"ssm_b200.h\"\nint main(void) {\n"
+                   "  printf(\"%zu\\n\", sizeof(ssm_launch));\n"
+                   + "".join(f"  printf(\"%zu\\n\", offsetof(ssm_launch, {f}));\n" for f in fields)
+                   + "  return 0;\n}\n")
+    exe = tmp_path / "layout"
+    subprocess.run([cc, "-I", str(ROOT / "include"), str(src), "-o", str(exe)], check=True)
+    got = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
+    assert got[0] == ctypes.sizeof(_lib.SsmLaunch)
+    assert got[1:] == [getattr(_lib.SsmLaunch, f).offset for f in fields]
+    assert getattr(_lib.SsmLaunch, "first_trial").offset == 16  # unchanged by refill_min (padding slot)

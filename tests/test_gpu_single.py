@@ -169,7 +169,7 @@ def test_results_do_not_depend_on_launch_shape(cuda):
     outs = []
     for bt, bps, ch in [(256, 0, 64), (128, 1, 32), (64, 2, 256)]:
         outs.append(_gpu("ddm_flexbound", th, N, K, spec, max_t=20.0, seed=77,
-                         launch=_lib.SsmLaunch(bt, bps, ch)))
+                         launch=_lib.SsmLaunch(block_threads=bt, blocks_per_sm=bps, chunk=ch)))
     for o in outs[1:]:
         for a, b in zip(outs[0][:3], o[:3]):
             np.testing.assert_array_equal(a, b)

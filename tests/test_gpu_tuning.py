@@ -1,5 +1,5 @@
 """The launch autotuner: results do not depend on the launch configuration
-(CTA size, CTAs per SM, warp claim size), and the tuner keeps the fastest
+(CTA size, CTAs per SM, warp claim size, ended walks collected before a refill), and the tuner keeps the fastest
 candidate for the simulator family."""
 
 import numpy as np
@@ -23,8 +23,8 @@ def _sim():
 def test_results_do_not_depend_on_the_launch_configuration(cuda):
     sim = _sim()
     ref = None
-    for bt, bps, ch in [(256, 0, 64), (128, 0, 32), (256, 2, 256), (64, 3, 128)]:
-        out = sim.run(want_steps=True, launch=D.launch_opts(bt, bps, ch))
+    for bt, bps, ch, rm in [(256, 0, 64, 0), (128, 0, 32, 1), (256, 2, 256, 32), (64, 3, 128, 3)]:
+        out = sim.run(want_steps=True, launch=D.launch_opts(bt, bps, ch, refill_min=rm))
         got = (out.rts.cpu().numpy().view(np.int32), out.choices.cpu().numpy(), out.steps.cpu().numpy())
         if ref is None:
             ref = got
@@ -37,12 +37,14 @@ def test_autotune_keeps_the_fastest_candidate(cuda):
     saved = dict(tuning._load())
     try:
         sim = _sim()
-        cands = [(128, 0, 64), (256, 0, 64), (256, 0, 256)]
+        cands = [(128, 0, 64), (256, 0, 64, 2), (256, 0, 256, 6)]
         res = tuning.autotune("ddm_flexbound", lambda opt: sim.run(launch=opt), candidates=cands, repeats=1)
         times = dict(res["timings"])
-        best = (res["best"]["block_threads"], res["best"]["blocks_per_sm"], res["best"]["chunk"])
-        assert best in cands and times[best] == min(times.values())
+        best = min(times, key=times.get)
+        assert best in cands
+        b = res["best"]
+        assert (b["block_threads"], b["blocks_per_sm"], b["chunk"], b["refill_min"]) == (tuple(best) + (0,))[:4]
         lo = tuning.launch_for("ddm_flexbound")
-        assert (lo.block_threads, lo.blocks_per_sm, lo.chunk) == best
+        assert (lo.block_threads, lo.blocks_per_sm, lo.chunk, lo.refill_min) == (tuple(best) + (0,))[:4]
     finally:
         tuning._cache = saved

@@ -15,6 +15,7 @@ import zlib
 import numpy as np
 import pytest
 
+from ssms_b200 import _lib
 from ssms_b200 import boundary_functions as bf
 from ssms_b200 import cssm
 from ssms_b200 import device as dev
@@ -207,6 +208,33 @@ def test_ddm_flex_noise_injection_bit_exact(cuda, oracle, drift, bname):
     np.testing.assert_array_equal(out.steps.cpu().numpy(), o_st)
     np.testing.assert_array_equal(out.choices.cpu().numpy(), o_ch)
     np.testing.assert_array_equal(_bits(out.rts.cpu().numpy()), _bits(o_rt))
+
+
+def test_ddm_flex_drift_rows_padded_or_not_give_identical_walks(cuda):
+    """Rows padded to 16-byte multiples are read as float4 pairs per 8-step
+    block, an odd row stride one float at a time; the walks are the same."""
+    import torch
+
+    from ssms_b200 import drift_functions as dfn
+
+    rng = np.random.default_rng(21)
+    K, N, max_t = 6, 3000, 3.0
+    th = _flex_theta(rng, K)
+    # weak drifts, wide bounds: many walks reach the end of the table
+    th["v"], th["tcoh"], th["dcoh"] = (f32(rng.uniform(-0.2, 0.2, K)) for _ in range(3))
+    t_s = bf.make_t_s(max_t, 0.001)
+    table = dfn.drift_table(dfn.conflict_ds_drift, {k: th[k] for k in dfn.DRIFTS["conflict_ds_drift"][1]}, K, t_s)
+    assert table.shape[1] % 4 != 0
+    outs = []
+    for tab in (dev.padded_drift_table(table), torch.from_numpy(table).cuda()):
+        o = dev.simulate_single("ddm_flex", v=th["v"], z=th["z"], t=th["t"], deadline=f32([999] * K),
+                                s=f32([1] * K), a=f32([3.0] * K), drift_table=tab, n_trials=K, n_samples=N,
+                                max_t=max_t, delta_t=0.001, bound_kind=_lib.BOUND_CONSTANT, seed=9,
+                                smooth_unif=True, want_steps=True)
+        outs.append((o.rts.view(torch.int32).cpu().numpy(), o.choices.cpu().numpy(), o.steps.cpu().numpy()))
+    assert outs[0][2].max() >= table.shape[1] - 8  # the table's last block is exercised
+    for a, b in zip(*outs):
+        np.testing.assert_array_equal(a, b)
 
 
 @pytest.mark.parametrize("drift,bname", [("gamma_drift", "constant"), ("conflict_ds_drift", "angle")])

@@ -54,7 +54,7 @@ def _call_static(fn, th, K, N, seed):
     rts = torch.full((K * N,), float("nan"), device="cuda")
     chs = torch.full((K * N,), 7, dtype=torch.int32, device="cuda")
     steps = torch.full((K * N,), -1, dtype=torch.int32, device="cuda")
-    opt = _lib.SsmLaunch(0, 0, 0)
+    opt = _lib.SsmLaunch()
     st = fn(th["v"].data_ptr(), th["a"].data_ptr(), th["z"].data_ptr(), th["t"].data_ptr(),
             th["deadline"].data_ptr(), th["s"].data_ptr(), K, N, None, 20.0, None, 0.001,
             _lib.BOUND_LINEAR, th["slope"].data_ptr(), None, None, 0, 0, seed, 1, None, 0, None,
@@ -100,7 +100,7 @@ def test_static_entry_rejects_sizes_beyond_its_array():
     lib, fn = _entry()
     dummy = torch.zeros(1, device="cuda")
     p = dummy.data_ptr()
-    opt = _lib.SsmLaunch(0, 0, 0)
+    opt = _lib.SsmLaunch()
     st = fn(p, p, p, p, p, p, MAX_TRIALS + 1, 1, None, 20.0, None, 0.001, _lib.BOUND_CONSTANT,
             None, None, None, 0, 0, 1, 0, None, 0, None, p, p, None, None, 0,
             ctypes.addressof(opt), torch.cuda.current_stream().cuda_stream)
