@@ -208,11 +208,11 @@ class ClockSampler:
 
 # ------------------------------------------------------------------ GPU side
 # DRAM bytes (read + write) of one k_single launch on the 4096-theta workload,
-# from one ncu capture of that launch (dram__bytes_read.sum 10,920,448 +
-# dram__bytes_write.sum 285,464,064).
+# from one ncu capture of that launch (dram__bytes_read.sum 12,092,928 +
+# dram__bytes_write.sum 286,508,032).
 # The algorithmic output is 8 B per trajectory (338 MB); part of it is still in
 # L2 when the kernel ends, so the measured writes sit slightly below it.
-K_SINGLE_TRAFFIC_BYTES = 10_920_448 + 285_464_064
+K_SINGLE_TRAFFIC_BYTES = 12_092_928 + 286_508_032
 
 
 def run_ours(args, rank, world, local_rank):

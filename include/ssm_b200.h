@@ -61,6 +61,17 @@ typedef struct ssm_launch {
      * sample_offsets (whose values stay global output indices) -- gives the
      * same outputs as one call over the whole batch. */
     int64_t first_trial;
+    /* Processing order of the trials (single-accumulator simulators, ragged
+     * layout only; NULL = index order): trial_order[j] is the trial simulated
+     * j-th and order_offsets[0..n_trials] the prefix sums of the sample
+     * counts in that order (order_offsets[0] = 0).  Outputs and random
+     * streams do not depend on the order; starting the longest walks first
+     * shortens the launch's tail.  An entry that does not match
+     * sample_offsets stores SSM_ERR_ARG and its position in the device error
+     * word (ssm_check_status then returns SSM_ERR_DEVICE) and its
+     * trajectories are skipped. */
+    const int32_t *trial_order;
+    const int64_t *order_offsets;
 } ssm_launch;
 
 /* Version / diagnostics -------------------------------------------------- */

@@ -517,6 +517,8 @@ static int run_race(int fam, const float *v, const float *z, const float *t, con
                 "max_t must be finite with max_t / delta_t <= 2^23");
     SSM_REQUIRE(n_trials == 0 || (v && z && t && s && deadline), "v, z, t, s, deadline are required");
     SSM_REQUIRE(fam != FAM_LCA || n_trials == 0 || (g && b), "lca needs g and b");
+    SSM_REQUIRE(!launch || (!launch->trial_order && !launch->order_offsets),
+                "a trial order is supported by the single-accumulator simulators only");
     SSM_REQUIRE((rts && choices) || (!offsets && n_trials * n_samples == 0), "rts and choices outputs are required");
     SSM_REQUIRE(bound >= SSM_BOUND_TABLE && bound <= SSM_BOUND_WEIBULL, "unknown boundary kind %d", bound);
     SSM_REQUIRE(bound == SSM_BOUND_TABLE || n_trials == 0 || a, "boundary height a is required");

@@ -64,6 +64,8 @@ struct SingleParams {
     PhiloxKeys key;
     const TrialRow *rows;
     const int64_t *offsets;  // ragged prefix sums (n_trials + 1) or nullptr
+    const int32_t *order;    // ragged only: trial simulated j-th (nullptr = index order)
+    const int64_t *qoff;     // prefix sums of the sample counts in that order
     int64_t n_trials;
     int64_t total;           // number of trajectories; -1 = offsets[n_trials] - offsets[0]
     uint32_t k_base;         // random-stream index of trial 0 (trial windows of a larger batch)
@@ -424,13 +426,27 @@ __device__ __forceinline__ void finalize(const SingleParams &p, const Lane &L) {
     if (p.steps) p.steps[L.w] = (int)L.ixf;
 }
 
+// Start lane L on the trajectory with queue index w; false (and the error
+// word set) if a caller-given processing order does not cover that index.
 template <int MODEL, bool NOISE>
-__device__ __forceinline__ void lane_init(const SingleParams &p, Lane &L, TrialRow &r, int64_t w,
+__device__ __forceinline__ bool lane_init(const SingleParams &p, Lane &L, TrialRow &r, int64_t w,
                                           int64_t &hint) {
     int64_t k, n;
     if (p.offsets == nullptr) {
         k = w % p.n_trials;
         n = w / p.n_trials;
+    } else if (p.order != nullptr) {
+        // queue index -> position j in the processing order -> trial k; the
+        // output index stays offsets[k] + n, so results do not depend on the order
+        const int64_t j = ragged_find(p.qoff, p.n_trials, w, hint);
+        hint = j;
+        k = __ldg(p.order + j);
+        n = w - __ldg(p.qoff + j);
+        if (k < 0 || k >= p.n_trials || n < 0 || n >= __ldg(p.offsets + k + 1) - __ldg(p.offsets + k)) {
+            raise_error(p.hdr, SSM_ERR_ARG, (int)j);
+            return false;
+        }
+        w = __ldg(p.offsets + k) + n;
     } else {
         w += __ldg(p.offsets);  // global output index (trial windows start past 0)
         k = ragged_find(p.offsets, p.n_trials, w, hint);
@@ -465,6 +481,7 @@ __device__ __forceinline__ void lane_init(const SingleParams &p, Lane &L, TrialR
         if (MODEL == M_FULL)
             L.y = __double2float_rn((double)L.y + (2.0 * ((double)uy - 0.5)) * (double)r.inv_alpha);
     }
+    return true;
 }
 
 // ------------------------------------------------------------------ main kernel
@@ -507,10 +524,7 @@ __global__ void __launch_bounds__(256, SSM_MIN_CTAS) k_single(const __grid_const
             if (!active) {
                 const int rank = __popc(need & lt_mask);
                 const int64_t w = (rank < avail) ? q_next + rank : base + (rank - avail);
-                if (w < total) {
-                    lane_init<MODEL, NOISE>(p, L, r, w, hint);
-                    active = true;
-                }
+                if (w < total) active = lane_init<MODEL, NOISE>(p, L, r, w, hint);
             }
             if (avail >= cnt) {
                 q_next += cnt;
@@ -572,7 +586,10 @@ struct Launcher {
         kern<<<grid, threads, 0, st>>>(p);
         SSM_CUDA(cudaGetLastError());
         if (p.traj && p.traj_len > 0) {
-            k_record<MODEL, BOUND, NOISE><<<1, 128, 0, st>>>(p);
+            SingleParams pr = p;  // trial 0 / sample 0, whatever the processing order
+            pr.order = nullptr;
+            pr.qoff = nullptr;
+            k_record<MODEL, BOUND, NOISE><<<1, 128, 0, st>>>(pr);
             SSM_CUDA(cudaGetLastError());
         }
         return SSM_OK;
@@ -662,6 +679,10 @@ static int run_single(const SingleCall &c) {
     }
     SSM_REQUIRE(!c.noise || (c.nlen > 0 && c.nunif), "noise_rows needs noise_row_len > 0 and noise_unif");
     SSM_REQUIRE(!c.traj || c.traj_len >= 1, "traj needs traj_len >= 1");
+    SSM_REQUIRE(!c.launch || (!c.launch->trial_order == !c.launch->order_offsets),
+                "trial_order and order_offsets go together");
+    SSM_REQUIRE(!c.launch || !c.launch->trial_order || c.offsets,
+                "a trial order needs the ragged layout (sample_offsets)");
     const size_t need = single_ws_bytes(c.n_trials);
     if (!c.ws || c.ws_bytes < need || ((uintptr_t)c.ws & 255u)) {
         set_error("workspace must be 256-byte aligned and hold %zu bytes", need);
@@ -687,6 +708,8 @@ static int run_single(const SingleCall &c) {
     p.key = philox_keys(c.seed);
     p.rows = rows;
     p.offsets = c.offsets;
+    p.order = c.offsets && c.launch ? c.launch->trial_order : nullptr;
+    p.qoff = p.order ? c.launch->order_offsets : nullptr;
     p.n_trials = c.n_trials;
     p.total = c.offsets ? -1 : c.n_trials * c.n_samples;
     p.k_base = (uint32_t)((c.launch && c.launch->first_trial > 0) ? c.launch->first_trial : 0);

@@ -28,10 +28,12 @@ BOUND_WEIBULL = 3
 
 class SsmLaunch(C.Structure):
     """Mirror of ``ssm_launch`` (block size, CTAs per SM, warp chunk, ended walks a warp
-    collects before restarting lanes, random-stream index of the call's first trial)."""
+    collects before restarting lanes, random-stream index of the call's first trial, device
+    pointers of an optional trial processing order and its sample-count prefix sums)."""
 
     _fields_ = [("block_threads", C.c_int), ("blocks_per_sm", C.c_int), ("chunk", C.c_int),
-                ("refill_min", C.c_int), ("first_trial", C.c_int64)]
+                ("refill_min", C.c_int), ("first_trial", C.c_int64), ("trial_order", C.c_void_p),
+                ("order_offsets", C.c_void_p)]
 
 
 class SsmError(RuntimeError):

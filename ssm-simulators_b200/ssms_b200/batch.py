@@ -36,16 +36,77 @@ BATCH_MODELS = {
 _EXTRA = {"full_ddm": ("sz", "sv", "st"), "ddm_sdv": ("sv",), "ornstein_uhlenbeck": ("g",)}
 
 
+def expected_walk_time(v, a, z, s=1.0, *, legacy: bool = False, bound_kind: int = _lib.BOUND_CONSTANT,
+                       p1=None, p2=None, t_cap=20.0) -> np.ndarray:
+    """Per-trial estimate of the mean walk duration, used only to order work.
+
+    Mean first-passage time of Brownian motion with drift v and diffusion s^2
+    out of (0, L) from x: (L (1 - e^{-2vx/s^2}) / (1 - e^{-2vL/s^2}) - x) / v,
+    x (L - x) / s^2 at v = 0; barriers +-a with start (2z - 1) a (L = 2a,
+    x = 2za), or 0 and a with start z a for the legacy DDM.  A collapsing
+    linear bound (slope p1 < 0) ends every walk by a / -p1, a Weibull bound
+    a exp(-(t/beta)^alpha) by about beta ln(a / 0.05)^(1/alpha); everything
+    is capped at t_cap (max_t, or the deadline)."""
+    v, a, z = (np.asarray(x, np.float64).reshape(-1) for x in (v, a, z))
+    K = v.shape[0]
+    s2 = np.broadcast_to(np.asarray(s, np.float64).reshape(-1), (K,)) ** 2
+    a = np.maximum(np.broadcast_to(a, (K,)), 1e-6)
+    z = np.clip(np.broadcast_to(z, (K,)), 0.0, 1.0)
+    L, x = (a, z * a) if legacy else (2 * a, 2 * z * a)
+    mu = np.where(v < 0, -v, v)
+    x = np.where(v < 0, L - x, x)  # reflect: drift towards the upper barrier
+    c = 2 * mu / np.maximum(s2, 1e-12)
+    with np.errstate(over="ignore", invalid="ignore", divide="ignore"):
+        drifting = (mu * L / np.maximum(s2, 1e-12)) > 1e-4
+        e = np.where(drifting, (L * np.expm1(-c * x) / np.expm1(-c * L) - x) / np.where(drifting, mu, 1.0),
+                     x * (L - x) / np.maximum(s2, 1e-12))
+    e = np.maximum(np.nan_to_num(e, nan=0.0, posinf=np.inf), 0.0)
+    cap = np.broadcast_to(np.asarray(t_cap, np.float64).reshape(-1), (K,)).copy()
+    if bound_kind == _lib.BOUND_LINEAR and p1 is not None:
+        slope = np.broadcast_to(np.asarray(p1, np.float64).reshape(-1), (K,))
+        with np.errstate(divide="ignore"):
+            cap = np.minimum(cap, np.where(slope < 0, a / np.maximum(-slope, 1e-12), np.inf))
+    elif bound_kind == _lib.BOUND_WEIBULL and p1 is not None and p2 is not None:
+        al = np.maximum(np.broadcast_to(np.asarray(p1, np.float64).reshape(-1), (K,)), 1e-3)
+        be = np.broadcast_to(np.asarray(p2, np.float64).reshape(-1), (K,))
+        cap = np.minimum(cap, be * np.log(np.maximum(a / 0.05, 1.0 + 1e-9)) ** (1.0 / al))
+    return np.minimum(e, cap)
+
+
+def longest_first(expected_time, n_samples) -> tuple[np.ndarray, np.ndarray]:
+    """(trial_order int32, order_offsets int64): trials by decreasing expected
+    walk time (ties in index order) and the prefix sums of their sample counts
+    in that order -- the longest walks start first, so the launch does not end
+    waiting on a long walk that started late."""
+    order = np.argsort(-np.asarray(expected_time, np.float64), kind="stable").astype(np.int32)
+    ns = np.asarray(n_samples, np.int64).reshape(-1)
+    return order, np.concatenate([[0], np.cumsum(ns[order])]).astype(np.int64)
+
+
+def with_order(base, order_t=None, qoff_t=None, first_trial: int | None = None) -> _lib.SsmLaunch:
+    """A copy of the launch options with the given trial order (device tensors
+    the caller keeps alive while the launch runs)."""
+    return _lib.SsmLaunch(block_threads=base.block_threads, blocks_per_sm=base.blocks_per_sm, chunk=base.chunk,
+                          refill_min=base.refill_min,
+                          first_trial=base.first_trial if first_trial is None else int(first_trial),
+                          trial_order=None if order_t is None else order_t.data_ptr(),
+                          order_offsets=None if qoff_t is None else qoff_t.data_ptr())
+
+
 class BatchedSimulator:
     """Device-resident batch of trials for the single-accumulator models.
 
     theta: dict of per-trial float32 arrays (model parameter names, e.g.
     v, a, z, t, theta for "angle"); n_samples: int array [n_trials].
+    order: "longest_first" (default) simulates the trials in decreasing order
+    of their expected walk time (``expected_walk_time``), "index" in index
+    order; outputs are the same either way.
     """
 
     def __init__(self, model: str, theta: dict, n_samples, *, max_t: float = 20.0,
                  max_t_per_trial=None, delta_t: float = 0.001, seed: int = 0,
-                 smooth_unif: bool = True, s=None, deadline=None, launch=None):
+                 smooth_unif: bool = True, s=None, deadline=None, launch=None,
+                 order: str = "longest_first"):
         if model not in BATCH_MODELS:
             raise ValueError(f"unsupported batched model {model!r}; choose from {sorted(BATCH_MODELS)}")
         family, bname, bkeys = BATCH_MODELS[model]
@@ -83,6 +144,20 @@ class BatchedSimulator:
             self.table = torch.from_numpy(np.ascontiguousarray(self.spec["table"])).cuda()
         self.p1 = None if self.spec["p1"] is None else D.to_dev_f32(self.spec["p1"], K, "p1")
         self.p2 = None if self.spec["p2"] is None else D.to_dev_f32(self.spec["p2"], K, "p2")
+        if order not in ("longest_first", "index"):
+            raise ValueError("order must be 'longest_first' or 'index'")
+        self.order_t = self.qoff_t = self.expected_time = None
+        self._window_orders: dict = {}
+        if order == "longest_first" and K > 1:
+            cap = np.full(K, float(max_t)) if max_t_per_trial is None else f(max_t_per_trial).astype(np.float64)
+            dl = np.full(K, 999.0) if deadline is None else f(deadline).astype(np.float64)
+            cap = np.minimum(cap, np.maximum(dl - th["t"], 0.0))
+            self.expected_time = expected_walk_time(
+                th["v"], th.get("a", np.ones(K, np.float32)), th["z"], 1.0 if s is None else f(s),
+                legacy=family == "ddm", bound_kind=self.spec["kind"], p1=self.spec["p1"], p2=self.spec["p2"],
+                t_cap=cap)
+            o, q = longest_first(self.expected_time, ns)
+            self.order_t, self.qoff_t = torch.from_numpy(o).cuda(), torch.from_numpy(q).cuda()
         self.offsets = torch.from_numpy(self.offsets_host).cuda()
         self.rts = torch.empty(self.total, dtype=torch.float32, device="cuda")
         self.choices = torch.empty(self.total, dtype=torch.int32, device="cuda")
@@ -94,15 +169,33 @@ class BatchedSimulator:
         """Launch the batch on the current stream (asynchronous)."""
         if self.family == "ddm" and self.max_t_k is not None:
             raise ValueError("per-trial max_t is supported by the flexible-bound families")
+        lopt = launch if launch is not None else self.launch
+        if lopt is None:
+            lopt = launch_for(self.family)
+        if self.order_t is not None and not lopt.trial_order:
+            lopt = with_order(lopt, self.order_t, self.qoff_t)
         self.last = dev.simulate_single(
             self.family, v=self.v, z=self.z, t=self.t, deadline=self.deadline, s=self.s, a=self.a,
             alpha=self.alpha, n_trials=self.n_trials, sample_offsets=self.offsets,
             max_t=self.max_t, max_t_per_trial=self.max_t_k, delta_t=self.delta_t,
             bound_kind=self.spec["kind"], bound_p1=self.p1, bound_p2=self.p2,
             bound_table=self.table, seed=self.seed, smooth_unif=self.smooth,
-            want_steps=want_steps, out_rts=self.rts, out_choices=self.choices,
-            launch=launch if launch is not None else self.launch, **self.extra)
+            want_steps=want_steps, out_rts=self.rts, out_choices=self.choices, launch=lopt, **self.extra)
         return self.last
+
+    def _window_order(self, bounds: np.ndarray) -> list:
+        """Per window [k0, k1): its trials longest-first, as window-local
+        indices with their sample-count prefix sums (device tensors, cached)."""
+        key = tuple(int(b) for b in bounds)
+        if key not in self._window_orders:
+            ns = np.diff(self.offsets_host)
+            out = []
+            for i in range(len(bounds) - 1):
+                k0, k1 = int(bounds[i]), int(bounds[i + 1])
+                o, q = longest_first(self.expected_time[k0:k1], ns[k0:k1])
+                out.append((torch.from_numpy(o).cuda(), torch.from_numpy(q).cuda()))
+            self._window_orders[key] = out
+        return self._window_orders[key]
 
     def capture(self) -> torch.cuda.CUDAGraph:
         """Capture one launch of the whole batch in a CUDA graph (replay() reruns it)."""
@@ -154,6 +247,7 @@ class BatchedSimulator:
         cs0, cs1, copy_s = self._streams
         bounds = self.window_bounds(chunks)
         base = launch_for(self.family) if self.launch is None else self.launch
+        orders = self._window_order(bounds) if self.expected_time is not None else None
         L = _lib.lib()
         span = int(np.max(np.diff(bounds)))
         for tag in (10, 11):  # reserve both workspaces before any window runs
@@ -165,8 +259,7 @@ class BatchedSimulator:
             k0, k1 = int(bounds[i]), int(bounds[i + 1])
             o0, o1 = int(self.offsets_host[k0]), int(self.offsets_host[k1])
             st = cs0 if i % 2 == 0 else cs1
-            lopt = _lib.SsmLaunch(block_threads=base.block_threads, blocks_per_sm=base.blocks_per_sm,
-                                  chunk=base.chunk, refill_min=base.refill_min, first_trial=k0)
+            lopt = with_order(base, *(orders[i] if orders else (None, None)), first_trial=k0)
             with torch.cuda.stream(st):
                 dev.simulate_single(
                     self.family, v=self.v[k0:k1], z=self.z[k0:k1], t=self.t[k0:k1],

@@ -18,6 +18,8 @@ from . import _device as D
 from . import boundary_functions as bf
 from . import device as dev
 from . import drift_functions as dfn
+from .batch import expected_walk_time, longest_first, with_order
+from .tuning import launch_for
 
 SINGLE = ("ddm_flexbound", "levy_flexbound", "ddm", "full_ddm", "ddm_sdv", "ornstein_uhlenbeck", "ddm_flex")
 _PER_TRIAL = {"full_ddm": ("sz", "sv", "st"), "ddm_sdv": ("sv",), "ornstein_uhlenbeck": ("g",)}
@@ -70,6 +72,16 @@ class SetBatch:
             self.deadline, self.s = _dev(_col(kwargs["deadline"], K), K), _dev(_col(kwargs["s"], K), K)
             self.alpha = _dev(_col(kwargs["alpha"], K), K) if sim_name == "levy_flexbound" else None
             self.extra = {k: _dev(_col(kwargs[k], K), K, k) for k in _PER_TRIAL.get(sim_name, ())}
+            # trials longest-first (outputs do not depend on the order)
+            self.order_t = self.qoff_t = None
+            if K > 1:
+                cap = np.minimum(self.max_t, np.maximum(np.asarray(_col(kwargs["deadline"], K), np.float64)
+                                                        - np.asarray(_col(kwargs["t"], K), np.float64), 0.0))
+                est = expected_walk_time(_col(kwargs["v"], K), spec["a"], _col(kwargs["z"], K),
+                                         _col(kwargs["s"], K), legacy=sim_name == "ddm", bound_kind=self.kind,
+                                         p1=spec["p1"], p2=spec["p2"], t_cap=cap)
+                o, q = longest_first(est, ns)
+                self.order_t, self.qoff_t = torch.from_numpy(o).cuda(), torch.from_numpy(q).cuda()
             if sim_name == "ddm_flex":
                 if not drift:
                     raise ValueError("ddm_flex needs the drift dict (drift_fun, drift_params)")
@@ -108,6 +120,10 @@ class SetBatch:
     def run(self, seed: int, want_steps: bool = False, launch=None) -> dev.SimOutput:
         K, total = self.K, self.total
         if self.sim_name in SINGLE:
+            if launch is None:
+                launch = launch_for(self.sim_name)
+            if self.order_t is not None and not launch.trial_order:
+                launch = with_order(launch, self.order_t, self.qoff_t)
             rts = torch.empty(total, dtype=torch.float32, device="cuda")
             chs = torch.empty(total, dtype=torch.int32, device="cuda")
             return dev.simulate_single(

@@ -113,3 +113,40 @@ def test_bin_simulator_output_counts():
            "metadata": {"max_t": 20.0, "possible_choices": [-1, 1], "n_samples": 4}}
     h = bin_simulator_output(out, nbins=4, max_t=-1, freq_cnt=True)
     assert h.shape == (4, 2) and h.sum() == 4 and h[3, 1] == 1  # rt 30 lands in the open last bin
+
+
+# ------------------------------------------------------------------ trial order
+def test_expected_walk_time_limits():
+    from ssms_b200 import _lib
+    from ssms_b200.batch import expected_walk_time
+
+    # no drift: x (L - x) / s^2 -> a^2 from the middle of +-a, a^2 z (1 - z) for [0, a]
+    np.testing.assert_allclose(expected_walk_time([0.0], [1.0], [0.5], t_cap=1e9), [1.0])
+    np.testing.assert_allclose(expected_walk_time([0.0], [2.0], [0.25], legacy=True, t_cap=1e9), [0.75])
+    np.testing.assert_allclose(expected_walk_time([0.0], [1.0], [0.5], s=[2.0], t_cap=1e9), [0.25])
+    # strong drift: distance to the barrier / v, the same for either sign
+    e = expected_walk_time([8.0, -8.0], [1.0, 1.0], [0.5, 0.5], t_cap=1e9)
+    np.testing.assert_allclose(e, [1.0 / 8.0, 1.0 / 8.0], rtol=1e-6)
+    # continuous through v = 0; from the middle, (a / v) tanh(a v), decreasing in |v|
+    e = expected_walk_time([0.0, 1e-7, 1e-3, 0.5, 2.0], [1.5] * 5, [0.5] * 5, t_cap=1e9)
+    assert abs(e[1] - e[0]) < 1e-5 and abs(e[2] - e[0]) < 1e-2 and e[2] > e[3] > e[4]
+    np.testing.assert_allclose(e[3:], 1.5 / np.array([0.5, 2.0]) * np.tanh(1.5 * np.array([0.5, 2.0])), rtol=1e-9)
+    # caps: max_t / deadline, a collapsing angle bound, a Weibull bound
+    assert expected_walk_time([0.0], [3.0], [0.5], t_cap=2.0)[0] == 2.0
+    e = expected_walk_time([0.0, 0.0], [3.0, 3.0], [0.5, 0.5], bound_kind=_lib.BOUND_LINEAR, p1=[-3.0, 0.5],
+                           t_cap=20.0)
+    np.testing.assert_allclose(e, [1.0, 9.0])
+    e = expected_walk_time([0.0], [3.0], [0.5], bound_kind=_lib.BOUND_WEIBULL, p1=[1.0], p2=[0.5], t_cap=20.0)
+    np.testing.assert_allclose(e, [0.5 * np.log(3.0 / 0.05)])
+    assert np.all(np.isfinite(expected_walk_time(np.linspace(-50, 50, 101), [0.01] * 101, [0.999] * 101)))
+
+
+def test_longest_first_order_and_offsets():
+    from ssms_b200.batch import longest_first
+
+    est = np.array([0.5, 3.0, 0.5, 1.0])
+    ns = np.array([10, 0, 7, 4])
+    order, qoff = longest_first(est, ns)
+    assert order.dtype == np.int32 and qoff.dtype == np.int64
+    np.testing.assert_array_equal(order, [1, 3, 0, 2])  # ties keep index order
+    np.testing.assert_array_equal(qoff, [0, 0, 4, 14, 21])
