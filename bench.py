@@ -208,11 +208,11 @@ class ClockSampler:
 
 # ------------------------------------------------------------------ GPU side
 # DRAM bytes (read + write) of one k_single launch on the 4096-theta workload,
-# from one ncu capture of that launch (dram__bytes_read.sum 12,092,928 +
-# dram__bytes_write.sum 286,508,032).
+# from one ncu capture of that launch (dram__bytes_read.sum 21,346,560 +
+# dram__bytes_write.sum 297,097,984).
 # The algorithmic output is 8 B per trajectory (338 MB); part of it is still in
 # L2 when the kernel ends, so the measured writes sit slightly below it.
-K_SINGLE_TRAFFIC_BYTES = 12_092_928 + 286_508_032
+K_SINGLE_TRAFFIC_BYTES = 21_346_560 + 297_097_984
 
 
 def run_ours(args, rank, world, local_rank):
