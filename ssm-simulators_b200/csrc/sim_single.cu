@@ -267,7 +267,8 @@ struct Lane {
     int64_t w;
     uint32_t k, n, blk;
     int ix;           // steps taken (maintained where an integer index is needed)
-    float y, tp, ixf; // position, float32 time accumulator, steps taken as float
+    float y, tp, ixf; // position, float32 time accumulator, steps taken as float (see step_block)
+    float tpb;        // time accumulator at the start of the current block
     float dinc;       // SDV/FULL: this trajectory's drift increment (v + sv g) dt
 };
 
@@ -334,6 +335,13 @@ __device__ __forceinline__ bool step_block(const SingleParams &p, Lane &L, const
         return false;
     }
     constexpr bool INT_IX = NOISE || RECORD || BOUND == SSM_BOUND_TABLE || MODEL == M_DFLEX;
+    // Without an integer index (device RNG, in-register bounds) step q of the
+    // block sits at step ixf0 + q: the step count advances once per block,
+    // the linear bound is a + ixf0 slope dt plus q slope dt, and finalize()
+    // recovers the steps of the last block from the time accumulator.
+    const float ixf0 = L.ixf;
+    const float b0 = (!INT_IX && BOUND == SSM_BOUND_LINEAR) ? fmaf(ixf0, r.dtp1, r.a) : 0.f;
+    if (!INT_IX) L.tpb = L.tp;
     const float *drow = (MODEL == M_DFLEX) ? p.dtable + (int64_t)L.k * p.dstride : nullptr;
     // device RNG: the block's drifts v(t_ix .. t_ix+7) are read before the
     // steps, off the dependency chain (a live walk starts every block at a
@@ -357,7 +365,10 @@ __device__ __forceinline__ bool step_block(const SingleParams &p, Lane &L, const
         if (MODEL == M_LEGACY) {
             inside = live && (L.y <= r.a) && (L.y >= 0.f) && (L.tp <= r.dl_tmp);
         } else {
-            const float b = bound_at<BOUND, NOISE>(r, L.ixf, L.ix, p, L.k);
+            float b;
+            if (INT_IX) b = bound_at<BOUND, NOISE>(r, L.ixf, L.ix, p, L.k);
+            else if (BOUND == SSM_BOUND_LINEAR) b = (q == 0) ? b0 : fmaf((float)q, r.dtp1, b0);
+            else b = bound_at<BOUND, NOISE>(r, ixf0 + (float)q, 0, p, L.k);
             inside = live && (fabsf(L.y) <= b) && (L.tp <= r.dl_tmp);
         }
         if (NOISE && inside && L.ix + (DrawnDrift<MODEL>::value ? 1 : 0) >= p.nlen) {
@@ -387,16 +398,35 @@ __device__ __forceinline__ bool step_block(const SingleParams &p, Lane &L, const
                 else L.y += g[q];
                 L.tp += p.dt;
             }
-            L.ixf += 1.0f;
-            if (INT_IX) L.ix += 1;
+            if (INT_IX) {
+                L.ixf += 1.0f;
+                L.ix += 1;
+            }
             if (RECORD && L.ix < p.traj_len) p.traj[L.ix] = L.y;
         }
         live = inside;
     }
+    if (!INT_IX) L.ixf = ixf0 + (float)BLK;
     return live;
 }
 
-template <int MODEL, bool NOISE>
+// Steps taken by a walk that has ended.  Without an integer index L.ixf
+// counts whole blocks; the steps of the last block are those that took the
+// time accumulator from L.tpb to L.tp (the same float additions replayed).
+template <int MODEL, int BOUND, bool NOISE>
+__device__ __forceinline__ int steps_taken(const SingleParams &p, const Lane &L) {
+    constexpr bool INT_IX = NOISE || BOUND == SSM_BOUND_TABLE || MODEL == M_DFLEX;
+    if (INT_IX) return (int)L.ixf;
+    float tt = L.tpb;
+    int c = 0;
+    while (c < BLK && tt != L.tp) {
+        tt += p.dt;
+        ++c;
+    }
+    return (int)L.ixf - BLK + c;
+}
+
+template <int MODEL, int BOUND, bool NOISE>
 __device__ __forceinline__ void finalize(const SingleParams &p, const Lane &L) {
     // fields needed only here are re-read instead of being held across the walk
     const TrialRow *row = p.rows + L.k;
@@ -423,7 +453,7 @@ __device__ __forceinline__ void finalize(const SingleParams &p, const Lane &L) {
     const int choice = (L.y > 0.f) - (L.y < 0.f);         // sign(y)
     p.rts[L.w] = rt;
     p.choices[L.w] = choice;
-    if (p.steps) p.steps[L.w] = (int)L.ixf;
+    if (p.steps) p.steps[L.w] = steps_taken<MODEL, BOUND, NOISE>(p, L);
 }
 
 // Start lane L on the trajectory with queue index w; false (and the error
@@ -494,7 +524,7 @@ __global__ void __launch_bounds__(256, SSM_MIN_CTAS) k_single(const __grid_const
 
     Lane L;
     TrialRow r;
-    L.w = 0; L.k = L.n = L.blk = 0; L.ix = 0; L.y = L.tp = L.ixf = L.dinc = 0.f;
+    L.w = 0; L.k = L.n = L.blk = 0; L.ix = 0; L.y = L.tp = L.ixf = L.dinc = L.tpb = 0.f;
     bool active = false;
     bool pending = false;  // walk ended, result not yet written
     bool exhausted = false;
@@ -508,7 +538,7 @@ __global__ void __launch_bounds__(256, SSM_MIN_CTAS) k_single(const __grid_const
         const unsigned need = __ballot_sync(FULL, !active);
         const bool pass = exhausted ? (__ballot_sync(FULL, pending) != 0u) : (__popc(need) >= p.refill_min);
         if (pass && pending) {
-            finalize<MODEL, NOISE>(p, L);
+            finalize<MODEL, BOUND, NOISE>(p, L);
             pending = false;
         }
         if (pass && !exhausted) {

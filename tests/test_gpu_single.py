@@ -160,6 +160,37 @@ def test_noise_rows_too_short_is_reported(cuda):
         _gpu("ddm_flexbound", th, 4, 1, spec, rows=rows, unif=f32([0.5] * 4))
 
 
+@pytest.mark.parametrize("model,bname", [("ddm_flexbound", "constant"), ("ddm_flexbound", "angle"),
+                                         ("ddm_flexbound", "weibull"), ("ddm", "constant"),
+                                         ("levy_flexbound", "angle")])
+def test_device_rng_step_counts_match_the_time_accumulator(cuda, model, bname):
+    """Without smoothing, rt = tp + t where tp is dt added `steps` times in
+    float32: the step counts the device path reports (counted per block,
+    the last block's steps recovered from the time accumulator) agree with
+    the rts it writes, for walks ending at every position in a block."""
+    rng = np.random.default_rng(41)
+    K, N, dt = 24, 3000, 0.001
+    th = _theta(rng, K)
+    th["alpha"] = f32(rng.uniform(1.0, 2.0, K))
+    th["beta"] = f32(rng.uniform(0.5, 7, K))
+    t_s = bf.make_t_s(3.0, dt)
+    if bname == "weibull":
+        spec = bf.kernel_spec(bf.weibull_cdf, {"a": th["a"], "alpha": th["alpha"], "beta": th["beta"]}, K, t_s)
+    elif bname == "angle":
+        spec = bf.kernel_spec(bf.angle, {"a": th["a"], "theta": th["theta"]}, K, t_s)
+    else:
+        spec = bf.kernel_spec(bf.constant, {"a": th["a"]}, K, t_s)
+    rts, chs, steps, _ = _gpu(model, th, N, K, spec, smooth=False, max_t=3.0, dt=dt, seed=12,
+                              alpha=th["alpha"] if model == "levy_flexbound" else None)
+    tp = np.zeros(int(steps.max()) + 1, np.float32)
+    for i in range(1, tp.shape[0]):
+        tp[i] = tp[i - 1] + np.float32(dt)
+    t = np.tile(th["t"], N)
+    ok = rts != -999.0
+    assert ok.mean() > 0.5 and len(np.unique(steps % 8)) == 8
+    np.testing.assert_array_equal(rts[ok], (tp[steps] + t)[ok])
+
+
 def test_results_do_not_depend_on_launch_shape(cuda):
     rng = np.random.default_rng(3)
     K, N = 16, 500
