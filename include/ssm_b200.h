@@ -61,8 +61,8 @@ typedef struct ssm_launch {
      * sample_offsets (whose values stay global output indices) -- gives the
      * same outputs as one call over the whole batch. */
     int64_t first_trial;
-    /* Processing order of the trials (single-accumulator simulators, ragged
-     * layout only; NULL = index order): trial_order[j] is the trial simulated
+    /* Processing order of the trials (every Euler simulator; ragged layout
+     * only; NULL = index order): trial_order[j] is the trial simulated
      * j-th and order_offsets[0..n_trials] the prefix sums of the sample
      * counts in that order (order_offsets[0] = 0).  Outputs and random
      * streams do not depend on the order; starting the longest walks first

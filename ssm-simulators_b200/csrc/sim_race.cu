@@ -42,6 +42,8 @@ struct RaceParams {
     const float *rows;
     int64_t row_floats;
     const int64_t *offsets;
+    const int32_t *order;     // ragged only: trial simulated j-th (nullptr = index order)
+    const int64_t *qoff;      // prefix sums of the sample counts in that order
     int64_t n_trials, total;  // total -1: offsets[n_trials] - offsets[0]
     uint32_t k_base;          // random-stream index of trial 0 (trial windows of a larger batch)
     int np;
@@ -296,12 +298,24 @@ __device__ __forceinline__ int64_t race_find(const int64_t *off, int64_t K, int6
 }
 
 template <int NP, int FAM, bool NOISE>
-__device__ __forceinline__ void race_init(const RaceParams &p, RaceLane<NP> &L, RaceHead &h,
+__device__ __forceinline__ bool race_init(const RaceParams &p, RaceLane<NP> &L, RaceHead &h,
                                           int64_t w, int64_t &hint, int np) {
     int64_t k, n;
     if (p.offsets == nullptr) {
         k = w % p.n_trials;
         n = w / p.n_trials;
+    } else if (p.order != nullptr) {
+        // queue index -> position j in the processing order -> trial k (outputs
+        // stay at offsets[k] + n); an entry that does not fit is reported
+        const int64_t j = race_find(p.qoff, p.n_trials, w, hint);
+        hint = j;
+        k = __ldg(p.order + j);
+        n = w - __ldg(p.qoff + j);
+        if (k < 0 || k >= p.n_trials || n < 0 || n >= __ldg(p.offsets + k + 1) - __ldg(p.offsets + k)) {
+            raise_error(p.hdr, SSM_ERR_ARG, (int)j);
+            return false;
+        }
+        w = __ldg(p.offsets + k) + n;
     } else {
         w += __ldg(p.offsets);  // global output index (trial windows start past 0)
         k = race_find(p.offsets, p.n_trials, w, hint);
@@ -342,6 +356,7 @@ __device__ __forceinline__ void race_init(const RaceParams &p, RaceLane<NP> &L, 
     L.ixf = 0.f;
     L.tp = 0.f;
     L.tpd = 0.0;
+    return true;
 }
 
 template <int NP, int FAM, int BOUND, bool NOISE>
@@ -382,8 +397,7 @@ __global__ void __launch_bounds__(256) k_race(const __grid_constant__ RaceParams
             if (!active) {
                 const int rank = __popc(need & lt_mask);
                 const int64_t w = (rank < avail) ? q_next + rank : base + (rank - avail);
-                if (w < total) {
-                    race_init<NP, FAM, NOISE>(p, L, h, w, hint, np);
+                if (w < total && race_init<NP, FAM, NOISE>(p, L, h, w, hint, np)) {
                     ctr = 0;
                     active = true;
                 }
@@ -455,7 +469,10 @@ static int race_launch(const RaceParams &p, const ssm_launch *opt, cudaStream_t 
     kern<<<sm_count() * per_sm, threads, 0, st>>>(p);
     SSM_CUDA(cudaGetLastError());
     if (p.traj && p.traj_len > 0) {
-        k_race_record<NP, FAM, BOUND, NOISE><<<1, 128, 0, st>>>(p);
+        RaceParams pr = p;  // trial 0 / sample 0, whatever the processing order
+        pr.order = nullptr;
+        pr.qoff = nullptr;
+        k_race_record<NP, FAM, BOUND, NOISE><<<1, 128, 0, st>>>(pr);
         SSM_CUDA(cudaGetLastError());
     }
     return SSM_OK;
@@ -517,8 +534,9 @@ static int run_race(int fam, const float *v, const float *z, const float *t, con
                 "max_t must be finite with max_t / delta_t <= 2^23");
     SSM_REQUIRE(n_trials == 0 || (v && z && t && s && deadline), "v, z, t, s, deadline are required");
     SSM_REQUIRE(fam != FAM_LCA || n_trials == 0 || (g && b), "lca needs g and b");
-    SSM_REQUIRE(!launch || (!launch->trial_order && !launch->order_offsets),
-                "a trial order is supported by the single-accumulator simulators only");
+    SSM_REQUIRE(!launch || (!launch->trial_order == !launch->order_offsets),
+                "trial_order and order_offsets go together");
+    SSM_REQUIRE(!launch || !launch->trial_order || offsets, "a trial order needs the ragged layout (sample_offsets)");
     SSM_REQUIRE((rts && choices) || (!offsets && n_trials * n_samples == 0), "rts and choices outputs are required");
     SSM_REQUIRE(bound >= SSM_BOUND_TABLE && bound <= SSM_BOUND_WEIBULL, "unknown boundary kind %d", bound);
     SSM_REQUIRE(bound == SSM_BOUND_TABLE || n_trials == 0 || a, "boundary height a is required");
@@ -549,6 +567,8 @@ static int run_race(int fam, const float *v, const float *z, const float *t, con
     RaceParams p;
     p.key = philox_keys(seed);
     p.rows = rows; p.row_floats = race_row_floats(np); p.offsets = offsets;
+    p.order = (offsets && launch) ? launch->trial_order : nullptr;
+    p.qoff = p.order ? launch->order_offsets : nullptr;
     p.n_trials = n_trials; p.total = total; p.np = np; p.dt = dt; p.smooth = smooth ? 1 : 0;
     p.k_base = (uint32_t)((launch && launch->first_trial > 0) ? launch->first_trial : 0);
     p.chunk = (launch && launch->chunk >= 32) ? launch->chunk : 64;

@@ -73,6 +73,28 @@ def expected_walk_time(v, a, z, s=1.0, *, legacy: bool = False, bound_kind: int 
     return np.minimum(e, cap)
 
 
+def expected_race_time(v, dist, s=1.0, *, bound_kind: int = _lib.BOUND_CONSTANT, a=None, p1=None,
+                       t_cap=20.0) -> np.ndarray:
+    """Per-trial estimate of a race's duration, used only to order work:
+    the shortest of the accumulators' times to cover ``dist`` (threshold
+    minus start) at drift v and noise s, each dist^2 / (s^2 + dist max(v, 0))
+    (dist / v for strong drift, dist^2 / s^2 for none), capped by a
+    collapsing linear bound (a / -p1) and t_cap."""
+    v = np.asarray(v, np.float64)
+    K = v.shape[0]
+    v = v.reshape(K, -1)
+    d = np.maximum(np.broadcast_to(np.asarray(dist, np.float64).reshape(K, -1), v.shape), 0.0)
+    s2 = np.broadcast_to(np.asarray(s, np.float64).reshape(K, -1) if np.ndim(s) else np.float64(s), v.shape) ** 2
+    e = (d * d / np.maximum(s2 + d * np.maximum(v, 0.0), 1e-12)).min(axis=1)
+    cap = np.broadcast_to(np.asarray(t_cap, np.float64).reshape(-1), (K,)).copy()
+    if bound_kind == _lib.BOUND_LINEAR and p1 is not None and a is not None:
+        slope = np.broadcast_to(np.asarray(p1, np.float64).reshape(-1), (K,))
+        av = np.broadcast_to(np.asarray(a, np.float64).reshape(-1), (K,))
+        with np.errstate(divide="ignore"):
+            cap = np.minimum(cap, np.where(slope < 0, av / np.maximum(-slope, 1e-12), np.inf))
+    return np.minimum(e, cap)
+
+
 def longest_first(expected_time, n_samples) -> tuple[np.ndarray, np.ndarray]:
     """(trial_order int32, order_offsets int64): trials by decreasing expected
     walk time (ties in index order) and the prefix sums of their sample counts

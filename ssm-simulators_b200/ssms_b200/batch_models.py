@@ -18,7 +18,7 @@ from . import _device as D
 from . import boundary_functions as bf
 from . import device as dev
 from . import drift_functions as dfn
-from .batch import expected_walk_time, longest_first, with_order
+from .batch import expected_race_time, expected_walk_time, longest_first, with_order
 from .tuning import launch_for
 
 SINGLE = ("ddm_flexbound", "levy_flexbound", "ddm", "full_ddm", "ddm_sdv", "ornstein_uhlenbeck", "ddm_flex")
@@ -53,6 +53,7 @@ class SetBatch:
         self.offsets_host = np.concatenate([[0], np.cumsum(ns)]).astype(np.int64)
         self.total = int(self.offsets_host[-1])
         self.offsets = torch.from_numpy(self.offsets_host).cuda()
+        self.order_t = self.qoff_t = None  # trials longest-first (outputs do not depend on the order)
         self.sim_name, self.K = sim_name, K
         self.n_samples = int(n_samples)
         self.max_t, self.delta_t, self.smooth = float(max_t), float(delta_t), bool(smooth_unif)
@@ -72,8 +73,6 @@ class SetBatch:
             self.deadline, self.s = _dev(_col(kwargs["deadline"], K), K), _dev(_col(kwargs["s"], K), K)
             self.alpha = _dev(_col(kwargs["alpha"], K), K) if sim_name == "levy_flexbound" else None
             self.extra = {k: _dev(_col(kwargs[k], K), K, k) for k in _PER_TRIAL.get(sim_name, ())}
-            # trials longest-first (outputs do not depend on the order)
-            self.order_t = self.qoff_t = None
             if K > 1:
                 cap = np.minimum(self.max_t, np.maximum(np.asarray(_col(kwargs["deadline"], K), np.float64)
                                                         - np.asarray(_col(kwargs["t"], K), np.float64), 0.0))
@@ -97,6 +96,11 @@ class SetBatch:
             self.g = _dev(_col(kwargs["g"], K), K) if lca else None
             self.b = _dev(_col(kwargs["b"], K), K) if lca else None
             self.v_shape = v.shape
+            a0 = np.asarray(spec["a"], np.float64).reshape(K, 1)  # start z_j b(0), threshold b(t)
+            est = expected_race_time(v, a0 * (1.0 - np.asarray(kwargs["z"], np.float64).reshape(K, -1)),
+                                     np.asarray(kwargs["s"], np.float32), bound_kind=self.kind, a=spec["a"],
+                                     p1=spec["p1"], t_cap=self._cap(kwargs, K))
+            self._set_order(est, ns)
         elif sim_name == "racing_diffusion_model":
             v = np.asarray(kwargs["v"], np.float32)
             self.n_acc = int(v.shape[1])
@@ -104,6 +108,10 @@ class SetBatch:
             self.v = _dev(v)
             self.b, self.A, self.t, self.s = (_dev(_col(kwargs[k], K), K, k) for k in ("b", "A", "t", "s"))
             self.deadline = _dev(_col(kwargs["deadline"], K), K)
+            dist = (np.asarray(_col(kwargs["b"], K), np.float64) - 0.5 * np.asarray(_col(kwargs["A"], K), np.float64))
+            est = expected_race_time(v, dist.reshape(K, 1), _col(kwargs["s"], K).reshape(K, 1),
+                                     t_cap=self._cap(kwargs, K))
+            self._set_order(est, ns)
         elif sim_name == "lba_vanilla":
             v = np.asarray(kwargs["v"], np.float32)
             sd = np.asarray(kwargs["sd"], np.float32).reshape(K, -1)
@@ -117,13 +125,24 @@ class SetBatch:
         else:
             raise ValueError(f"no batched device path for simulator {sim_name!r}")
 
+    def _cap(self, kwargs, K):
+        """min(max_t, deadline - t) per trial: no walk lasts longer."""
+        return np.minimum(self.max_t, np.maximum(np.asarray(_col(kwargs["deadline"], K), np.float64)
+                                                 - np.asarray(_col(kwargs["t"], K), np.float64), 0.0))
+
+    def _set_order(self, est, ns):
+        if self.K > 1:
+            o, q = longest_first(est, ns)
+            self.order_t, self.qoff_t = torch.from_numpy(o).cuda(), torch.from_numpy(q).cuda()
+
     def run(self, seed: int, want_steps: bool = False, launch=None) -> dev.SimOutput:
         K, total = self.K, self.total
-        if self.sim_name in SINGLE:
+        if self.sim_name != "lba_vanilla":
             if launch is None:
                 launch = launch_for(self.sim_name)
             if self.order_t is not None and not launch.trial_order:
                 launch = with_order(launch, self.order_t, self.qoff_t)
+        if self.sim_name in SINGLE:
             rts = torch.empty(total, dtype=torch.float32, device="cuda")
             chs = torch.empty(total, dtype=torch.int32, device="cuda")
             return dev.simulate_single(

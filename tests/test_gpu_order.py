@@ -1,7 +1,8 @@
 """Trial processing order (ssm_launch.trial_order / order_offsets): outputs,
-random streams and step counts do not depend on the order the trials are
-simulated in; a malformed order is reported in the device error word and
-skips only the trajectories it cannot place."""
+random streams and step counts of the single-accumulator and race kernels do
+not depend on the order the trials are simulated in; a malformed order is
+reported in the device error word and skips only the trajectories it cannot
+place."""
 
 import numpy as np
 import pytest
@@ -82,7 +83,30 @@ def test_malformed_order_sets_the_error_word(cuda):
     assert b"code 1 (detail 3)" in lib.ssm_last_error()  # SSM_ERR_ARG at order position 3
 
 
-def test_order_needs_the_ragged_layout_and_a_single_accumulator_model(cuda):
+@pytest.mark.parametrize("model", ["race_no_bias_angle_3", "lca_no_bias_3", "racing_diffusion_3"])
+def test_race_family_orders_give_the_index_order_results(cuda, model):
+    from ssms_b200 import Simulator, model_config
+    from ssms_b200.batch_models import SetBatch
+
+    rng = np.random.default_rng(17)
+    K = 97
+    lo, hi = (np.asarray(b, np.float64) for b in model_config[model]["param_bounds"])
+    theta = {p: rng.uniform(lo[j], hi[j], K).astype(np.float32) for j, p in enumerate(model_config[model]["params"])}
+    prep = Simulator(model).prepare(theta, n_samples=600, random_state=1)
+    sb = SetBatch(prep["config"]["simulator"].__name__, prep["theta"], prep["boundary"], 600, max_t=20.0,
+                  delta_t=0.001)
+    assert sb.order_t is not None
+    ident = torch.arange(K, dtype=torch.int32, device="cuda")
+    outs = []
+    for lo_ in (with_order(D.launch_opts(), ident, sb.offsets), None):
+        o = sb.run(23, want_steps=True, launch=lo_)
+        assert _lib.lib().ssm_check_status(D.ptr(o.workspace), D.stream_ptr()) == _lib.SSM_OK
+        outs.append((o.rts.view(torch.int32).cpu().numpy(), o.choices.cpu().numpy(), o.steps.cpu().numpy()))
+    for a, b in zip(*outs):
+        np.testing.assert_array_equal(a, b)
+
+
+def test_order_needs_the_ragged_layout(cuda):
     K = 4
     ot = torch.arange(K, dtype=torch.int32, device="cuda")
     qt = torch.arange(0, (K + 1) * 10, 10, dtype=torch.int64, device="cuda")
@@ -96,7 +120,7 @@ def test_order_needs_the_ragged_layout_and_a_single_accumulator_model(cuda):
     with pytest.raises(ValueError, match="together"):
         _single(th, K, np.full(K, 10), half)
     v = f32(np.ones((K, 2)))
-    with pytest.raises(ValueError, match="single-accumulator"):
+    with pytest.raises(ValueError, match="ragged"):
         dev.simulate_race("race_model", v=v, z=f32(np.full((K, 2), 0.3)), t=th["t"], s=f32(np.ones((K, 2))),
                           deadline=f32([999] * K), n_trials=K, n_samples=10, a=th["a"],
                           bound_kind=_lib.BOUND_CONSTANT, seed=1, launch=lo)

@@ -150,3 +150,19 @@ def test_longest_first_order_and_offsets():
     assert order.dtype == np.int32 and qoff.dtype == np.int64
     np.testing.assert_array_equal(order, [1, 3, 0, 2])  # ties keep index order
     np.testing.assert_array_equal(qoff, [0, 0, 4, 14, 21])
+
+
+def test_expected_race_time_limits():
+    from ssms_b200 import _lib
+    from ssms_b200.batch import expected_race_time
+
+    # one accumulator: dist / v for strong drift, dist^2 / s^2 without drift
+    np.testing.assert_allclose(expected_race_time([[50.0]], [[2.0]], 1.0), [4.0 / (1 + 100)])
+    np.testing.assert_allclose(expected_race_time([[0.0]], [[2.0]], [[2.0]]), [1.0])
+    # the fastest accumulator decides; negative drifts count as none
+    e = expected_race_time([[0.5, 3.0, -1.0]], [[1.0, 1.0, 1.0]], 1.0, t_cap=1e9)
+    np.testing.assert_allclose(e, [1.0 / (1.0 + 3.0)])
+    # caps
+    assert expected_race_time([[0.0]], [[10.0]], 1.0, t_cap=5.0)[0] == 5.0
+    e = expected_race_time([[0.0]], [[10.0]], 1.0, bound_kind=_lib.BOUND_LINEAR, a=[2.0], p1=[-4.0], t_cap=20.0)
+    np.testing.assert_allclose(e, [0.5])
