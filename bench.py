@@ -215,6 +215,26 @@ class ClockSampler:
 K_SINGLE_TRAFFIC_BYTES = 21_346_560 + 297_097_984
 
 
+def max_over_ranks(x: float, world: int) -> float:
+    """The largest value of x over the ranks (device time of the slowest
+    replica); x itself on one rank."""
+    if world <= 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    tt = torch.tensor([float(x)], device=dev, dtype=torch.float64)
+    dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    return float(tt.item())
+
+
+def replica_value(trajectories_per_rank: int, world: int, steps: int, t_ms: float) -> float:
+    """Whole-job trajectories/s: every rank simulates its own replica of the
+    workload, timed by the slowest rank."""
+    return world * trajectories_per_rank * steps / (t_ms / 1e3)
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
 
@@ -253,13 +273,9 @@ def run_ours(args, rank, world, local_rank):
             ms.append(e0.elapsed_time(e1))
     torch.cuda.synchronize()
     dist_barrier()
-    t_sum = sum(ms)
-    if world > 1:
-        tt = torch.tensor([t_sum], device="cuda", dtype=torch.float64)
-        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
-        t_sum = float(tt.item())
+    t_sum = max_over_ranks(sum(ms), world)
     ms_per_step = t_sum / args.steps
-    value = world * total * args.steps / (t_sum / 1e3)
+    value = replica_value(total, world, args.steps, t_sum)
 
     # end to end: pinned host theta -> device, graph replay, rts+choices -> pinned host
     host_theta = {k: torch.from_numpy(np.ascontiguousarray(theta[k])).pin_memory()
@@ -283,12 +299,8 @@ def run_ours(args, rank, world, local_rank):
         torch.cuda.synchronize()
         if i >= args.warmup:
             e2e_ms.append((time.perf_counter() - t0) * 1e3)
-    e2e_t = sum(e2e_ms)
-    if world > 1:
-        tt = torch.tensor([e2e_t], device="cuda", dtype=torch.float64)
-        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
-        e2e_t = float(tt.item())
-    e2e_value = world * total * args.steps / (e2e_t / 1e3)
+    e2e_t = max_over_ranks(sum(e2e_ms), world)
+    e2e_value = replica_value(total, world, args.steps, e2e_t)
 
     clocks = clk.summary()
     f_max = (clocks.get("sm_max_mhz") or 1965.0) * 1e6
