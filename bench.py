@@ -42,11 +42,14 @@ METRIC = "trajectories/s"
 WORKLOAD = ("ddm_flexbound angle boundary, 4096 theta ~ U(v[-3,3], a[0.3,3], z[0.1,0.9], "
             "t[0.001,2], theta[-0.1,1.3]), n_samples ~ U{1000..20000} per theta, dt=1e-3, max_t=20, "
             "one persistent graph-captured launch")
-# Issue-slot roofline of the Euler step: the minimum warp-instruction count per
-# accumulator-step of the algorithm (Philox4x32-10 = 60 instructions per 4
-# normals -> 15; Box-Muller ~6.5 per normal incl. 2 SFU ops; update, boundary
-# and exit test ~6.5) -> 28 lane-instructions per accumulator-step.
-INSTR_PER_STEP = 28.0
+# Issue-slot roofline of the Euler step: the minimum lane-instruction count per
+# accumulator-step of the algorithm, with no block, queue or per-walk overhead.
+# Philox4x32-10: 10 rounds x (2 wide multiplies + 2 three-input XORs) + the
+# counter = 42 instructions per 4 normals -> 10.5; Box-Muller: 12 per pair
+# (two bit-to-float conversions, log2, scale, sqrt, sin, cos, range scale,
+# two fused multiply-adds) -> 6; the step: bound, two compares, predicate,
+# position and time updates -> 5.5.  Total 22 lane-instructions.
+INSTR_PER_STEP = 22.0
 E2E_WINDOWS = 5
 N_SM = 148
 LANES_PER_SM_CLK = 128
@@ -208,11 +211,11 @@ class ClockSampler:
 
 # ------------------------------------------------------------------ GPU side
 # DRAM bytes (read + write) of one k_single launch on the 4096-theta workload,
-# from one ncu capture of that launch (dram__bytes_read.sum 21,346,560 +
-# dram__bytes_write.sum 297,097,984).
+# from one ncu capture of that launch (dram__bytes_read.sum 12,520,960 +
+# dram__bytes_write.sum 289,847,552).
 # The algorithmic output is 8 B per trajectory (338 MB); part of it is still in
 # L2 when the kernel ends, so the measured writes sit slightly below it.
-K_SINGLE_TRAFFIC_BYTES = 21_346_560 + 297_097_984
+K_SINGLE_TRAFFIC_BYTES = 12_520_960 + 289_847_552
 
 
 def max_over_ranks(x: float, world: int) -> float:

@@ -12,10 +12,10 @@
 //    hands them the next trajectories of its chunk (popc rank) in one
 //    divergent pass, so that pass is paid once per several trajectories and
 //    an ended lane idles for a few blocks at most.
-//  * Steps run in blocks of sixteen (eight for ddm_flex and Levy): four independent
-//    Philox4x32-10 calls yield sixteen 32-bit words = eight Box-Muller pairs =
-//    the block's increments, already scaled to drift + s sqrt(dt) N(0,1); the
-//    steps themselves are predicated (no per-step branch).
+//  * Steps run in blocks of 32 (8 for ddm_flex and Levy): eight independent
+//    Philox4x32-10 calls yield 32 words = 16 Box-Muller pairs = the block's
+//    increments, already scaled to drift + s sqrt(dt) N(0,1); the steps
+//    themselves are predicated (no per-step branch).
 //  * Boundaries are evaluated in registers (constant / linear collapse /
 //    Weibull) or read from a caller-evaluated table for arbitrary shapes.
 //  * Noise injection replaces the generator by caller rows and switches every
@@ -26,10 +26,6 @@
 #include "common.cuh"
 
 
-// Resident CTAs per SM the compiler must fit (register cap 65536 / (256 * n)).
-#ifndef SSM_MIN_CTAS
-#define SSM_MIN_CTAS 4
-#endif
 
 
 namespace ssm {
@@ -261,16 +257,21 @@ __device__ __forceinline__ float cms_stable(uint32_t bu, uint32_t bw, const Tria
 }
 
 // Euler steps per block.  One Philox4x32-10 call gives four words = two
-// Box-Muller pairs = four increments, so a 16-step block makes four
-// independent Philox calls whose latencies overlap (11 % faster than 8-step
-// blocks on the angle batch at 64 registers).  ddm_flex keeps 8-step blocks,
-// whose eight drift values per block fit in registers, and the Levy model,
-// whose stable draws already give each block enough independent work (16-step
-// blocks measured 8 % slower there).  The Gaussian counter of call h of block
-// b is (BLK/4) b + h, so those streams do not depend on the block size.
+// Box-Muller pairs = four increments, so a 32-step block makes eight
+// independent Philox calls whose latencies overlap.  Measured on the 4096-set
+// angle batch (ms per launch): 8 steps 37.9, 16 steps 34.5 (64 registers, 4
+// CTAs per SM), 32 steps 32.9 (80 registers, 3 CTAs per SM), 40 steps 32.9,
+// 64 steps 33.5 (128 registers, 2 CTAs).  ddm_flex keeps 8-step blocks, whose
+// eight drift values per block fit in registers, and the Levy model, whose
+// stable draws already give each block enough independent work (16-step blocks
+// measured 8 % slower there).  The Gaussian counter of call h of block b is
+// (BLK/4) b + h, so those streams do not depend on the block size.
 template <int MODEL> struct Blk {
-    static constexpr int value = (MODEL == M_DFLEX || MODEL == M_LEVY) ? 8 : 16;
+    static constexpr int value = (MODEL == M_DFLEX || MODEL == M_LEVY) ? 8 : 32;
 };
+// Resident 256-thread CTAs per SM the compiler must fit (register cap
+// 65536 / (256 n)): 3 (80 registers) for the 32-step blocks, 4 otherwise.
+template <int MODEL> struct MinCtas { static constexpr int value = Blk<MODEL>::value > 16 ? 3 : 4; };
 
 struct Lane {
     int64_t w;
@@ -531,7 +532,7 @@ __device__ __forceinline__ bool lane_init(const SingleParams &p, Lane &L, TrialR
 
 // ------------------------------------------------------------------ main kernel
 template <int MODEL, int BOUND, bool NOISE>
-__global__ void __launch_bounds__(256, SSM_MIN_CTAS) k_single(const __grid_constant__ SingleParams p) {
+__global__ void __launch_bounds__(256, MinCtas<MODEL>::value) k_single(const __grid_constant__ SingleParams p) {
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const unsigned lt_mask = (1u << lane) - 1u;
