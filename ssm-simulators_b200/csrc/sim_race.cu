@@ -126,6 +126,9 @@ __device__ __forceinline__ float2 std_normal_pair(uint32_t a, uint32_t b) {
     return box_muller(a, b);
 }
 
+// Steps whose normals a lane draws ahead (models with at most 4 accumulators).
+constexpr int RACE_PRE = 4;
+
 template <int NP>
 struct RaceLane {
     int64_t w;
@@ -138,10 +141,12 @@ struct RaceLane {
 };
 
 // One Euler step of every accumulator.  Returns false when the loop condition
-// failed before the step (the walk is over).
-template <int NP, int FAM, int BOUND, bool NOISE, bool RECORD>
+// failed before the step (the walk is over).  With PRE the step's normals come
+// from `pre` (drawn ahead from the same counters); ctr still counts the steps.
+template <int NP, int FAM, int BOUND, bool NOISE, bool RECORD, bool PRE = false>
 __device__ __forceinline__ bool race_step(const RaceParams &p, RaceLane<NP> &L, const RaceHead &h,
-                                          const float *v, const float *sq, int np, uint32_t &ctr) {
+                                          const float *v, const float *sq, int np, uint32_t &ctr,
+                                          const float *pre = nullptr) {
     if (L.ixf >= h.capf) {
         raise_error(p.hdr, SSM_ERR_DEVICE, (int)L.w);
         return false;
@@ -166,6 +171,10 @@ __device__ __forceinline__ bool race_step(const RaceParams &p, RaceLane<NP> &L, 
         const float *row = p.noise + L.w * p.nlen + base;
 #pragma unroll
         for (int j = 0; j < NP; ++j) gsn[j] = (j < np) ? __ldg(row + j) : 0.f;
+    } else if (PRE) {
+#pragma unroll
+        for (int j = 0; j < NP; ++j) gsn[j] = pre[j];
+        ctr += 1;
     } else {
 #pragma unroll
         for (int j0 = 0; j0 < NP; j0 += 4) {
@@ -421,9 +430,28 @@ __global__ void __launch_bounds__(256) k_race(const __grid_constant__ RaceParams
                 sr[j] = (j < np) ? __ldg(sq + j) : 0.f;
             }
             bool live = true;
+            if (!NOISE && NP <= 4) {
+                // the next RACE_PRE steps' normals first: independent Philox
+                // calls whose latencies overlap (counters ctr .. ctr + RACE_PRE - 1,
+                // one call per step, as the steps themselves would draw them)
+                float pre[RACE_PRE][NP];
+#pragma unroll
+                for (int s = 0; s < RACE_PRE; ++s) {
+                    const uint4 r = philox10(make_uint4(ctr + (uint32_t)s, L.n, L.k + p.k_base, 0u), p.key);
+                    const float2 a = std_normal_pair(r.x, r.y);
+                    const float2 b = std_normal_pair(r.z, r.w);
+                    const float four[4] = {a.x, a.y, b.x, b.y};
+#pragma unroll
+                    for (int j = 0; j < NP; ++j) pre[s][j] = four[j];
+                }
+#pragma unroll
+                for (int s = 0; s < RACE_PRE; ++s)
+                    if (live) live = race_step<NP, FAM, BOUND, NOISE, false, true>(p, L, h, vr, sr, np, ctr, pre[s]);
+            } else {
 #pragma unroll 1
-            for (int s = 0; s < 4 && live; ++s)
-                live = race_step<NP, FAM, BOUND, NOISE, false>(p, L, h, vr, sr, np, ctr);
+                for (int s = 0; s < 4 && live; ++s)
+                    live = race_step<NP, FAM, BOUND, NOISE, false>(p, L, h, vr, sr, np, ctr);
+            }
             if (!live) {
                 active = false;
                 pending = true;
