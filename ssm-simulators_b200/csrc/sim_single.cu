@@ -12,7 +12,7 @@
 //    hands them the next trajectories of its chunk (popc rank) in one
 //    divergent pass, so that pass is paid once per several trajectories and
 //    an ended lane idles for a few blocks at most.
-//  * Steps run in blocks of 32 (8 for ddm_flex and Levy): eight independent
+//  * Steps run in blocks of 32 (16 for ddm_flex, 8 for Levy): eight independent
 //    Philox4x32-10 calls yield 32 words = 16 Box-Muller pairs = the block's
 //    increments, already scaled to drift + s sqrt(dt) N(0,1); the steps
 //    themselves are predicated (no per-step branch).
@@ -261,17 +261,18 @@ __device__ __forceinline__ float cms_stable(uint32_t bu, uint32_t bw, const Tria
 // independent Philox calls whose latencies overlap.  Measured on the 4096-set
 // angle batch (ms per launch): 8 steps 37.9, 16 steps 34.5 (64 registers, 4
 // CTAs per SM), 32 steps 32.9 (80 registers, 3 CTAs per SM), 40 steps 32.9,
-// 64 steps 33.5 (128 registers, 2 CTAs).  ddm_flex keeps 8-step blocks, whose
-// eight drift values per block fit in registers, and the Levy model, whose
-// stable draws already give each block enough independent work (16-step blocks
-// measured 8 % slower there).  The Gaussian counter of call h of block b is
-// (BLK/4) b + h, so those streams do not depend on the block size.
+// 64 steps 33.5 (128 registers, 2 CTAs).  ddm_flex uses 16-step blocks (its
+// per-block drift values take registers too; 20.4 -> 18.4 ms against 8-step
+// blocks on the conflict_ds sets), and the Levy model 8-step blocks (its
+// stable draws already give each block enough independent work; 16-step
+// blocks measured 8 % slower there).  The Gaussian counter of call h of block
+// b is (BLK/4) b + h, so those streams do not depend on the block size.
 template <int MODEL> struct Blk {
-    static constexpr int value = (MODEL == M_DFLEX || MODEL == M_LEVY) ? 8 : 32;
+    static constexpr int value = (MODEL == M_LEVY) ? 8 : (MODEL == M_DFLEX ? 16 : 32);
 };
 // Resident 256-thread CTAs per SM the compiler must fit (register cap
-// 65536 / (256 n)): 3 (80 registers) for the 32-step blocks, 4 otherwise.
-template <int MODEL> struct MinCtas { static constexpr int value = Blk<MODEL>::value > 16 ? 3 : 4; };
+// 65536 / (256 n)): 3 (80 registers) for blocks longer than 8 steps, 4 otherwise.
+template <int MODEL> struct MinCtas { static constexpr int value = Blk<MODEL>::value > 8 ? 3 : 4; };
 
 struct Lane {
     int64_t w;
