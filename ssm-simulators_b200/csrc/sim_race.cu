@@ -376,6 +376,7 @@ __global__ void __launch_bounds__(256) k_race(const __grid_constant__ RaceParams
     const int lane = threadIdx.x & 31;
     const unsigned lt_mask = (1u << lane) - 1u;
     const int64_t total = (p.total >= 0) ? p.total : __ldg(p.offsets + p.n_trials) - __ldg(p.offsets);
+    const int64_t chunk = warp_chunk(p.chunk, total);
     const int np = (NP == RACE_MAX_NP) ? p.np : NP;
     RaceLane<NP> L;
     RaceHead h;
@@ -401,7 +402,7 @@ __global__ void __launch_bounds__(256) k_race(const __grid_constant__ RaceParams
             int64_t base = 0;
             if (avail < cnt) {
                 unsigned long long bb = 0ull;
-                if (lane == 0) bb = atomicAdd(&p.hdr->counter, (unsigned long long)p.chunk);
+                if (lane == 0) bb = atomicAdd(&p.hdr->counter, (unsigned long long)chunk);
                 base = (int64_t)__shfl_sync(FULL, bb, 0);
                 if (base >= total) exhausted = true;
             }
@@ -417,7 +418,7 @@ __global__ void __launch_bounds__(256) k_race(const __grid_constant__ RaceParams
                 q_next += cnt;
             } else {
                 q_next = base + (cnt - avail);
-                q_end = base + p.chunk;
+                q_end = base + chunk;
             }
         }
         if (__ballot_sync(FULL, active) == 0u) break;

@@ -538,6 +538,7 @@ __global__ void __launch_bounds__(256, MinCtas<MODEL>::value) k_single(const __g
     const int lane = threadIdx.x & 31;
     const unsigned lt_mask = (1u << lane) - 1u;
     const int64_t total = (p.total >= 0) ? p.total : __ldg(p.offsets + p.n_trials) - __ldg(p.offsets);
+    const int64_t chunk = warp_chunk(p.chunk, total);
 
     Lane L;
     TrialRow r;
@@ -564,7 +565,7 @@ __global__ void __launch_bounds__(256, MinCtas<MODEL>::value) k_single(const __g
             int64_t base = 0;
             if (avail < cnt) {
                 unsigned long long b = 0ull;
-                if (lane == 0) b = atomicAdd(&p.hdr->counter, (unsigned long long)p.chunk);
+                if (lane == 0) b = atomicAdd(&p.hdr->counter, (unsigned long long)chunk);
                 base = (int64_t)__shfl_sync(FULL, b, 0);
                 if (base >= total) exhausted = true;
             }
@@ -577,7 +578,7 @@ __global__ void __launch_bounds__(256, MinCtas<MODEL>::value) k_single(const __g
                 q_next += cnt;
             } else {
                 q_next = base + (cnt - avail);
-                q_end = base + p.chunk;
+                q_end = base + chunk;
             }
         }
         if (__ballot_sync(FULL, active) == 0u) break;
