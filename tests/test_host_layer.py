@@ -166,3 +166,19 @@ def test_expected_race_time_limits():
     assert expected_race_time([[0.0]], [[10.0]], 1.0, t_cap=5.0)[0] == 5.0
     e = expected_race_time([[0.0]], [[10.0]], 1.0, bound_kind=_lib.BOUND_LINEAR, a=[2.0], p1=[-4.0], t_cap=20.0)
     np.testing.assert_allclose(e, [0.5])
+
+
+def test_with_order_copies_the_launch_options():
+    import torch
+
+    from ssms_b200 import _device as D
+    from ssms_b200.batch import with_order
+
+    base = D.launch_opts(block_threads=128, blocks_per_sm=2, chunk=96, first_trial=7, refill_min=3)
+    o = torch.arange(4, dtype=torch.int32)
+    q = torch.arange(5, dtype=torch.int64)
+    lo = with_order(base, o, q)
+    assert (lo.block_threads, lo.blocks_per_sm, lo.chunk, lo.refill_min, lo.first_trial) == (128, 2, 96, 3, 7)
+    assert lo.trial_order == o.data_ptr() and lo.order_offsets == q.data_ptr()
+    lo = with_order(base, first_trial=11)
+    assert lo.first_trial == 11 and not lo.trial_order and not lo.order_offsets
