@@ -357,9 +357,9 @@ __device__ __forceinline__ bool step_block(const SingleParams &p, Lane &L, const
     const float b0 = (!INT_IX && BOUND == SSM_BOUND_LINEAR) ? fmaf(ixf0, r.dtp1, r.a) : 0.f;
     if (!INT_IX) L.tpb = L.tp;
     const float *drow = (MODEL == M_DFLEX) ? p.dtable + (int64_t)L.k * p.dstride : nullptr;
-    // device RNG: the block's drifts v(t_ix .. t_ix+7) are read before the
-    // steps, off the dependency chain (a live walk starts every block at a
-    // multiple of 8 steps); past the table's end the last entry repeats
+    // device RNG: the block's drifts v(t_ix .. t_ix+BLK-1) are read before
+    // the steps, off the dependency chain (a live walk starts every block at
+    // a multiple of BLK steps); past the table's end the last entry repeats
     float dvq[BLK];
     if (MODEL == M_DFLEX && !NOISE) {
         if (p.dvec && (L.ix & 3) == 0 && L.ix + BLK <= p.dlen) {
