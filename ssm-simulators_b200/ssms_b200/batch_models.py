@@ -35,6 +35,38 @@ def _dev(x, K=None, name="array"):
     return None if x is None else D.to_dev_f32(x, K, name)
 
 
+def boundary_spec(sim_name: str, kwargs: dict, boundary: dict, K: int, max_t: float, delta_t: float) -> dict:
+    """The kernel's boundary form of the sets' boundary (``bf.kernel_spec``;
+    the legacy DDM's [0, a] needs only a)."""
+    if sim_name == "ddm":
+        return {"kind": 1, "a": _col(kwargs["a"], K), "p1": None, "p2": None, "table": None}
+    return bf.kernel_spec(boundary["boundary_fun"], boundary["boundary_params"], K, bf.make_t_s(max_t, delta_t))
+
+
+def expected_set_time(sim_name: str, kwargs: dict, spec: dict | None, K: int, max_t: float) -> np.ndarray | None:
+    """Per-set estimate of the mean walk duration that orders the sets
+    longest-first (``expected_walk_time`` / ``expected_race_time``), capped by
+    min(max_t, deadline - t); None for a model without an Euler walk."""
+    if sim_name == "lba_vanilla":
+        return None
+    cap = np.minimum(float(max_t), np.maximum(np.asarray(_col(kwargs["deadline"], K), np.float64)
+                                              - np.asarray(_col(kwargs["t"], K), np.float64), 0.0))
+    if sim_name in SINGLE:
+        return expected_walk_time(_col(kwargs["v"], K), spec["a"], _col(kwargs["z"], K), _col(kwargs["s"], K),
+                                  legacy=sim_name == "ddm", bound_kind=int(spec["kind"]), p1=spec["p1"],
+                                  p2=spec["p2"], t_cap=cap)
+    v = np.asarray(kwargs["v"], np.float64).reshape(K, -1)
+    if sim_name in RACE:  # start z_j b(0), threshold b(t)
+        a0 = np.asarray(spec["a"], np.float64).reshape(K, 1)
+        dist = a0 * (1.0 - np.asarray(kwargs["z"], np.float64).reshape(K, -1))
+        return expected_race_time(v, dist, np.asarray(kwargs["s"], np.float64).reshape(K, -1),
+                                  bound_kind=int(spec["kind"]), a=spec["a"], p1=spec["p1"], t_cap=cap)
+    if sim_name == "racing_diffusion_model":  # start U(0, A), threshold b
+        dist = np.asarray(_col(kwargs["b"], K), np.float64) - 0.5 * np.asarray(_col(kwargs["A"], K), np.float64)
+        return expected_race_time(v, dist.reshape(K, 1), _col(kwargs["s"], K).reshape(K, 1), t_cap=cap)
+    raise ValueError(f"no batched device path for simulator {sim_name!r}")
+
+
 class SetBatch:
     """K parameter sets of one simulator, resident on the device.
 
@@ -53,17 +85,14 @@ class SetBatch:
         self.offsets_host = np.concatenate([[0], np.cumsum(ns)]).astype(np.int64)
         self.total = int(self.offsets_host[-1])
         self.offsets = torch.from_numpy(self.offsets_host).cuda()
-        self.order_t = self.qoff_t = None  # trials longest-first (outputs do not depend on the order)
+        self.order_t = self.qoff_t = None
         self.sim_name, self.K = sim_name, K
         self.n_samples = int(n_samples)
         self.max_t, self.delta_t, self.smooth = float(max_t), float(delta_t), bool(smooth_unif)
         self.n_acc = 1
+        spec = None
         if sim_name in SINGLE or sim_name in RACE:
-            if sim_name == "ddm":
-                spec = {"kind": 1, "a": _col(kwargs["a"], K), "p1": None, "p2": None, "table": None}
-            else:
-                spec = bf.kernel_spec(boundary["boundary_fun"], boundary["boundary_params"], K,
-                                      bf.make_t_s(max_t, delta_t))
+            spec = boundary_spec(sim_name, kwargs, boundary, K, max_t, delta_t)
             self.kind = int(spec["kind"])
             self.a, self.p1, self.p2 = _dev(spec["a"], K, "a"), _dev(spec["p1"], K), _dev(spec["p2"], K)
             self.table = None if spec["table"] is None else D.to_dev_f32(np.ascontiguousarray(spec["table"]))
@@ -73,14 +102,6 @@ class SetBatch:
             self.deadline, self.s = _dev(_col(kwargs["deadline"], K), K), _dev(_col(kwargs["s"], K), K)
             self.alpha = _dev(_col(kwargs["alpha"], K), K) if sim_name == "levy_flexbound" else None
             self.extra = {k: _dev(_col(kwargs[k], K), K, k) for k in _PER_TRIAL.get(sim_name, ())}
-            if K > 1:
-                cap = np.minimum(self.max_t, np.maximum(np.asarray(_col(kwargs["deadline"], K), np.float64)
-                                                        - np.asarray(_col(kwargs["t"], K), np.float64), 0.0))
-                est = expected_walk_time(_col(kwargs["v"], K), spec["a"], _col(kwargs["z"], K),
-                                         _col(kwargs["s"], K), legacy=sim_name == "ddm", bound_kind=self.kind,
-                                         p1=spec["p1"], p2=spec["p2"], t_cap=cap)
-                o, q = longest_first(est, ns)
-                self.order_t, self.qoff_t = torch.from_numpy(o).cuda(), torch.from_numpy(q).cuda()
             if sim_name == "ddm_flex":
                 if not drift:
                     raise ValueError("ddm_flex needs the drift dict (drift_fun, drift_params)")
@@ -96,11 +117,6 @@ class SetBatch:
             self.g = _dev(_col(kwargs["g"], K), K) if lca else None
             self.b = _dev(_col(kwargs["b"], K), K) if lca else None
             self.v_shape = v.shape
-            a0 = np.asarray(spec["a"], np.float64).reshape(K, 1)  # start z_j b(0), threshold b(t)
-            est = expected_race_time(v, a0 * (1.0 - np.asarray(kwargs["z"], np.float64).reshape(K, -1)),
-                                     np.asarray(kwargs["s"], np.float32), bound_kind=self.kind, a=spec["a"],
-                                     p1=spec["p1"], t_cap=self._cap(kwargs, K))
-            self._set_order(est, ns)
         elif sim_name == "racing_diffusion_model":
             v = np.asarray(kwargs["v"], np.float32)
             self.n_acc = int(v.shape[1])
@@ -108,10 +124,6 @@ class SetBatch:
             self.v = _dev(v)
             self.b, self.A, self.t, self.s = (_dev(_col(kwargs[k], K), K, k) for k in ("b", "A", "t", "s"))
             self.deadline = _dev(_col(kwargs["deadline"], K), K)
-            dist = (np.asarray(_col(kwargs["b"], K), np.float64) - 0.5 * np.asarray(_col(kwargs["A"], K), np.float64))
-            est = expected_race_time(v, dist.reshape(K, 1), _col(kwargs["s"], K).reshape(K, 1),
-                                     t_cap=self._cap(kwargs, K))
-            self._set_order(est, ns)
         elif sim_name == "lba_vanilla":
             v = np.asarray(kwargs["v"], np.float32)
             sd = np.asarray(kwargs["sd"], np.float32).reshape(K, -1)
@@ -124,14 +136,8 @@ class SetBatch:
             self.t, self.deadline = _dev(_col(kwargs["t"], K), K), _dev(_col(kwargs["deadline"], K), K)
         else:
             raise ValueError(f"no batched device path for simulator {sim_name!r}")
-
-    def _cap(self, kwargs, K):
-        """min(max_t, deadline - t) per trial: no walk lasts longer."""
-        return np.minimum(self.max_t, np.maximum(np.asarray(_col(kwargs["deadline"], K), np.float64)
-                                                 - np.asarray(_col(kwargs["t"], K), np.float64), 0.0))
-
-    def _set_order(self, est, ns):
-        if self.K > 1:
+        est = expected_set_time(sim_name, kwargs, spec, K, max_t) if K > 1 else None
+        if est is not None:  # sets longest-first (outputs do not depend on the order)
             o, q = longest_first(est, ns)
             self.order_t, self.qoff_t = torch.from_numpy(o).cuda(), torch.from_numpy(q).cuda()
 

@@ -182,3 +182,33 @@ def test_with_order_copies_the_launch_options():
     assert lo.trial_order == o.data_ptr() and lo.order_offsets == q.data_ptr()
     lo = with_order(base, first_trial=11)
     assert lo.first_trial == 11 and not lo.trial_order and not lo.order_offsets
+
+
+def test_set_order_estimates_for_every_configured_model():
+    """The longest-first estimate behind SetBatch (host only) is finite,
+    non-negative and within max_t for every configured model."""
+    from ssms_b200 import Simulator, model_config
+    from ssms_b200.batch_models import boundary_spec, expected_set_time
+
+    rng = np.random.default_rng(3)
+    K = 6
+    done = 0
+    for name, cfg in sorted(model_config.items()):
+        lo, hi = (np.asarray(b, np.float64) for b in cfg["param_bounds"])
+        theta = {p: rng.uniform(lo[j], hi[j], K).astype(np.float32) for j, p in enumerate(cfg["params"])}
+        try:
+            prep = Simulator(name).prepare(theta, n_samples=100, random_state=1)
+        except ValueError:  # draws outside the model's constraints: its defaults instead
+            theta = {p: np.full(K, d, np.float32) for p, d in zip(cfg["params"], cfg["default_params"])}
+            prep = Simulator(name).prepare(theta, n_samples=100, random_state=1)
+        sim_name = prep["config"]["simulator"].__name__
+        spec = None
+        if sim_name not in ("racing_diffusion_model", "lba_vanilla"):
+            spec = boundary_spec(sim_name, prep["theta"], prep["boundary"], K, 20.0, 0.001)
+        est = expected_set_time(sim_name, prep["theta"], spec, K, 20.0)
+        if sim_name == "lba_vanilla":
+            assert est is None
+            continue
+        assert est.shape == (K,) and np.all(np.isfinite(est)) and np.all(est >= 0) and np.all(est <= 20.0), name
+        done += 1
+    assert done >= 40
