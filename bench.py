@@ -218,6 +218,18 @@ class ClockSampler:
 K_SINGLE_TRAFFIC_BYTES = 12_520_960 + 289_847_552
 
 
+def hbm_peak() -> tuple[float, str]:
+    """(GB/s, basis): the measured copy bandwidth of this pool's B200s from
+    MEASURED_PEAKS.json, else the earlier measurement 6 650 GB/s."""
+    try:
+        v = float(json.loads((ROOT / "MEASURED_PEAKS.json").read_text())["hbm_gbs"])
+        if v > 0:
+            return v, "measured"
+    except (OSError, ValueError, KeyError, TypeError):
+        pass
+    return 6650.0, "fallback"
+
+
 def max_over_ranks(x: float, world: int) -> float:
     """The largest value of x over the ranks (device time of the slowest
     replica); x itself on one rank."""
@@ -309,6 +321,7 @@ def run_ours(args, rank, world, local_rank):
     f_max = (clocks.get("sm_max_mhz") or 1965.0) * 1e6
     peak_steps = N_SM * LANES_PER_SM_CLK * f_max / INSTR_PER_STEP
     achieved_steps = steps_per_launch / (ms_per_step / 1e3)
+    hbm_gbs, hbm_basis = hbm_peak()
     traffic = K_SINGLE_TRAFFIC_BYTES if args.n_theta == N_THETA else None
     line = {
         "metric": METRIC, "value": value, "unit": "trajectories/s", "n_gpus": world,
@@ -324,7 +337,9 @@ def run_ours(args, rank, world, local_rank):
                      "algorithmic_bytes": total * 8,
                      "peak_basis": f"{N_SM} SMs x {LANES_PER_SM_CLK} lanes/clk x {f_max/1e6:.0f} MHz / "
                                    f"{INSTR_PER_STEP:.0f} lane-instructions per accumulator-step",
-                     "output_hbm_gbs": total * 8 / (ms_per_step / 1e3) / 1e9},
+                     "output_hbm_gbs": total * 8 / (ms_per_step / 1e3) / 1e9,
+                     "hbm_peak_gbs": hbm_gbs, "hbm_peak_basis": hbm_basis,
+                     "hbm_frac": total * 8 / (ms_per_step / 1e3) / 1e9 / hbm_gbs},
         "e2e": {"value": e2e_value, "unit": "trajectories/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
         "gpu_launches": 2 * args.steps,

@@ -52,3 +52,12 @@ def test_timing_is_the_slowest_rank_and_value_aggregates_replicas():
     got = sorted(q.get(timeout=10) for _ in range(2))
     assert [g[1] for g in got] == [15.0, 15.0]  # both ranks report the slower rank's time
     assert got[0][2] == pytest.approx(2 * 1000 * 4 / 0.015)
+
+
+def test_hbm_peak_reads_the_measured_file_or_falls_back():
+    import bench
+
+    v, basis = bench.hbm_peak()
+    assert v > 1000 and basis in ("measured", "fallback")
+    if (ROOT / "MEASURED_PEAKS.json").exists():
+        assert basis == "measured"
