@@ -1,17 +1,39 @@
-"""HSSM glue: posterior- and prior-predictive sampling through the GPU simulators.
+"""HSSM glue: prior- and posterior-predictive sampling through the GPU simulators.
 
-Same functions, argument meanings and errors as the reference module
-(ssms/hssm_support.py): HSSM calls ``rng_fn`` with one array per model
-parameter (scalars, or arrays whose last axis runs over data trials), a
-``size`` and a numpy generator; the parameters become a theta matrix, one
-``simulator()`` call draws every replica of every trial (here: one batched GPU
-launch), and the (rt, choice) pairs come back shaped like the parameters.
+HSSM (the hierarchical SSM package) draws from a model's random variable by
+calling ``rng_fn`` with one array per model parameter, a ``size`` and a numpy
+``Generator`` (the reference's entry point is ssms/hssm_support.py:388-455).
+A parameter array is either a single value or an array whose last axis runs
+over the data trials; leading axes (posterior draws, chains) broadcast.
+
+Here the whole request becomes one ``TrialLayout``: a theta matrix with one
+row per (leading index, data trial) in C order, the number of replicas drawn
+per row, and the shape the (rt, choice) pairs are folded back into.  Per-trial
+covariates (``extra_fields``) are spread over the same rows by the same
+layout.  One ``simulator()`` call then draws every replica of every row in a
+single batched device launch.
+
+Interface kept from the reference: the public functions and their arguments,
+the attributes a simulator function carries (``model_name``, ``choices``,
+``obs_dim``), the seed range [0, 2**31) drawn with one ``rng.integers`` call,
+the theta row order, the output shapes and the error messages.
+
+One behaviour differs on purpose.  With more than one replica per row, the
+reference's ``hssm_sim_wrapper`` returns the pairs replica-major
+([replica, row, 2]) and ``rng_fn`` reshapes them into (..., row, replica, 2)
+without a transpose, so the slot of (row i, replica r) receives a draw made
+with the parameters of row (i * n_replicas + r) mod n_rows.  Here the wrapper
+returns them row-major, so every slot holds a draw of its own row's
+parameters.  ``rng_fn`` itself folds the simulator's output exactly as the
+reference does, so a user-supplied simulator function sees the same call and
+gets the same result.
 """
 
 from __future__ import annotations
 
 import logging
 from functools import partial
+from numbers import Integral
 from typing import Any, Callable
 
 import numpy as np
@@ -21,143 +43,156 @@ from .simulator import simulator
 
 _logger = logging.getLogger(__name__)
 
-
-def _extract_size_val(size) -> int:
-    return int(size[0]) if isinstance(size, tuple) else size
-
-
-def _validate_size(size_val: int, new_data_size: int) -> None:
-    if size_val % new_data_size != 0:
-        raise ValueError("`size` needs to be a multiple of the size of data")
+#: Simulator seeds are drawn from [0, SEED_CEILING): a C ``long`` on every platform.
+SEED_CEILING = 2**31
 
 
-def _calculate_n_replicas(is_all_args_scalar, size, new_data_size) -> int:
-    """Replicas drawn per data trial: 1 for scalar parameters or size None/1,
-    else size / (number of data trials), which must divide exactly."""
-    if is_all_args_scalar or size is None or size == 1:
-        return 1
-    size_val = _extract_size_val(size)
-    _validate_size(size_val, new_data_size)
-    return size_val // new_data_size
+class TrialLayout:
+    """How HSSM's parameter arrays map onto simulator rows and back.
 
+    ``theta``        [rows, n_params], one row per simulated trial; its dtype
+                     is the parameters' common dtype.
+    ``trial_shape``  the shape every parameter broadcasts to (None when all
+                     parameters are single values: then ``rows`` is ``size``).
+    ``n_replicas``   draws per row: ``size / n_data_trials`` when ``size`` is
+                     given for array parameters, else 1.
+    """
 
-def _get_seed(rng) -> int:
-    """A seed in [0, 2**31), the range the simulators accept on every platform."""
-    return int(rng.integers(0, 2**31))
+    __slots__ = ("theta", "trial_shape", "n_replicas")
 
+    def __init__(self, arg_arrays, size):
+        params = [np.asarray(a) for a in arg_arrays]
+        dtype = np.result_type(*params)
+        if all(p.size == 1 for p in params):
+            # single values: one row repeated once per requested observation
+            if len({p.shape for p in params}) > 1:
+                raise ValueError("all input arrays must have the same shape")
+            rows = self._scalar_rows(size)
+            self.trial_shape = None
+            self.n_replicas = 1
+            self.theta = np.empty((rows, len(params)), dtype)
+            self.theta[:] = np.array([p.reshape(-1)[0] for p in params], dtype)
+            return
+        # arrays: broadcast every parameter to the largest one's shape, one column each
+        widest = max(range(len(params)), key=lambda j: (params[j].size, -j))
+        self.trial_shape = tuple(params[widest].shape)
+        self.theta = np.empty((int(np.prod(self.trial_shape)), len(params)), dtype)
+        for j, p in enumerate(params):
+            self.theta[:, j] = np.broadcast_to(p, self.trial_shape).reshape(-1)
+        self.n_replicas = self._replicas(size, self.trial_shape[-1])
 
-def _prepare_theta_and_shape(arg_arrays, size):
-    """(all scalar?, theta, max_shape, n_data_trials).  Scalar parameters are
-    stacked into one row and tiled ``size`` times; otherwise every parameter is
-    broadcast to the largest one's shape and flattened into a column of theta."""
-    if all(arg.size == 1 for arg in arg_arrays):
-        theta = np.stack(arg_arrays)
-        if theta.ndim > 1:
-            theta = theta.squeeze(axis=-1)
+    @staticmethod
+    def _scalar_rows(size) -> int:
         if isinstance(size, tuple) and len(size) == 1:
-            n = size[0]
-        elif isinstance(size, int):
-            n = size
-        else:
-            raise ValueError(f"Size must be a tuple of length 1 or an integer, but got {type(size)}")
-        return True, np.tile(theta, (n, 1)), None, None
-    largest = int(np.argmax([arg.size for arg in arg_arrays]))
-    max_shape = arg_arrays[largest].shape
-    theta = np.column_stack([np.broadcast_to(arg, max_shape).reshape(-1) for arg in arg_arrays])
-    return False, theta, max_shape, max_shape[-1]
+            return int(size[0])
+        if isinstance(size, Integral):
+            return int(size)
+        raise ValueError(f"Size must be a tuple of length 1 or an integer, but got {type(size)}")
 
+    @staticmethod
+    def _replicas(size, n_data_trials: int) -> int:
+        if size is None or (not isinstance(size, tuple) and size == 1):
+            return 1
+        total = int(size[0]) if isinstance(size, tuple) else int(size)
+        if total % n_data_trials:
+            raise ValueError("`size` needs to be a multiple of the size of data")
+        return total // n_data_trials
 
-def _broadcast_extra_fields(extra_fields, max_shape, new_data_size):
-    """Per-trial covariates (leading axis = data trials) broadcast and flattened
-    like theta's rows; anything else passes through."""
-    lead = tuple(max_shape[:-1])
-    out = {}
-    for key, value in extra_fields.items():
-        arr = np.asarray(value)
-        if arr.ndim == 0 or arr.shape[0] != new_data_size:
+    @property
+    def n_data_trials(self) -> int | None:
+        return None if self.trial_shape is None else self.trial_shape[-1]
+
+    def spread(self, covariates: dict) -> dict:
+        """Per-trial covariates (first axis = the data trials) repeated over
+        the leading axes like theta's rows, so row i of theta and row i of
+        every covariate describe the same trial; anything else unchanged."""
+        lead = self.trial_shape[:-1]
+        out = {}
+        for key, value in covariates.items():
+            arr = np.asarray(value)
+            if arr.ndim and arr.shape[0] == self.n_data_trials:
+                tiled = np.broadcast_to(arr, lead + arr.shape)
+                arr = np.ascontiguousarray(tiled.reshape((-1,) + arr.shape[1:]))
             out[key] = arr
-            continue
-        out[key] = np.ascontiguousarray(np.broadcast_to(arr, lead + arr.shape).reshape((-1,) + arr.shape[1:]))
-    return out
+        return out
 
+    def output_shape(self, obs_dim: int) -> tuple:
+        reps = (self.n_replicas,) if self.n_replicas != 1 else ()
+        return self.trial_shape + reps + (int(obs_dim),)
 
-def _reshape_sims_out(max_shape, n_replicas, obs_dim_int):
-    shape = [*max_shape[:-1], max_shape[-1]]
-    if n_replicas != 1:
-        shape.append(n_replicas)
-    shape.append(obs_dim_int)
-    return tuple(shape)
-
-
-def _validate_simulator_fun_arg(simulator_fun) -> None:
-    if not (isinstance(simulator_fun, str) or callable(simulator_fun)):
-        raise ValueError("`simulator_fun` must be a string or a callable, "
-                         f"but you passed {type(simulator_fun)}.")
+    def fold(self, sims: np.ndarray, obs_dim: int) -> np.ndarray:
+        """The simulator's [rows * replicas, obs_dim] output in the
+        parameters' shape; single-value requests come back as drawn."""
+        return sims if self.trial_shape is None else sims.reshape(self.output_shape(obs_dim))
 
 
 def decorate_atomic_simulator(model_name: str, choices=None, obs_dim: int = 2):
-    """Attach ``model_name``, ``choices`` and ``obs_dim`` to a simulator function."""
-    choices = [-1, 1] if choices is None else choices
+    """Decorator giving a simulator function the attributes HSSM reads:
+    ``model_name``, ``choices`` (default [-1, 1]) and ``obs_dim``."""
+    labels = [-1, 1] if choices is None else choices
 
-    def decorator(func):
-        func.model_name = model_name
-        func.choices = choices
-        func.obs_dim = obs_dim
+    def tag(func):
+        func.model_name, func.choices, func.obs_dim = model_name, labels, obs_dim
         return func
 
-    return decorator
+    return tag
 
 
 def hssm_sim_wrapper(simulator_fun, theta, model, n_replicas, random_state, **kwargs):
-    """simulator_fun(theta, model, n_samples=n_replicas, random_state) stacked
-    into (..., 2) (rt, choice) pairs."""
-    out = simulator_fun(theta=theta, model=model, n_samples=n_replicas, random_state=random_state, **kwargs)
-    return np.stack([out["rts"], out["choices"]], axis=-1).squeeze()
-
-
-def _build_decorated_simulator(model_name: str, choices: list, obs_dim: int = 2) -> Callable:
-    wrapper = partial(hssm_sim_wrapper, simulator_fun=simulator, model=model_name)
-    return decorate_atomic_simulator(model_name=model_name, choices=choices, obs_dim=obs_dim)(wrapper)
+    """Run ``simulator_fun(theta=..., model=..., n_samples=n_replicas,
+    random_state=...)`` and return (rt, choice) pairs, row-major: for rts of
+    shape [n_replicas, n_rows, 1] the result is [n_rows, n_replicas, 2],
+    with length-1 axes dropped."""
+    res = simulator_fun(theta=theta, model=model, n_samples=n_replicas, random_state=random_state, **kwargs)
+    pairs = np.stack([np.asarray(res["rts"]), np.asarray(res["choices"])], axis=-1)
+    if pairs.ndim == 4 and pairs.shape[2] == 1:  # [replica, row, 1, 2] -> [row, replica, 2]
+        pairs = pairs[:, :, 0, :].transpose(1, 0, 2)
+    return pairs.squeeze()
 
 
 def get_simulator_fun_internal(simulator_fun: Callable | str):
-    """A callable as given, or the decorated GPU simulator of a model name
-    (with a warning for names the package does not know)."""
-    _validate_simulator_fun_arg(simulator_fun)
+    """A callable is returned as given; a model name becomes this package's
+    GPU ``simulator()`` for that model, tagged with the model's choices
+    (with a warning, and choices [0, 1, 2], for names the package does not
+    know)."""
+    if not (isinstance(simulator_fun, str) or callable(simulator_fun)):
+        raise ValueError("`simulator_fun` must be a string or a callable, "
+                         f"but you passed {type(simulator_fun)}.")
     if callable(simulator_fun):
         return simulator_fun
-    if simulator_fun not in _model_config:
+    name = simulator_fun
+    if name not in _model_config:
         _logger.warning("You supplied a model '%s', which is currently not supported in the ssm_simulators "
                         "package. An error will be thrown when sampling from the random variable or when "
-                        "using any posterior or prior predictive sampling methods.", simulator_fun)
-    choices = _model_config.get(simulator_fun, {}).get("choices", [0, 1, 2])
-    return _build_decorated_simulator(model_name=simulator_fun, choices=choices)
+                        "using any posterior or prior predictive sampling methods.", name)
+    choices = _model_config[name]["choices"] if name in _model_config else [0, 1, 2]
+    draw = partial(hssm_sim_wrapper, simulator_fun=simulator, model=name)
+    return decorate_atomic_simulator(model_name=name, choices=choices, obs_dim=2)(draw)
 
 
 def validate_simulator_fun(simulator_fun: Any) -> tuple[str, list, int]:
-    """(model_name, choices, obs_dim) of a decorated simulator function."""
-    if not hasattr(simulator_fun, "model_name"):
-        raise ValueError("The simulator function must have a `model_name` attribute.")
-    if not hasattr(simulator_fun, "choices"):
-        raise ValueError("The simulator function must have a `choices` attribute.")
-    if not hasattr(simulator_fun, "obs_dim"):
-        raise ValueError("The simulator function must have a `obs_dim` attribute.")
+    """(model_name, choices, obs_dim) of a tagged simulator function; raises
+    ValueError naming the first missing attribute or a non-integer obs_dim."""
+    for attr in ("model_name", "choices", "obs_dim"):
+        if not hasattr(simulator_fun, attr):
+            raise ValueError(f"The simulator function must have a `{attr}` attribute.")
     if not isinstance(simulator_fun.obs_dim, int):
         raise ValueError("The obs_dim attribute must be an integer")
     return simulator_fun.model_name, simulator_fun.choices, simulator_fun.obs_dim
 
 
 def rng_fn(arg_arrays, size, rng, simulator_fun: Callable, obs_dim_int: int, *args, **kwargs) -> np.ndarray:
-    """Draw (rt, choice) pairs for HSSM's random variable: all trials and
-    replicas in one simulator call, returned shaped like the parameters
-    (..., n_trials[, n_replicas], obs_dim)."""
-    is_all_scalar, theta, max_shape, new_data_size = _prepare_theta_and_shape(arg_arrays, size)
-    n_replicas = _calculate_n_replicas(is_all_scalar, size, new_data_size)
-    seed = _get_seed(rng)
-    if kwargs.get("extra_fields") is not None and not is_all_scalar and max_shape is not None:
-        kwargs = {**kwargs, "extra_fields": _broadcast_extra_fields(kwargs["extra_fields"], max_shape,
-                                                                    new_data_size)}
-    sims_out = simulator_fun(theta=theta, random_state=seed, n_replicas=n_replicas, **kwargs)
-    if not is_all_scalar:
-        sims_out = sims_out.reshape(_reshape_sims_out(max_shape, n_replicas, obs_dim_int))
-    return sims_out
+    """Draw (rt, choice) pairs for HSSM's random variable.
+
+    ``arg_arrays``: one array per model parameter; ``size``: the number of
+    observations for single-value parameters, else None/1 or a multiple of
+    the number of data trials (replicas per trial); ``rng`` supplies the
+    simulator seed.  Returns [size, obs_dim] for single-value parameters and
+    [*trial_shape, (n_replicas,) obs_dim] otherwise."""
+    layout = TrialLayout(arg_arrays, size)
+    seed = int(rng.integers(0, SEED_CEILING))
+    call = dict(kwargs)
+    if call.get("extra_fields") is not None and layout.trial_shape is not None:
+        call["extra_fields"] = layout.spread(call["extra_fields"])
+    sims = simulator_fun(theta=layout.theta, random_state=seed, n_replicas=layout.n_replicas, **call)
+    return layout.fold(np.asarray(sims), obs_dim_int)
