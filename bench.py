@@ -26,6 +26,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 from pathlib import Path
 
@@ -125,11 +126,15 @@ class CpuPool:
         # warm the workers (imports, library loads)
         self.pool.map(_cpu_worker, [(self.kind, [(0.5, 1.0, 0.5, 0.1, 0.2, 10, 1)])] * self.cores)
 
-    def sample_rows(self, theta, n_samples, per_core: int = 24):
-        m = min(len(n_samples), per_core * self.cores)
+    def sample_rows(self, theta, n_samples, per_core: int = 24, start: int = 0):
+        """per_core x cores consecutive theta rows from ``start`` (wrapping
+        around the batch), each with its own seed."""
+        K = len(n_samples)
+        m = min(K, per_core * self.cores)
+        idx = [(start + j) % K for j in range(m)]
         return [(float(theta["v"][i]), float(theta["a"][i]), float(theta["z"][i]),
                  float(theta["t"][i]), float(theta["theta"][i]), int(n_samples[i]), 1000 + i)
-                for i in range(m)]
+                for i in idx]
 
     def run(self, rows) -> tuple[int, float]:
         """Rows are handed out one at a time, longest first, so no core idles
@@ -157,10 +162,14 @@ def cpu_baseline_record(theta, n_samples) -> dict:
 
 # ------------------------------------------------------------------ clocks
 class ClockSampler:
+    """nvidia-smi clock samples every 200 ms while the block runs, written to a
+    file in ``$SSM_BENCH_CLOCKS_DIR`` (default: a fresh temporary directory)."""
+
     def __init__(self, index: int):
         self.index = index
         self.proc = None
-        self.path = ROOT / "gpurun_out" / f"clocks_{index}_{os.getpid()}.csv"
+        folder = os.environ.get("SSM_BENCH_CLOCKS_DIR") or tempfile.mkdtemp(prefix="ssm_bench_clocks_")
+        self.path = Path(folder) / f"clocks_{index}_{os.getpid()}.csv"
 
     def __enter__(self):
         q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
@@ -648,17 +657,27 @@ def run_other_workloads(args) -> dict:
 
 
 def run_reference(args):
+    """The reference's compiled sequential simulator on every host core.  Each
+    warm-up and timed step takes the next block of theta rows of the batch
+    (wrapping around), so the steps together cover distinct rows of the
+    workload instead of re-timing one block."""
     theta, n_samples = workload(SEED)
     pool = CpuPool()
-    rows = pool.sample_rows(theta, n_samples, per_core=8)
+    per_core = 8
+    block = per_core * pool.cores
+    step = 0
     for _ in range(args.warmup):
-        pool.run(rows)
+        pool.run(pool.sample_rows(theta, n_samples, per_core=per_core, start=step * block))
+        step += 1
     done_total, sec_total = 0, 0.0
     for _ in range(args.steps):
-        done, sec = pool.run(rows)
+        done, sec = pool.run(pool.sample_rows(theta, n_samples, per_core=per_core, start=step * block))
+        step += 1
         done_total += done
         sec_total += sec
     pool.close()
+    covered = min(N_THETA, step * block)
+    rows = [None] * min(block, N_THETA)
     value = done_total / sec_total
     return {
         "metric": METRIC, "value": value, "unit": "trajectories/s", "n_gpus": 0,
@@ -666,11 +685,13 @@ def run_reference(args):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded uniform parameter draws; no dataset)",
         "config": {"workload": WORKLOAD, "n_theta": N_THETA,
-                   "sample_theta_per_step": len(rows), "seed": SEED},
+                   "sample_theta_per_step": len(rows), "theta_rows_covered": covered, "seed": SEED},
         "impl": "reference",
         "cpu_baseline": {"value": value, "unit": METRIC, "cores": pool.cores, "kind": pool.kind,
-                         "sample": f"first {len(rows)} theta rows per step ({done_total // max(args.steps, 1)} "
-                                   f"trajectories), {pool.cores} spawned processes"},
+                         "sample": f"{len(rows)} consecutive theta rows per step, the next block each step "
+                                   f"({covered} of {N_THETA} rows over warm-up and timed steps; "
+                                   f"{done_total // max(args.steps, 1)} trajectories per timed step), "
+                                   f"{pool.cores} spawned processes"},
         "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
 

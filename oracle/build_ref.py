@@ -15,6 +15,10 @@ optimisation level.  GSL is absent on this image, so the parallel path is
 compiled with the header's stubs and ``check_parallel_request`` clamps
 ``n_threads`` to 1 (src/cssm/_openmp_status.pyx:228-242).
 
+The reference sources are found through ``reference_root()``: the
+directory named by the environment variable ``SSM_REFERENCE_ROOT``, else a
+checkout named ``reference`` beside this repository's own directory.
+
 Usage:  python oracle/build_ref.py [--reference-root DIR]
 """
 
@@ -38,6 +42,15 @@ MODULES = ["_utils", "_openmp_status", "ddm_models", "race_models", "levy_models
 
 CXX_FLAGS = ["-O3", "-ffast-math", "-march=x86-64-v2", "-funroll-loops", "-fopenmp",
              "-fPIC", "-shared", "-DHAVE_OPENMP=1", "-w"]
+
+
+def reference_root() -> Path | None:
+    """The reference source tree (a directory holding ``src/cssm`` and
+    ``ssms``): ``$SSM_REFERENCE_ROOT``, else ``../reference`` relative to the
+    repository root; None when neither exists."""
+    env = os.environ.get("SSM_REFERENCE_ROOT")
+    cand = Path(env) if env else HERE.parent.parent / "reference"
+    return cand if (cand / "src" / "cssm").is_dir() else None
 
 
 def _find_cxx() -> str:
@@ -78,10 +91,14 @@ def build(reference_root: Path, force: bool = False) -> Path:
 
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference-root", default=os.environ.get("SSM_REFERENCE_ROOT", "/root/reference"))
+    ap.add_argument("--reference-root", default=None,
+                    help="reference source tree (default: $SSM_REFERENCE_ROOT, else ../reference)")
     ap.add_argument("--force", action="store_true")
     args = ap.parse_args()
-    build(Path(args.reference_root), force=args.force)
+    root = Path(args.reference_root) if args.reference_root else reference_root()
+    if root is None:
+        raise SystemExit("reference sources not found: set SSM_REFERENCE_ROOT or pass --reference-root")
+    build(root, force=args.force)
 
 
 if __name__ == "__main__":

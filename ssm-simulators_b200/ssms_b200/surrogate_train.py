@@ -4,13 +4,22 @@ against simulation + KDE.
     python -m ssms_b200.surrogate_train --model angle --train-sets 100000 \\
         --n-samples 100000 --epochs 20 --out angle_surrogate.pt --report report.json
 
-Records come from ``BatchedKdePipeline`` (the reference's LAN-KDE generator
-config: 1000 rows per parameter set, mixture 0.8 KDE resamples / 0.1 uniform
-rts / 0.1 negative rts) and never leave the device.  The judge draws fresh
-parameter sets, simulates ``n_samples`` trajectories for each, fits the LogKDE
-and evaluates it at uniform (rt, choice) queries; the error is the mean
-absolute difference of log-likelihoods with both sides raised to the
-surrogate's label lower bound.
+Records come from ``BatchedKdePipeline`` with the reference's LAN-KDE
+generator config (ssms/config/data_generator_config.py) and 1000 rows per
+parameter set: 800 KDE resamples and 200 uniform rts in (0, max_t) with a
+uniform choice (``RECORD_MIXTURE``), no negative-rt rows.  They never leave
+the device.
+
+The judge draws fresh parameter sets and uniform (rt, choice) queries and
+compares the surrogate with simulation + KDE (``n_samples`` trajectories per
+set, the reference's LogKDE).  One simulation + KDE estimate is itself noisy:
+two independent runs at 1e5 trajectories differ by about 0.08 in mean
+absolute log-likelihood, more than the 0.05 the surrogate is held to.  So the
+judge is the average of ``runs`` independent simulation + KDE estimates, each
+raised to the label lower bound first -- the quantity the network's
+(Huber, delta 1) training estimates, since every record's label is one such
+estimate -- and its own noise is reported as the mean absolute difference of
+two judges built from disjoint runs.
 """
 
 from __future__ import annotations
@@ -27,12 +36,18 @@ from .dataset_generators import BatchedKdePipeline, get_lan_kde_config
 from .surrogate import DIN, MlpSurrogate, kde_loglik
 
 
+#: KDE resamples / uniform rts / negative rts per parameter set: 800 + 200 + 0
+#: of 1000 rows, the training-data configuration the surrogate is built on.
+RECORD_MIXTURE = (0.8, 0.2, 0.0)
+
+
 def make_records(model: str, n_sets: int, *, n_samples: int, seed: int, n_per_set: int = 1000,
-                 batch_size: int = 4096) -> torch.Tensor:
+                 batch_size: int = 4096, mixture=RECORD_MIXTURE) -> torch.Tensor:
     """[n_sets * n_per_set, 8] float32 training records on the device."""
     cfg = get_lan_kde_config(model)
     cfg["simulator"]["n_samples"] = int(n_samples)
     cfg["training"]["n_samples_per_param"] = int(n_per_set)
+    cfg["training"]["mixture_probabilities"] = [float(p) for p in mixture]
     pipe = BatchedKdePipeline(cfg, model_config[model], batch_size=batch_size)
     return pipe.generate(n_sets, seed=seed, on_device=True)["records"]
 
@@ -50,20 +65,37 @@ def uniform_queries(model: str, n_theta: int, n_per_theta: int, *, seed: int, rt
     return th, np.ascontiguousarray(x, np.float32)
 
 
-def judge(net: MlpSurrogate, model: str, x: np.ndarray, *, n_samples: int, seed: int) -> dict:
-    """Surrogate vs simulation + KDE on query rows x (rows sharing theta share one simulation)."""
-    ref = kde_loglik(model, x[:, :DIN - 2], x[:, DIN - 2], x[:, DIN - 1], n_samples=n_samples, seed=seed)
-    # a second, independent simulation + KDE: the judge's own run-to-run noise
-    ref2 = kde_loglik(model, x[:, :DIN - 2], x[:, DIN - 2], x[:, DIN - 1], n_samples=n_samples, seed=seed + 1)
-    pred = net.forward(torch.from_numpy(x)).double().cpu().numpy()
-    lb = net.label_lower_bound if net.label_lower_bound is not None else -np.inf
-    r, r2, p = np.maximum(ref, lb), np.maximum(ref2, lb), np.maximum(pred, lb)
-    err = np.abs(p - r)
-    err2 = np.abs(r2 - r)
-    live = r > lb  # queries where the reference density is above the floor
-    return {"mae": float(err.mean()), "mae_above_floor": float(err[live].mean()) if live.any() else 0.0,
-            "kde_vs_kde_mae": float(err2.mean()),
-            "kde_vs_kde_mae_above_floor": float(err2[live].mean()) if live.any() else 0.0,
+def judge_loglik(model: str, x: np.ndarray, *, n_samples: int, seed: int, runs: int,
+                 lower_bound: float) -> np.ndarray:
+    """Mean over ``runs`` independent simulation + KDE estimates (seeds seed,
+    seed + 1, ...) of max(log-likelihood, lower_bound) at query rows x."""
+    acc = np.zeros(x.shape[0], np.float64)
+    for r in range(int(runs)):
+        ll = kde_loglik(model, x[:, :DIN - 2], x[:, DIN - 2], x[:, DIN - 1], n_samples=n_samples, seed=seed + r)
+        acc += np.maximum(ll, lower_bound)
+    return acc / int(runs)
+
+
+def judge(net: MlpSurrogate, model: str, x: np.ndarray, *, n_samples: int, seed: int, runs: int = 16) -> dict:
+    """Surrogate vs simulation + KDE on query rows x (rows sharing theta share
+    one simulation per run).
+
+    ``mae``: surrogate against the average of ``runs`` clipped estimates.
+    ``judge_noise_mae``: that judge against a second one built from ``runs``
+    other seeds -- the judge's own resolution.  ``single_run_mae``: one
+    estimate against the judge (what a single simulation + KDE run scores)."""
+    lb = net.label_lower_bound if net.label_lower_bound is not None else -1e30
+    ref = judge_loglik(model, x, n_samples=n_samples, seed=seed, runs=runs, lower_bound=lb)
+    ref2 = judge_loglik(model, x, n_samples=n_samples, seed=seed + runs, runs=runs, lower_bound=lb)
+    one = np.maximum(kde_loglik(model, x[:, :DIN - 2], x[:, DIN - 2], x[:, DIN - 1], n_samples=n_samples,
+                                seed=seed + 2 * runs), lb)
+    pred = np.maximum(net.forward(torch.from_numpy(x)).double().cpu().numpy(), lb)
+    err = np.abs(pred - ref)
+    live = ref > lb + 1e-9  # queries where the judge sits above the floor
+    return {"mae": float(err.mean()), "judge_runs": int(runs), "n_samples": int(n_samples),
+            "judge_noise_mae": float(np.abs(ref2 - ref).mean()),
+            "single_run_mae": float(np.abs(one - ref).mean()),
+            "mae_above_floor": float(err[live].mean()) if live.any() else 0.0,
             "frac_above_floor": float(live.mean()), "max_abs_err": float(err.max()), "n": int(x.shape[0])}
 
 
@@ -107,6 +139,7 @@ def main(argv=None) -> dict:
     ap.add_argument("--loss", default="huber")
     ap.add_argument("--judge-sets", type=int, default=1000)
     ap.add_argument("--judge-per-set", type=int, default=1000)
+    ap.add_argument("--judge-runs", type=int, default=16)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--out", default=None)
     ap.add_argument("--report", default=None)
@@ -146,7 +179,8 @@ def main(argv=None) -> dict:
     del rec
 
     _, xq = uniform_queries(a.model, a.judge_sets, a.judge_per_set, seed=a.seed + 11)
-    rep["judge_uniform"] = judge(net, a.model, xq, n_samples=a.n_samples, seed=a.seed + 13)
+    rep["judge_uniform"] = judge(net, a.model, xq, n_samples=a.n_samples, seed=a.seed + 13,
+                                 runs=a.judge_runs)
     rep["surrogate_evals_per_s"] = time_surrogate(net, xq, want_dx=False)
     rep["surrogate_grad_evals_per_s"] = time_surrogate(net, xq, want_dx=True)
     rep["sim_kde_evals_per_s"] = time_sim_kde(a.model, xq, n_samples=a.n_samples, seed=a.seed + 17)

@@ -5,9 +5,11 @@ name, parameter names, parameter bounds, default values, choices, number of
 particles, boundary name and the simulator's name.  The transforms applied to
 parameters before simulation are restated in ``ssms_b200/config/__init__.py``.
 
+This generator reads the reference; the package only reads its output.
+
 Usage (needs the reference sources and its compiled simulators, see
 oracle/build_ref.py):
-    python ssm-simulators_b200/ssms_b200/config/gen_model_table.py [--reference-root DIR]
+    python tests/golden/gen_model_table.py [--reference-root DIR]
 """
 
 from __future__ import annotations
@@ -20,7 +22,8 @@ import types
 from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
-REPO = HERE.parents[2]
+REPO = HERE.parents[1]
+TABLE = REPO / "ssm-simulators_b200" / "ssms_b200" / "config" / "model_table.json"
 SIMULATORS = {"ddm_flexbound", "ddm", "race_model", "lca", "levy_flexbound", "lba_vanilla", "full_ddm",
               "ddm_sdv", "ornstein_uhlenbeck", "ddm_flex", "racing_diffusion_model"}
 
@@ -56,9 +59,16 @@ def _import_reference(root: Path):
 
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference-root", default="/root/reference")
+    ap.add_argument("--reference-root", default=None)
     args = ap.parse_args()
-    model_config = _import_reference(Path(args.reference_root))
+    if args.reference_root is None:
+        sys.path.insert(0, str(HERE))
+        from make_adapter_golden import reference_root
+
+        root = reference_root()
+    else:
+        root = Path(args.reference_root)
+    model_config = _import_reference(root)
     table = {}
     for name, cfg in model_config.items():
         sim = getattr(cfg["simulator"], "__name__", "")
@@ -77,8 +87,8 @@ def main() -> None:
             "n_particles": int(cfg["n_particles"]), "simulator": sim,
             "drift_name": cfg.get("drift_name"),
         }
-    (HERE / "model_table.json").write_text(json.dumps(table, indent=1))
-    print(f"wrote {len(table)} models to {HERE / 'model_table.json'}")
+    TABLE.write_text(json.dumps(table, indent=1))
+    print(f"wrote {len(table)} models to {TABLE}")
 
 
 if __name__ == "__main__":

@@ -22,6 +22,17 @@ HERE = Path(__file__).resolve().parent
 ROOT = HERE.parents[1]
 
 
+def reference_root() -> Path:
+    """The reference source tree, located by oracle/build_ref.py."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    from build_ref import reference_root as locate
+
+    root = locate()
+    if root is None:
+        raise SystemExit("reference sources not found: set SSM_REFERENCE_ROOT")
+    return root
+
+
 def _reference():
     orig = im.version
     im.version = lambda name: "0.13.2" if name == "ssm-simulators" else orig(name)
@@ -38,7 +49,7 @@ def _reference():
             if not k.startswith("_"):
                 setattr(cssm, k, getattr(mod, k))
     cssm.__getattr__ = lambda name: (lambda *a, **k: None)
-    sys.path.insert(0, "/root/reference")
+    sys.path.insert(0, str(reference_root()))
     from ssms.basic_simulators.simulator_class import Simulator
     from ssms.config import model_config
 

@@ -81,7 +81,9 @@ def _reference_drifts():
     """The reference's drift functions, loaded from its source file."""
     import importlib.util
 
-    ref = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    from make_adapter_golden import reference_root
+
+    ref = Path(sys.argv[1]) if len(sys.argv) > 1 and not sys.argv[1].startswith("--") else reference_root()
     spec = importlib.util.spec_from_file_location("ref_drift_functions",
                                                   ref / "ssms" / "basic_simulators" / "drift_functions.py")
     mod = importlib.util.module_from_spec(spec)

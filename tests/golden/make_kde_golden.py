@@ -21,10 +21,14 @@ def main():
     sys.path.insert(0, str(ROOT / "oracle" / "_ref"))
     from cssm.ddm_models import ddm_flexbound
 
-    sys.path.insert(0, "/root/reference")
+    sys.path.insert(0, str(HERE))
+    from make_adapter_golden import reference_root
+
+    ref_root = reference_root()
+    sys.path.insert(0, str(ref_root))
     import importlib.util
 
-    spec = importlib.util.spec_from_file_location("ref_kde", "/root/reference/ssms/support_utils/kde_class.py",
+    spec = importlib.util.spec_from_file_location("ref_kde", str(ref_root / "ssms" / "support_utils" / "kde_class.py"),
                                                   submodule_search_locations=None)
     # kde_class imports OMISSION_SENTINEL from ssms.basic_simulators.simulator; provide it
     import types
