@@ -51,6 +51,39 @@ WORKLOAD = ("ddm_flexbound angle boundary, 4096 theta ~ U(v[-3,3], a[0.3,3], z[0
 # two fused multiply-adds) -> 6; the step: bound, two compares, predicate,
 # position and time updates -> 5.5.  Total 22 lane-instructions.
 INSTR_PER_STEP = 22.0
+
+# The same accounting for the other benchmarked families, per accumulator-step
+# (lane-instructions, no block, queue or per-walk overhead).  A Gaussian
+# increment costs 16.5 (Philox 10.5 + Box-Muller 6, folded scale and drift);
+# the step of one accumulator against a constant bound costs 4.5 (two
+# compares, predicate, position and time updates), 5.5 against a moving bound.
+GAUSS_INCREMENT = 16.5
+INSTR_MIN = {
+    # constant bound: 16.5 + 4.5
+    "plain_ddm": (21.0, "Gaussian increment 16.5 + constant-bound step 4.5"),
+    "full_ddm": (21.0, "Gaussian increment 16.5 + constant-bound step 4.5 (per-walk draws amortised)"),
+    # the leaky update y (1 - g dt) + increment is one FFMA, like the plain add
+    "ornstein": (21.0, "Gaussian increment 16.5 + constant-bound step 4.5 (leak folded into one FFMA)"),
+    # drift table: one FFMA v(t) dt + increment, a 16-byte load per four steps
+    "conflict_ds": (22.25, "Gaussian increment 16.5 + constant-bound step 4.5 + drift-table FFMA 1 "
+                           "+ vector load 0.25"),
+    # two Philox words per stable variate (21), Chambers-Mallows-Stuck with
+    # reduced-angle polynomials: uniform and fold 5, W = -ln u 5, three
+    # polynomial sin/cos 23, three log2 + exponent + ex2 7, product, sign,
+    # clamp and NaN guard 6, scale FFMA 1 = 47; constant-bound step 4.5
+    "levy": (72.5, "Philox 21 (two words per variate) + CMS 47 + constant-bound step 4.5"),
+    # per accumulator: increment 16.5, add + clamp at 0 + threshold compare 3;
+    # per step over 4 accumulators: moving bound, time update and test,
+    # predicate 3.5 / 4
+    "race_no_bias_angle_4": (20.375, "Gaussian increment 16.5 + add, clamp, compare 3 + shared step 3.5/4"),
+    # per accumulator: increment 16.5, (x + (v - g x - b (S - x)) dt) + noise
+    # 5, clamp 1, compare 1; the sum S 3/4; per step the float64 time update,
+    # test and predicate 3 / 4
+    "lca_no_bias_4": (25.25, "Gaussian increment 16.5 + LCA update 5 + clamp, compare 2 + sum 0.75 "
+                             "+ shared step 3/4"),
+    # per accumulator: increment 16.5, add + compare 2; shared step 3.5 / 3
+    "racing_diffusion_3": (19.67, "Gaussian increment 16.5 + add, compare 2 + shared step 3.5/3"),
+}
 E2E_WINDOWS = 5
 N_SM = 148
 LANES_PER_SM_CLK = 128
@@ -360,6 +393,7 @@ def run_ours(args, rank, world, local_rank):
 
 SUR_MODEL = "angle"
 SUR_QUERIES_THETA, SUR_QUERIES_PER_THETA = 1000, 1000
+SUR_JUDGE_RUNS = 16                 # independent simulation + KDE runs averaged by the judge
 TANH_PER_EVAL = 100 + 100 + 120     # MUFU.TANH per forward evaluation
 MUFU_PER_SM_CLK = 16
 
@@ -396,7 +430,7 @@ def run_surrogate(args, clocks: dict) -> dict:
     # 10^6 uniform queries: 1000 theta x 1000 (rt, choice)
     _, xq = T.uniform_queries(SUR_MODEL, SUR_QUERIES_THETA, SUR_QUERIES_PER_THETA, seed=SEED + 2)
     clk = ClockSampler(0).__enter__()  # sampled over the whole evaluation (timed launches are short)
-    judge = T.judge(net, SUR_MODEL, xq, n_samples=100_000, seed=SEED + 3)
+    judge = T.judge(net, SUR_MODEL, xq, n_samples=100_000, seed=SEED + 3, runs=SUR_JUDGE_RUNS)
     n = xq.shape[0]
     xd = torch.from_numpy(xq).cuda()
     out = torch.empty(n, device="cuda")
@@ -465,7 +499,11 @@ def run_surrogate(args, clocks: dict) -> dict:
         "queries": n, "ms_per_forward": fwd_ms, "ms_per_forward_grad": grad_ms,
         "mae_vs_sim_kde_holdout_records": mae_hold,
         "mae_vs_sim_kde_uniform_queries": judge["mae"],
-        "sim_kde_vs_sim_kde_mae_uniform_queries": judge["kde_vs_kde_mae"],
+        "mae_gate": 0.05,
+        "judge": {"runs": judge["judge_runs"], "trajectories_per_theta_per_run": judge["n_samples"],
+                  "noise_mae": judge["judge_noise_mae"], "single_run_mae": judge["single_run_mae"],
+                  "what": "mean over runs of max(log-lik, lower bound) from independent simulation + KDE runs; "
+                          "noise_mae = two such judges from disjoint runs; single_run_mae = one run vs judge"},
         "mae_vs_exact_theta0": float(np.abs(clip(so) - clip(ex)).mean()),
         "sim_kde_mae_vs_exact_theta0": float(np.abs(clip(kd) - clip(ex)).mean()),
         "theta_grad_cosine_vs_exact_theta0": cos,
@@ -562,7 +600,7 @@ def _row_calls(prep: dict, rows: int, n: int, seed0: int) -> list:
     return calls
 
 
-def run_other_workloads(args) -> dict:
+def run_other_workloads(args, f_max: float = 1965e6) -> dict:
     """The mix workload (lca_no_bias_4, race_no_bias_angle_4, levy) and the
     plain DDM case: device throughput (inputs resident, one launch per step,
     CUDA events, L2 flushed), end to end through Simulator.simulate (host
@@ -613,13 +651,19 @@ def run_other_workloads(args) -> dict:
             if k >= args.warmup:
                 e2e.append(time.perf_counter() - t0)
         label = model if model != "ddm" else "plain_ddm"
+        acc_rate = steps * sb.n_acc / (dev_ms / 1e3)
         res[label] = {
             "simulator": name, "parameter_sets": sb.K, "n_samples": n, "trajectories": sb.total,
             "accumulators": sb.n_acc, "euler_steps": steps, "accumulator_steps": steps * sb.n_acc,
             "ms_per_launch": dev_ms, "trajectories_per_s": sb.total / (dev_ms / 1e3),
-            "accumulator_steps_per_s": steps * sb.n_acc / (dev_ms / 1e3),
+            "accumulator_steps_per_s": acc_rate,
             "e2e_trajectories_per_s": sb.total * len(e2e) / sum(e2e),
         }
+        if label in INSTR_MIN:
+            imin, basis = INSTR_MIN[label]
+            peak = N_SM * LANES_PER_SM_CLK * f_max / imin
+            res[label]["roofline"] = {"bound": "issue", "instr_min_per_accumulator_step": imin, "basis": basis,
+                                      "peak_accumulator_steps_per_s": peak, "frac": acc_rate / peak}
         if name in _REF_MODULE:
             cpu_jobs.append((label, name, prep, n))
         del sb, o
@@ -734,7 +778,7 @@ def main():
     if rank == 0 and world == 1 and not args.no_surrogate:
         line["surrogate"] = run_surrogate(args, line["clocks"])
     if rank == 0 and world == 1 and not args.no_other_workloads:
-        line["other_workloads"] = run_other_workloads(args)
+        line["other_workloads"] = run_other_workloads(args, (line["clocks"].get("sm_max_mhz") or 1965.0) * 1e6)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_record(theta, n_samples)
     if world > 1:
@@ -744,6 +788,19 @@ def main():
         torch.distributed.destroy_process_group()
     if rank == 0:
         print(json.dumps(line), flush=True)
+        if "surrogate" in line:
+            print(surrogate_summary(line["surrogate"]), flush=True)
+
+
+def surrogate_summary(sur: dict) -> str:
+    """One short line with the learned part's headline figures (it follows
+    the JSON line, which is long)."""
+    j = sur.get("judge", {})
+    return (f"surrogate: {sur['value']:.3e} evals/s = {sur['speedup_vs_sim_kde']:.0f}x simulation+KDE "
+            f"({sur['sim_kde_value']:.3e}/s); MAE {sur['mae_vs_sim_kde_uniform_queries']:.4f} vs sim+KDE judge "
+            f"(gate {sur.get('mae_gate', 0.05)}; judge noise {j.get('noise_mae', float('nan')):.4f} over "
+            f"{j.get('runs', '?')} runs; one run scores {j.get('single_run_mae', float('nan')):.4f}); "
+            f"theta-gradient cosines {sur.get('theta_grad_cosine_vs_exact_theta0')}")
 
 
 if __name__ == "__main__":

@@ -218,6 +218,30 @@ int ssm_ddm_flex(const float *v, const float *a, const float *z, const float *t,
                  int64_t traj_len, const ssm_launch *launch, void *workspace,
                  size_t workspace_bytes, void *stream);
 
+/*
+ * ssm_drift_table -- the drift table ssm_ddm_flex reads, evaluated on the
+ * device for the registered drift functions
+ * (ssms/basic_simulators/drift_functions.py; registry in
+ * ssms/config/_modelconfig/base.py).  Replaces the reference's per-trial
+ * host evaluation drift_fun(t=t_s, **params_k)
+ * (src/cssm/ddm_models.pyx:1063-1066) for the device-RNG path: one thread per
+ * (trial, time) entry with the reference's float32 / float64 operation order;
+ * values agree with numpy's to a few float32 ulps (the math library
+ * differs).  params: float32 [n_params][n_trials] in the registry's parameter
+ * order for `kind` (SSM_DRIFT_*); t_s: float32 [t_len], increasing; table:
+ * float32 [n_trials * stride], entries t_len .. stride-1 of each row zeroed.
+ */
+#define SSM_DRIFT_CONSTANT 0              /* v */
+#define SSM_DRIFT_GAMMA 1                 /* v, shape, scale, c */
+#define SSM_DRIFT_CONFLICT_DS 2           /* v, tinit, dinit, tslope, dslope, tfixedp, tcoh, dcoh */
+#define SSM_DRIFT_CONFLICT_DSSTIMFLEX 3   /* ... conflict_ds + tonset, donset (onsets relative to the first) */
+#define SSM_DRIFT_CONFLICT_STIMFLEX 4     /* v, vt, vd, tcoh, dcoh, tonset, donset */
+#define SSM_DRIFT_CONFLICT_STIMFLEXREL1 5 /* as STIMFLEX, onsets relative to the first */
+#define SSM_DRIFT_ATTEND 6                /* v, ptarget, pouter, pinner, r, sda */
+#define SSM_DRIFT_ATTEND_SIMPLE 7         /* v, ptarget, pouter, r, sda */
+int ssm_drift_table(int kind, const float *params, int n_params, int64_t n_trials, const float *t_s,
+                    int64_t t_len, float *table, int64_t stride, void *stream);
+
 /* ---- multi-accumulator race / LCA --------------------------------------- */
 
 /* Bytes of scratch ssm_race_model / ssm_lca need. */
@@ -400,7 +424,10 @@ int ssm_simulator_summary(const float *rts, const int32_t *choices, int64_t n_sa
  * loading this library holds until the process exits; n_trials above
  * SSM_STATIC_MAX_TRIALS is rejected with SSM_ERR_ARG.  The first call on a
  * device looks up the array's device address (cudaGetSymbolAddress) with that
- * device current, so make that first call before any stream capture.  Every
+ * device current, so make that first call before any stream capture.  The
+ * address is cached per device with the id of the CUDA context it belongs to;
+ * after a cudaDeviceReset (a new context) the next call looks it up again,
+ * and that call, too, belongs before any stream capture.  Every
  * call shares the one array: calls that overlap on the GPU (other streams,
  * other host threads) race and must be serialised by the caller.  Device-side
  * error flags of this variant are not reported; use the workspace form when

@@ -75,6 +75,7 @@ _SIGNATURES: dict[str, tuple] = {
     "ssm_ornstein_uhlenbeck": (_I, [_P, _P, _P, _P, _P, _P, _P, _I64, _I64, _P, _F, _F, _I, _P, _P, _P,
                                     _I64, _I64, _U64, _I, _P, _I64, _P, _P, _P, _P, _P, _I64, _P, _P,
                                     C.c_size_t, _P]),
+    "ssm_drift_table": (_I, [_I, _P, _I, _I64, _P, _I64, _P, _I64, _P]),
     "ssm_ddm_flex": (_I, [_P, _P, _P, _P, _P, _P, _I64, _I64, _P, _F, _F, _I, _P, _P, _P, _I64, _I64, _P, _I64,
                           _I64, _U64, _I, _P, _I64, _P, _P, _P, _P, _P, _I64, _P, _P, C.c_size_t, _P]),
     "ssm_race_workspace_bytes": (C.c_size_t, [_I64, _I]),

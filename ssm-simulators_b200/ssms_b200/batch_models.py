@@ -105,8 +105,12 @@ class SetBatch:
             if sim_name == "ddm_flex":
                 if not drift:
                     raise ValueError("ddm_flex needs the drift dict (drift_fun, drift_params)")
-                tab = dfn.drift_table(drift["drift_fun"], drift["drift_params"], K, bf.make_t_s(max_t, delta_t))
-                self.extra["drift_table"] = dev.padded_drift_table(tab)
+                t_s = bf.make_t_s(max_t, delta_t)
+                # registered drift functions are evaluated on the device, any other callable on the host
+                tab = dfn.device_drift_table(drift["drift_fun"], drift["drift_params"], K, t_s)
+                if tab is None:
+                    tab = dev.padded_drift_table(dfn.drift_table(drift["drift_fun"], drift["drift_params"], K, t_s))
+                self.extra["drift_table"] = tab
         elif sim_name in RACE:
             v = np.asarray(kwargs["v"], np.float32)
             self.n_acc = int(v.shape[1])

@@ -172,13 +172,18 @@ def ddm_flex(v, a, z, t, deadline, s, delta_t=0.001, max_t=20, n_samples=20000, 
              random_state=None, return_option="full", smooth_unif=False, n_threads=1, **kwargs):
     """DDM with flexible bounds and a time-varying drift v(t) = drift_fun(t,
     **drift_params) (src/cssm/ddm_models.pyx:884-1193).  The drift function is
-    evaluated per trial on the time grid (the reference's own procedure) into
-    the table the kernel reads; ``v`` is carried by the drift function."""
+    evaluated on the time grid into the table the kernel reads: on the device
+    for the registered drift functions, per trial on the host (the
+    reference's own procedure) for any other callable; ``v`` is carried by
+    the drift function."""
     _check_return_option(return_option)
     if drift_fun is None:
         raise TypeError("drift_fun is required")
     n_trials = int(n_trials)
-    table = dfn.drift_table(drift_fun, drift_params, n_trials, bf.make_t_s(max_t, delta_t))
+    t_s = bf.make_t_s(max_t, delta_t)
+    table = dfn.device_drift_table(drift_fun, drift_params, n_trials, t_s) if n_trials > 0 else None
+    if table is None:
+        table = dfn.drift_table(drift_fun, drift_params, n_trials, t_s)
     out = _run_flex("ddm_flex", v, a, z, t, deadline, s, None, max_t, delta_t, n_samples, n_trials,
                     boundary_fun, boundary_params, random_state, return_option, smooth_unif, kwargs,
                     drift_table=table)
@@ -186,7 +191,12 @@ def ddm_flex(v, a, z, t, deadline, s, delta_t=0.001, max_t=20, n_samples=20000, 
     meta["drift_fun_type"] = boundary_fun.__name__  # as the reference records it
     if return_option == "full":
         meta.update(drift_params)
-        meta["drift"] = table[-1].copy() if n_trials > 0 else np.zeros(table.shape[1], np.float32)
+        if n_trials == 0:
+            meta["drift"] = np.zeros(len(t_s), np.float32)
+        elif isinstance(table, np.ndarray):
+            meta["drift"] = table[-1].copy()
+        else:
+            meta["drift"] = table[-1].cpu().numpy()
     return out
 
 

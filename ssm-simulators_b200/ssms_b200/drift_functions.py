@@ -147,6 +147,51 @@ DRIFTS = {
 }
 
 
+#: registered drift functions the device evaluates (SSM_DRIFT_* in include/ssm_b200.h)
+DEVICE_KINDS = {"constant": 0, "gamma_drift": 1, "conflict_ds_drift": 2, "conflict_dsstimflex_drift": 3,
+                "conflict_stimflex_drift": 4, "conflict_stimflexrel1_drift": 5, "attend_drift": 6,
+                "attend_drift_simple": 7}
+
+
+def device_kind(drift_fun) -> tuple[int, list] | None:
+    """(SSM_DRIFT_* code, parameter names) when drift_fun is a registered
+    drift function the device evaluates, else None."""
+    for name, code in DEVICE_KINDS.items():
+        fun, names = DRIFTS[name]
+        if drift_fun is fun:
+            return code, names
+    return None
+
+
+def device_drift_table(drift_fun, drift_params: dict, n_trials: int, t_s: np.ndarray):
+    """The drift table of a registered drift function, evaluated on the
+    current CUDA device into a buffer whose rows are padded to a multiple of
+    8 floats (the [:, :len(t_s)] view is returned, as padded_drift_table
+    does for host tables); None for any other callable, whose table is
+    evaluated on the host as the reference does."""
+    hit = device_kind(drift_fun)
+    if hit is None:
+        return None
+    import torch
+
+    from . import _device as D
+    from . import _lib
+
+    code, names = hit
+    if set(drift_params) != set(names):  # other keywords (offsets, flags) keep the host evaluation
+        return None
+    K, n = int(n_trials), int(t_s.shape[0])
+    par = np.stack([np.broadcast_to(np.asarray(drift_params[k], np.float32).reshape(-1), (K,)) for k in names])
+    dev = D.require_cuda()
+    par_t = torch.from_numpy(np.ascontiguousarray(par)).to(dev)
+    ts_t = torch.from_numpy(np.ascontiguousarray(t_s, np.float32)).to(dev)
+    stride = (n + 7) // 8 * 8
+    buf = torch.empty((K, stride), dtype=torch.float32, device=dev)
+    _lib.check(_lib.lib().ssm_drift_table(code, D.ptr(par_t), len(names), K, D.ptr(ts_t), n, D.ptr(buf), stride,
+                                          D.stream_ptr()))
+    return buf[:, :n]
+
+
 def drift_table(drift_fun, drift_params: dict, n_trials: int, t_s: np.ndarray) -> np.ndarray:
     """float32 [n_trials, len(t_s)]: drift_fun evaluated on the time grid with
     each trial's parameters, as the reference evaluates it per trial."""

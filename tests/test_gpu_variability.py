@@ -176,6 +176,37 @@ def _flex_theta(rng, K):
     return th
 
 
+@pytest.mark.parametrize("drift", ["constant", "gamma_drift", "conflict_ds_drift", "conflict_dsstimflex_drift",
+                                   "conflict_stimflex_drift", "conflict_stimflexrel1_drift", "attend_drift",
+                                   "attend_drift_simple"])
+def test_device_drift_table_matches_host_table(cuda, drift):
+    """ssm_drift_table against the host evaluation (the reference's numpy
+    functions) on the 20 001-point grid: equal to a few float32 ulps, the
+    rows' padding zeroed; a callable outside the registry stays on the host."""
+    import torch
+
+    from ssms_b200 import drift_functions as dfn
+
+    rng = np.random.default_rng(zlib.crc32(f"devdrift/{drift}".encode()))
+    K = 48
+    th = _flex_theta(rng, K)
+    th["tonset"], th["donset"] = f32(rng.uniform(0, 1.5, K)), f32(rng.uniform(0, 1.5, K))
+    th["vt"], th["vd"] = f32(rng.uniform(-2, 2, K)), f32(rng.uniform(-2, 2, K))
+    dfun, dkeys = dfn.DRIFTS[drift]
+    dp = {k: th[k] for k in dkeys}
+    t_s = bf.make_t_s(20.0, 0.001)
+    host = dfn.drift_table(dfun, dp, K, t_s)
+    tab = dfn.device_drift_table(dfun, dp, K, t_s)
+    assert tab is not None and tuple(tab.shape) == host.shape and tab.stride(0) % 8 == 0
+    got = tab.cpu().numpy()
+    scale = 1.0 + np.abs(host).max(axis=1, keepdims=True)
+    assert np.all(np.abs(got - host) <= 4e-6 * scale), np.abs(got - host).max()
+    full = tab.as_strided((K, tab.stride(0)), (tab.stride(0), 1)).cpu().numpy()
+    assert np.all(full[:, host.shape[1]:] == 0.0)
+    assert dfn.device_drift_table(lambda t=None, **kw: np.zeros_like(t), {"v": th["v"]}, K, t_s) is None
+    assert dfn.device_drift_table(dfun, {**dp, "extra": th["v"]}, K, t_s) is None
+
+
 FLEX_CASES = [("constant", "constant"), ("gamma_drift", "angle"), ("conflict_ds_drift", "constant"),
               ("attend_drift", "angle"), ("attend_drift_simple", "constant")]
 
