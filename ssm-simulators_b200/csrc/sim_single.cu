@@ -21,6 +21,8 @@
 //  * Noise injection replaces the generator by caller rows and switches every
 //    float operation to explicit round-to-nearest intrinsics, giving results
 //    bit-identical to the sequential CPU restatement.
+#include <cuda.h>  // CUcontext / CUresult types of the driver entry points below
+
 #include <mutex>
 
 #include "common.cuh"
@@ -924,11 +926,49 @@ int ssm_ddm_flex(const float *v, const float *a, const float *z, const float *t,
 // ---------------------------------------------------------------------------
 // Allocation-free variant.  Its scratch is this file-scope device array; host
 // code must not hand the symbol itself to a kernel (in host code it names a
-// host-side stand-in), so the device address is looked up once per device.
+// host-side stand-in), so the device address is looked up with the device
+// current and cached per device together with the unique id of the CUDA
+// context it was looked up in.  A call under another context of that device
+// (after cudaDeviceReset, or a primary-context reset) looks the address up
+// again instead of reusing one from a context that no longer exists.
 namespace ssm {
 static __device__ __align__(256) unsigned char g_static_ws[SSM_STATIC_WS_BYTES];
 static std::mutex g_static_mu;
-static void *g_static_ptr[64] = {};
+struct StaticSlot {
+    unsigned long long ctx_id;  // 0: not looked up yet
+    void *ptr;
+};
+static StaticSlot g_static_slot[64] = {};
+
+using PfnCtxGetCurrent = CUresult (*)(CUcontext *);
+using PfnCtxGetId = CUresult (*)(CUcontext, unsigned long long *);
+
+// Unique id of the calling thread's current CUDA context (cuCtxGetId, CUDA
+// 12.0+, reached through the runtime's driver entry points); 0 when no context
+// is current or the driver does not offer the query.  Called under g_static_mu.
+static unsigned long long current_context_id() {
+    static bool resolved = false;
+    static PfnCtxGetCurrent get_current = nullptr;
+    static PfnCtxGetId get_id = nullptr;
+    if (!resolved) {
+        resolved = true;
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f, 12000, cudaEnableDefault, &q) ==
+                cudaSuccess && q == cudaDriverEntryPointSuccess)
+            get_current = reinterpret_cast<PfnCtxGetCurrent>(f);
+        f = nullptr;
+        q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetId", &f, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = reinterpret_cast<PfnCtxGetId>(f);
+    }
+    if (get_current == nullptr || get_id == nullptr) return 0;
+    CUcontext ctx = nullptr;
+    if (get_current(&ctx) != CUDA_SUCCESS || ctx == nullptr) return 0;
+    unsigned long long id = 0;
+    return get_id(ctx, &id) == CUDA_SUCCESS ? id : 0;
+}
 
 static int static_workspace(void **out) {
     int dev = 0;
@@ -938,13 +978,16 @@ static int static_workspace(void **out) {
         return SSM_ERR_ARG;
     }
     std::lock_guard<std::mutex> lock(g_static_mu);
-    if (g_static_ptr[dev] == nullptr) {
+    StaticSlot &slot = g_static_slot[dev];
+    const unsigned long long id = current_context_id();
+    if (slot.ctx_id == 0 || id != slot.ctx_id) {
         void *p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_static_ws);
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_static_ws);  // makes the device's context current
         if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_static_ws)");
-        g_static_ptr[dev] = p;
+        slot.ptr = p;
+        slot.ctx_id = current_context_id();
     }
-    *out = g_static_ptr[dev];
+    *out = slot.ptr;
     return SSM_OK;
 }
 }  // namespace ssm

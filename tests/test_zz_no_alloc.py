@@ -46,48 +46,76 @@ def _inputs(K, seed):
     return th
 
 
-def _call_static(fn, th, K, N, seed):
+def _call_static(fn, th, K, N, seed, offsets=None, launch=None):
+    """The allocation-free entry point; N samples per trial, or the ragged
+    layout when ``offsets`` (int64 [K+1] on the device) is given."""
     import torch
 
     from ssms_b200 import _lib
 
-    rts = torch.full((K * N,), float("nan"), device="cuda")
-    chs = torch.full((K * N,), 7, dtype=torch.int32, device="cuda")
-    steps = torch.full((K * N,), -1, dtype=torch.int32, device="cuda")
-    opt = _lib.SsmLaunch()
+    total = K * N if offsets is None else int(offsets[-1].item())
+    rts = torch.full((total,), float("nan"), device="cuda")
+    chs = torch.full((total,), 7, dtype=torch.int32, device="cuda")
+    steps = torch.full((total,), -1, dtype=torch.int32, device="cuda")
+    opt = _lib.SsmLaunch() if launch is None else launch
     st = fn(th["v"].data_ptr(), th["a"].data_ptr(), th["z"].data_ptr(), th["t"].data_ptr(),
-            th["deadline"].data_ptr(), th["s"].data_ptr(), K, N, None, 20.0, None, 0.001,
-            _lib.BOUND_LINEAR, th["slope"].data_ptr(), None, None, 0, 0, seed, 1, None, 0, None,
-            rts.data_ptr(), chs.data_ptr(), steps.data_ptr(), None, 0, ctypes.addressof(opt),
+            th["deadline"].data_ptr(), th["s"].data_ptr(), K, N, None if offsets is None else offsets.data_ptr(),
+            20.0, None, 0.001, _lib.BOUND_LINEAR, th["slope"].data_ptr(), None, None, 0, 0, seed, 1, None, 0,
+            None, rts.data_ptr(), chs.data_ptr(), steps.data_ptr(), None, 0, ctypes.addressof(opt),
             torch.cuda.current_stream().cuda_stream)
     _lib.check(st)
     torch.cuda.synchronize()
     return rts.cpu().numpy(), chs.cpu().numpy(), steps.cpu().numpy()
 
 
-def _call_workspace(th, K, N, seed):
+def _call_workspace(th, K, N, seed, offsets=None):
     from ssms_b200 import device as dev
 
     out = dev.simulate_single("ddm_flexbound", v=th["v"], z=th["z"], t=th["t"],
                               deadline=th["deadline"], s=th["s"], a=th["a"], n_trials=K,
-                              n_samples=N, max_t=20.0, delta_t=0.001, bound_kind=2,
-                              bound_p1=th["slope"], seed=seed, smooth_unif=True, want_steps=True)
+                              n_samples=N if offsets is None else 0, sample_offsets=offsets, max_t=20.0,
+                              delta_t=0.001, bound_kind=2, bound_p1=th["slope"], seed=seed, smooth_unif=True,
+                              want_steps=True)
     return out.rts.cpu().numpy(), out.choices.cpu().numpy(), out.steps.cpu().numpy()
 
 
+def _same(got, ref):
+    for a, b in zip(got, ref):
+        np.testing.assert_array_equal(a, b)  # same Philox streams: bit-identical
+    assert not np.isnan(got[0]).any() and np.all(got[2] >= 0)
+
+
 def test_static_entry_matches_workspace_entry_on_consecutive_calls():
+    """Calls in a row, each against the workspace form: two small dense
+    launches, one at exactly SSM_STATIC_MAX_TRIALS trials (the array's
+    header and per-trial rows fill it to the last byte), and a ragged launch
+    whose trials are processed longest-first through ``ssm_launch``."""
     import torch
+
+    from ssms_b200 import _device as D
+    from ssms_b200.batch import expected_walk_time, longest_first, with_order
 
     if not torch.cuda.is_available():
         pytest.skip("no CUDA device")
     _, fn = _entry()
-    for call, (K, N, seed) in enumerate([(64, 1000, 11), (200, 300, 12)]):
+    for call, (K, N, seed) in enumerate([(64, 1000, 11), (200, 300, 12), (MAX_TRIALS, 4, 13)]):
         th = _inputs(K, 100 + call)
-        got = _call_static(fn, th, K, N, seed)
-        ref = _call_workspace(th, K, N, seed)
-        for a, b in zip(got, ref):
-            np.testing.assert_array_equal(a, b)  # same Philox streams: bit-identical
-        assert not np.isnan(got[0]).any() and np.all(got[2] >= 0)
+        _same(_call_static(fn, th, K, N, seed), _call_workspace(th, K, N, seed))
+    # ragged sample counts (some trials empty), processed longest-first
+    K = 300
+    th = _inputs(K, 104)
+    ns = np.random.default_rng(5).integers(0, 600, K)
+    ns[[0, 7, 99]] = 0
+    offs = torch.from_numpy(np.concatenate([[0], np.cumsum(ns)]).astype(np.int64)).cuda()
+    host = {k: th[k].cpu().numpy() for k in ("v", "a", "z", "slope")}
+    est = expected_walk_time(host["v"], host["a"], host["z"], bound_kind=2, p1=host["slope"])
+    order, qoff = longest_first(est, ns)
+    ot, qt = torch.from_numpy(order).cuda(), torch.from_numpy(qoff).cuda()
+    launch = with_order(D.launch_opts(), ot, qt)
+    _same(_call_static(fn, th, K, 0, 14, offsets=offs, launch=launch), _call_workspace(th, K, 0, 14, offsets=offs))
+    # and once more at the full size after the ragged call (the array keeps the last call's contents)
+    th = _inputs(MAX_TRIALS, 105)
+    _same(_call_static(fn, th, MAX_TRIALS, 2, 15), _call_workspace(th, MAX_TRIALS, 2, 15))
 
 
 def test_static_entry_rejects_sizes_beyond_its_array():
