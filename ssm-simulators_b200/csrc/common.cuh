@@ -112,6 +112,20 @@ __device__ __forceinline__ float uniform_co(uint32_t x) {
     return (float)(x >> 8) * 5.9604645e-08f;  // 2^-24
 }
 
+// SFU approximations in their flush-to-zero forms.  Every argument the
+// generators pass is a normal float (uniforms are at least 2^-24, angles 0 or
+// at least 2^-21), for which these give the same results as the non-ftz
+// forms, without the extra instructions that rescale subnormal inputs.
+__device__ __forceinline__ float lg2_ftz(float x) {
+    float y;
+    asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ void sincos_ftz(float x, float &s, float &c) {
+    asm("sin.approx.ftz.f32 %0, %1;" : "=f"(s) : "f"(x));
+    asm("cos.approx.ftz.f32 %0, %1;" : "=f"(c) : "f"(x));
+}
+
 // Box-Muller transform of two 32-bit words into two N(0,1) variates
 // (r = sqrt(-2 ln u1), phase 2 pi u2).  Uses the SFU approximations of log2,
 // rsqrt, sin and cos: 4 MUFU operations per pair.

@@ -27,6 +27,22 @@
 
 #include "common.cuh"
 
+#ifndef SSM_EXP_FTZ
+#define SSM_EXP_FTZ 0
+#endif
+#ifndef SSM_EXP_TBLOCK
+#define SSM_EXP_TBLOCK 0
+#endif
+#ifndef SSM_EXP_SIX
+#define SSM_EXP_SIX 0
+#endif
+#ifndef SSM_EXP_SIX_BLK
+#define SSM_EXP_SIX_BLK 48
+#endif
+#ifndef SSM_EXP_MINCTAS
+#define SSM_EXP_MINCTAS 3
+#endif
+
 
 
 
@@ -270,11 +286,11 @@ __device__ __forceinline__ float cms_stable(uint32_t bu, uint32_t bw, const Tria
 // blocks measured 8 % slower there).  The Gaussian counter of call h of block
 // b is (BLK/4) b + h, so those streams do not depend on the block size.
 template <int MODEL> struct Blk {
-    static constexpr int value = (MODEL == M_LEVY) ? 8 : (MODEL == M_DFLEX ? 16 : 32);
+    static constexpr int value = (MODEL == M_LEVY) ? 8 : (MODEL == M_DFLEX ? 16 : (SSM_EXP_SIX ? SSM_EXP_SIX_BLK : 32));
 };
 // Resident 256-thread CTAs per SM the compiler must fit (register cap
 // 65536 / (256 n)): 3 (80 registers) for blocks longer than 8 steps, 4 otherwise.
-template <int MODEL> struct MinCtas { static constexpr int value = Blk<MODEL>::value > 8 ? 3 : 4; };
+template <int MODEL> struct MinCtas { static constexpr int value = Blk<MODEL>::value > 8 ? SSM_EXP_MINCTAS : 4; };
 
 struct Lane {
     int64_t w;
@@ -294,14 +310,46 @@ __device__ __forceinline__ void bm_increment(uint32_t a, uint32_t b, float c2, f
                                              float &g0, float &g1) {
     const float u1 = __uint_as_float(0x3f800000u | (a & 0x007fffffu)) - 0.99999994f;  // (0, 1)
     const float ang = fmaf(__uint_as_float(0x3f800000u | (b & 0x007fffffu)), 6.2831853f, -6.2831853f);
+#if SSM_EXP_FTZ
+    const float e = c2 * lg2_ftz(u1);
+#else
     const float e = c2 * __log2f(u1);
+#endif
     float r;
     asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(e));
     float sn, cs;
+#if SSM_EXP_FTZ
+    sincos_ftz(ang, sn, cs);
+#else
     __sincosf(ang, &sn, &cs);
+#endif
     g0 = fmaf(r, cs, drift);
     g1 = fmaf(r, sn, drift);
 }
+
+#if SSM_EXP_SIX
+// Six increments from one Philox call (128 bits): three Box-Muller pairs whose
+// radii take 23-bit uniforms from the low bits of x, y and z, and whose phases
+// take the low 23 bits of w, and 18 bits each from the top nine bits of (w, x)
+// and of (y, z).
+__device__ __forceinline__ void bm6_increment(uint4 b, float c2, float drift, float *g) {
+    const uint32_t rad[3] = {b.x, b.y, b.z};
+    const uint32_t ph[3] = {b.w & 0x007fffffu, ((b.w >> 9) & 0x7fc000u) | ((b.x >> 18) & 0x3fe0u),
+                            ((b.y >> 9) & 0x7fc000u) | ((b.z >> 18) & 0x3fe0u)};
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        const float u1 = __uint_as_float(0x3f800000u | (rad[i] & 0x007fffffu)) - 0.99999994f;  // (0, 1)
+        const float ang = fmaf(__uint_as_float(0x3f800000u | ph[i]), 6.2831853f, -6.2831853f);
+        const float e = c2 * lg2_ftz(u1);
+        float r;
+        asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(e));
+        float sn, cs;
+        sincos_ftz(ang, sn, cs);
+        g[2 * i] = fmaf(r, cs, drift);
+        g[2 * i + 1] = fmaf(r, sn, drift);
+    }
+}
+#endif
 
 // The block's increments.  Noise injection returns the raw caller draws (the
 // step applies drift and scale with explicit rounding); the device RNG returns
@@ -326,6 +374,17 @@ __device__ __forceinline__ void draw_block(const SingleParams &p, const Lane &L,
             g[2 * h + 2] = fmaf(r.scale, cms_stable(c.x, c.y, r), r.drift);
             g[2 * h + 3] = fmaf(r.scale, cms_stable(c.z, c.w, r), r.drift);
         }
+    } else if (SSM_EXP_SIX && MODEL != M_DFLEX) {
+#if SSM_EXP_SIX
+        const float drift = DrawnDrift<MODEL>::value ? L.dinc : r.drift;
+        static_assert(MODEL == M_LEVY || MODEL == M_DFLEX || BLK % 6 == 0, "six increments per Philox call");
+#pragma unroll
+        for (int h = 0; h < BLK / 6; ++h) {
+            const uint4 b = philox10(make_uint4((uint32_t)(BLK / 6) * L.blk + (uint32_t)h, L.n, L.k + p.k_base, 0u),
+                                     p.key);
+            bm6_increment(b, r.c2, drift, g + 6 * h);
+        }
+#endif
     } else {
         const float drift = DrawnDrift<MODEL>::value ? L.dinc : (MODEL == M_DFLEX ? 0.f : r.drift);
 #pragma unroll
@@ -342,7 +401,7 @@ __device__ __forceinline__ void draw_block(const SingleParams &p, const Lane &L,
 // reference's `while` condition (ddm_models.pyx:719; legacy DDM :451); once it
 // fails the remaining steps of the block are predicated off.  Returns whether
 // the walk is still running.
-template <int MODEL, int BOUND, bool NOISE, bool RECORD>
+template <int MODEL, int BOUND, bool NOISE, bool RECORD, bool TCHK = true>
 __device__ __forceinline__ bool step_block(const SingleParams &p, Lane &L, const TrialRow &r,
                                            const float g[Blk<MODEL>::value]) {
     constexpr int BLK = Blk<MODEL>::value;
@@ -380,14 +439,16 @@ __device__ __forceinline__ bool step_block(const SingleParams &p, Lane &L, const
 #pragma unroll
     for (int q = 0; q < BLK; ++q) {
         bool inside;
+        // the time test; a block whose every step is known to pass it skips it (TCHK false)
+        const bool in_time = !TCHK || (L.tp <= r.dl_tmp);
         if (MODEL == M_LEGACY) {
-            inside = live && (L.y <= r.a) && (L.y >= 0.f) && (L.tp <= r.dl_tmp);
+            inside = live && (L.y <= r.a) && (L.y >= 0.f) && in_time;
         } else {
             float b;
             if (INT_IX) b = bound_at<BOUND, NOISE>(r, L.ixf, L.ix, p, L.k);
             else if (BOUND == SSM_BOUND_LINEAR) b = (q == 0) ? b0 : fmaf((float)q, r.dtp1, b0);
             else b = bound_at<BOUND, NOISE>(r, ixf0 + (float)q, 0, p, L.k);
-            inside = live && (fabsf(L.y) <= b) && (L.tp <= r.dl_tmp);
+            inside = live && (fabsf(L.y) <= b) && in_time;
         }
         if (NOISE && inside && L.ix + (DrawnDrift<MODEL>::value ? 1 : 0) >= p.nlen) {
             raise_error(p.hdr, SSM_ERR_NOISE_RANGE, (int)L.w);
@@ -426,6 +487,20 @@ __device__ __forceinline__ bool step_block(const SingleParams &p, Lane &L, const
     }
     if (!INT_IX) L.ixf = ixf0 + (float)BLK;
     return live;
+}
+
+// True when all BLK time tests of the lane's next block are known to pass
+// (device RNG, in-register bounds only).  Step q of the block tests the float
+// accumulator after q more additions of dt, at most t + (BLK-1) dt plus the
+// additions' rounding; below 65536 dt an ulp of t is at most dt/64, so that
+// rounding stays under dt/4, and t + (BLK+1) dt <= dl_tmp, evaluated in float,
+// leaves more than that margin.
+template <int MODEL, int BOUND, bool NOISE>
+__device__ __forceinline__ bool block_in_time(const SingleParams &p, const Lane &L, const TrialRow &r) {
+    constexpr bool INT_IX = NOISE || BOUND == SSM_BOUND_TABLE || MODEL == M_DFLEX;
+    if (INT_IX) return false;
+    constexpr float SPAN = (float)(Blk<MODEL>::value + 1);
+    return (L.tp < p.dt * 65536.f) && (fmaf(SPAN, p.dt, L.tp) <= r.dl_tmp);
 }
 
 // Steps taken by a walk that has ended.  Without an integer index L.ixf
@@ -534,6 +609,27 @@ __device__ __forceinline__ bool lane_init(const SingleParams &p, Lane &L, TrialR
 }
 
 // ------------------------------------------------------------------ main kernel
+#ifndef SSM_EXP_COMPACT
+#define SSM_EXP_COMPACT 0
+#endif
+
+// CTA barrier without the .aligned guarantee: warps reach the drain phase's
+// barriers at different times, each when it has seen the queue empty.
+__device__ __forceinline__ void cta_barrier() { asm volatile("barrier.sync 0;" ::: "memory"); }
+
+// Each warp runs three phases.
+//  CLAIM: lanes take trajectories from the global work counter (batched
+//    restarts, see above) until the warp finds the counter past the end.
+//  WAIT: the warp steps its own walks until every warp of the CTA has found
+//    the queue empty (a shared counter); a warp with nothing to step sleeps.
+//  DRAIN (SSM_EXP_COMPACT): block-synchronous over the CTA.  Before each
+//    block the CTA counts its surviving walks and, when they occupy more
+//    warps than needed, re-deals them through shared memory -- round-robin
+//    over the first four warps (one per SM sub-partition) while they fit,
+//    densely otherwise -- so the last long walks share a few warps instead of
+//    crawling along in many sparse ones.
+// Without SSM_EXP_COMPACT a warp leaves as soon as the queue is empty and its
+// own walks have ended.
 template <int MODEL, int BOUND, bool NOISE>
 __global__ void __launch_bounds__(256, MinCtas<MODEL>::value) k_single(const __grid_constant__ SingleParams p) {
     const unsigned FULL = 0xffffffffu;
@@ -541,6 +637,17 @@ __global__ void __launch_bounds__(256, MinCtas<MODEL>::value) k_single(const __g
     const unsigned lt_mask = (1u << lane) - 1u;
     const int64_t total = (p.total >= 0) ? p.total : __ldg(p.offsets + p.n_trials) - __ldg(p.offsets);
     const int64_t chunk = warp_chunk(p.chunk, total);
+#if SSM_EXP_COMPACT
+    const int warp = threadIdx.x >> 5;
+    const int nwarps = blockDim.x >> 5;
+    __shared__ int s_exhausted;  // warps of this CTA that found the queue empty
+    __shared__ int s_count[8];   // live walks per warp (drain phase)
+    __shared__ Lane s_walk[256]; // walks being re-dealt (drain phase)
+    if (threadIdx.x == 0) s_exhausted = 0;
+    __syncthreads();
+    int phase = 0;  // 0 claim, 1 wait, 2 drain (warp-uniform)
+    unsigned naps = 0;
+#endif
 
     Lane L;
     TrialRow r;
@@ -551,43 +658,112 @@ __global__ void __launch_bounds__(256, MinCtas<MODEL>::value) k_single(const __g
     int64_t q_next = 0, q_end = 0, hint = 0;
 
     for (;;) {
-        // Lanes whose walk ended wait (predicated off) until refill_min of
-        // them have: finishing and restarting lanes runs divergently, with the
-        // rest of the warp idle, so it is done for several lanes in one pass.
-        // Once the queue is empty, pending results are written at once.
-        const unsigned need = __ballot_sync(FULL, !active);
-        const bool pass = exhausted ? (__ballot_sync(FULL, pending) != 0u) : (__popc(need) >= p.refill_min);
-        if (pass && pending) {
-            finalize<MODEL, BOUND, NOISE>(p, L);
-            pending = false;
+#if SSM_EXP_COMPACT
+        if (phase == 2) {
+            cta_barrier();
+            if (pending) {
+                finalize<MODEL, BOUND, NOISE>(p, L);
+                pending = false;
+            }
+            const unsigned live = __ballot_sync(FULL, active);
+            if (lane == 0) s_count[warp] = __popc(live);
+            cta_barrier();
+            int T = 0, before = 0, busy = 0;
+            for (int i = 0; i < nwarps; ++i) {
+                const int c = s_count[i];
+                before += (i < warp) ? c : 0;
+                T += c;
+                busy += (c > 0) ? 1 : 0;
+            }
+            if (T == 0) break;  // CTA-uniform
+            const int spread = nwarps < 4 ? nwarps : 4;
+            const int want = (T <= 32 * spread) ? spread : (T + 31) >> 5;
+            if (busy > want) {  // CTA-uniform: re-deal walk j to warp j % want, lane j / want
+                if (active) s_walk[before + __popc(live & lt_mask)] = L;
+                cta_barrier();
+                const int j = lane * want + warp;
+                active = (warp < want) && (j < T);
+                if (active) {
+                    L = s_walk[j];
+                    const float4 *src = reinterpret_cast<const float4 *>(p.rows + L.k);
+                    float4 *dst = reinterpret_cast<float4 *>(&r);
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) dst[i] = __ldg(src + i);
+                }
+            }
+        } else
+#endif
+        {
+            // Lanes whose walk ended wait (predicated off) until refill_min of
+            // them have: finishing and restarting lanes runs divergently, with the
+            // rest of the warp idle, so it is done for several lanes in one pass.
+            // Once the queue is empty, pending results are written at once.
+            const unsigned need = __ballot_sync(FULL, !active);
+            const bool pass = exhausted ? (__ballot_sync(FULL, pending) != 0u) : (__popc(need) >= p.refill_min);
+            if (pass && pending) {
+                finalize<MODEL, BOUND, NOISE>(p, L);
+                pending = false;
+            }
+            if (pass && !exhausted) {
+                const int cnt = __popc(need);
+                const int64_t avail = q_end - q_next;
+                int64_t base = 0;
+                if (avail < cnt) {
+                    unsigned long long b = 0ull;
+                    if (lane == 0) b = atomicAdd(&p.hdr->counter, (unsigned long long)chunk);
+                    base = (int64_t)__shfl_sync(FULL, b, 0);
+                    if (base >= total) exhausted = true;
+                }
+                if (!active) {
+                    const int rank = __popc(need & lt_mask);
+                    const int64_t w = (rank < avail) ? q_next + rank : base + (rank - avail);
+                    if (w < total) active = lane_init<MODEL, NOISE>(p, L, r, w, hint);
+                }
+                if (avail >= cnt) {
+                    q_next += cnt;
+                } else {
+                    q_next = base + (cnt - avail);
+                    q_end = base + chunk;
+                }
+                if (q_next >= total) exhausted = true;  // nothing left for this warp to hand out
+            }
+#if SSM_EXP_COMPACT
+            if (phase == 0 && exhausted) {
+                phase = 1;
+                if (lane == 0) atomicAdd(&s_exhausted, 1);
+            }
+            if (phase == 1 && *(volatile int *)&s_exhausted >= nwarps) {
+                phase = 2;
+                continue;
+            }
+            if (__ballot_sync(FULL, active) == 0u) {
+                if (phase == 1) {
+                    // nothing to step until the CTA's other warps find the queue
+                    // empty (their walks are bounded by the step cap); the wait is
+                    // bounded too, after which the drain phase is entered anyway
+                    __nanosleep(200);
+                    if (++naps > (1u << 24)) {
+                        if (lane == 0) raise_error(p.hdr, SSM_ERR_DEVICE, -1);
+                        phase = 2;
+                    }
+                }
+                continue;
+            }
+#else
+            if (__ballot_sync(FULL, active) == 0u) break;
+#endif
         }
-        if (pass && !exhausted) {
-            const int cnt = __popc(need);
-            const int64_t avail = q_end - q_next;
-            int64_t base = 0;
-            if (avail < cnt) {
-                unsigned long long b = 0ull;
-                if (lane == 0) b = atomicAdd(&p.hdr->counter, (unsigned long long)chunk);
-                base = (int64_t)__shfl_sync(FULL, b, 0);
-                if (base >= total) exhausted = true;
-            }
-            if (!active) {
-                const int rank = __popc(need & lt_mask);
-                const int64_t w = (rank < avail) ? q_next + rank : base + (rank - avail);
-                if (w < total) active = lane_init<MODEL, NOISE>(p, L, r, w, hint);
-            }
-            if (avail >= cnt) {
-                q_next += cnt;
-            } else {
-                q_next = base + (cnt - avail);
-                q_end = base + chunk;
-            }
-        }
-        if (__ballot_sync(FULL, active) == 0u) break;
+#if SSM_EXP_TBLOCK
+        // warp-uniform: skip the per-step time test when no active lane can reach its limit in this block
+        const bool skip_time = __all_sync(FULL, !active || block_in_time<MODEL, BOUND, NOISE>(p, L, r));
+#else
+        const bool skip_time = false;
+#endif
         if (active) {
             float g[Blk<MODEL>::value];
             draw_block<MODEL, NOISE>(p, L, r, g);
-            const bool live = step_block<MODEL, BOUND, NOISE, false>(p, L, r, g);
+            const bool live = skip_time ? step_block<MODEL, BOUND, NOISE, false, false>(p, L, r, g)
+                                        : step_block<MODEL, BOUND, NOISE, false, true>(p, L, r, g);
             L.blk += 1;
             if (!live) {
                 active = false;
