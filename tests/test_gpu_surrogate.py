@@ -2,10 +2,16 @@
 analytic DDM density, its theta-gradient against finite differences and the
 analytic gradient, and what it gains over simulation + KDE.
 
-A network is trained once per module on device-generated records -- the full
-training-data configuration: 100000 ddm_angle parameter sets x 100000
-trajectories, 1000 records each, 30 epochs -- by the device kernels; this
-takes under a minute on one B200."""
+A network is trained once per module on device-generated records -- the
+training-data configuration of the benchmark: 100000 ddm_angle parameter sets
+x 100000 trajectories, 1000 records each (800 KDE resamples, 200 uniform
+rts), 30 epochs -- by the device kernels; this takes under a minute on one
+B200.
+
+The judge of the 0.05 mean-absolute-error gate is the average of 16
+independent simulation + KDE estimates per query (each raised to the label
+floor log(1e-7)): two such judges from disjoint runs differ by about 0.026,
+while a single simulation + KDE run differs from the judge by about 0.07."""
 
 import numpy as np
 import pytest
@@ -17,6 +23,8 @@ from ssms_b200 import surrogate as S
 from ssms_b200 import surrogate_train as T
 
 pytestmark = pytest.mark.gpu
+
+MAE_GATE = 0.05
 
 
 @pytest.fixture(scope="module")
@@ -45,12 +53,13 @@ def _slices():
 
 def test_error_against_simulation_kde(trained):
     net, hold = trained
-    assert net.mae(hold) < 0.05           # held-out records, labels clipped at log(1e-7)
+    assert net.mae(hold) < MAE_GATE           # held-out records, labels clipped at log(1e-7)
     _, xq = T.uniform_queries("angle", 200, 1000, seed=5)
-    j = T.judge(net, "angle", xq, n_samples=100_000, seed=7)
-    # uniform queries: within the judge's own run-to-run noise (two independent
-    # simulation + KDE runs differ by kde_vs_kde_mae)
-    assert j["mae"] < 1.2 * j["kde_vs_kde_mae"], j
+    j = T.judge(net, "angle", xq, n_samples=100_000, seed=7, runs=16)
+    print(j)
+    assert j["judge_noise_mae"] < 0.5 * MAE_GATE, j  # the judge resolves the gate
+    assert j["mae"] < MAE_GATE, j                    # uniform (theta, rt in [0, 20], choice) queries
+    assert j["mae"] < j["single_run_mae"], j         # closer to the judge than one simulation + KDE run
 
 
 def test_gain_over_simulation_kde(trained):
@@ -67,7 +76,7 @@ def test_gain_over_simulation_kde(trained):
     kde = S.kde_loglik("angle", x[:, :5], x[:, 5], x[:, 6], n_samples=100_000, seed=3)
     e_sur = np.abs(clip(sur) - clip(exact)).mean()
     e_kde = np.abs(clip(kde) - clip(exact)).mean()
-    assert e_sur < 1.25 * e_kde, (e_sur, e_kde)
+    assert e_sur < e_kde, (e_sur, e_kde)
     _, xq = T.uniform_queries("angle", 200, 1000, seed=9)
     fast = T.time_surrogate(net, xq, want_dx=False, reps=10)
     slow = T.time_sim_kde("angle", xq, n_samples=100_000, seed=4)
@@ -75,6 +84,14 @@ def test_gain_over_simulation_kde(trained):
 
 
 def test_theta_gradient_against_analytic_gradient(trained):
+    """d loglik / d theta of the backward kernel against the analytic
+    float64 DDM gradient on theta = 0 slices, where the exact log-density is
+    above -8.  v, a and z everywhere there; t past the mode of each slice's
+    density.  Before the mode, d/dt of the exact density follows its steep
+    leading edge, which the training labels do not have: the KDE smooths log
+    rt with a Silverman bandwidth of about 0.1-0.2, so the surrogate (and
+    simulation + KDE itself) rises more gently there and its d/dt is smaller
+    (cosine about 0.73 over the whole core, 0.998 past the mode)."""
     net, _ = trained
     x = _slices()
     exact = NO.ddm_loglik(x[:, 5].astype(np.float64), x[:, 6], x[:, 0].astype(np.float64),
@@ -86,10 +103,13 @@ def test_theta_gradient_against_analytic_gradient(trained):
     ll.sum().backward()
     d = th.grad.double().cpu().numpy()
     core = np.isfinite(exact) & (exact > -8)
-    for j in range(3):  # v, a, z
-        a1, b1 = d[core, j], g[core, j]
+    ex = np.nan_to_num(exact, neginf=-1e9).reshape(-1, 200)  # 200 rts per slice
+    past_mode = (np.arange(200)[None, :] > ex.argmax(axis=1)[:, None]).reshape(-1)
+    for j, region in ((0, core), (1, core), (2, core), (3, core & past_mode)):
+        a1, b1 = d[region, j], g[region, j]
         cos = a1 @ b1 / np.linalg.norm(a1) / np.linalg.norm(b1)
-        assert cos > 0.9, ("vaz"[j], cos)
+        print("vazt"[j], cos, int(region.sum()))
+        assert cos > (0.9 if j < 3 else 0.97), ("vazt"[j], cos)
 
 
 def test_theta_gradient_against_finite_differences(trained):
