@@ -128,14 +128,15 @@ __device__ __forceinline__ void sincos_ftz(float x, float &s, float &c) {
 
 // Box-Muller transform of two 32-bit words into two N(0,1) variates
 // (r = sqrt(-2 ln u1), phase 2 pi u2).  Uses the SFU approximations of log2,
-// rsqrt, sin and cos: 4 MUFU operations per pair.
+// rsqrt, sin and cos: 4 MUFU operations per pair (u1 >= 2^-24 and the phase
+// is 0 or at least 2 pi 2^-23: normal floats, so the ftz forms apply).
 __device__ __forceinline__ float2 box_muller(uint32_t a, uint32_t b) {
     const float u1 = uniform_open(a);
     const float u2 = bits_to_1_2(b) - 1.0f;
-    const float e = -1.3862944f * __log2f(u1);  // -2 ln u1 > 0
+    const float e = -1.3862944f * lg2_ftz(u1);  // -2 ln u1 > 0
     const float r = e * rsqrtf(e);
     float s, c;
-    __sincosf(6.2831853f * u2, &s, &c);
+    sincos_ftz(6.2831853f * u2, s, c);
     return make_float2(r * c, r * s);
 }
 

@@ -27,12 +27,6 @@
 
 #include "common.cuh"
 
-#ifndef SSM_EXP_FTZ
-#define SSM_EXP_FTZ 0
-#endif
-#ifndef SSM_EXP_TBLOCK
-#define SSM_EXP_TBLOCK 0
-#endif
 #ifndef SSM_EXP_SIX
 #define SSM_EXP_SIX 0
 #endif
@@ -248,7 +242,7 @@ __device__ __forceinline__ float cms_stable(uint32_t bu, uint32_t bw, const Tria
     const float m = fmaxf(0.5f - fabsf(u01 - 0.5f), 3.1830988e-08f);  // V >= 1e-7 (the U clamp)
     const float V = 3.14159265f * m;
     const float aU = 1.57079633f - V;  // |U|
-    const float W = fmaxf(-__logf(uniform_open(bw)), 1e-10f);
+    const float W = fmaxf(-0.69314718f * lg2_ftz(uniform_open(bw)), 1e-10f);
     float X;
     if (r.alpha == 1.0f) {
         X = cos_q(V) / sin_q(V);  // |tan U|
@@ -264,7 +258,7 @@ __device__ __forceinline__ float cms_stable(uint32_t bu, uint32_t bw, const Tria
         // which does not cancel as alpha -> 2
         float A = r.alpha * aU;
         if (A > 1.57079633f) A = fmaf(r.alpha, V, 3.14159265f * fmaf(-0.5f, r.alpha, 1.0f));
-        const float e = fmaf(r.expo, __log2f(cua) - __log2f(W), -r.inv_alpha * __log2f(cu));
+        const float e = fmaf(r.expo, lg2_ftz(cua) - lg2_ftz(W), -r.inv_alpha * lg2_ftz(cu));
         float p2;
         asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(p2) : "f"(e));
         X = sin_q(A) * p2;  // |sin(alpha U)| ...
@@ -310,19 +304,11 @@ __device__ __forceinline__ void bm_increment(uint32_t a, uint32_t b, float c2, f
                                              float &g0, float &g1) {
     const float u1 = __uint_as_float(0x3f800000u | (a & 0x007fffffu)) - 0.99999994f;  // (0, 1)
     const float ang = fmaf(__uint_as_float(0x3f800000u | (b & 0x007fffffu)), 6.2831853f, -6.2831853f);
-#if SSM_EXP_FTZ
     const float e = c2 * lg2_ftz(u1);
-#else
-    const float e = c2 * __log2f(u1);
-#endif
     float r;
     asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(e));
     float sn, cs;
-#if SSM_EXP_FTZ
     sincos_ftz(ang, sn, cs);
-#else
-    __sincosf(ang, &sn, &cs);
-#endif
     g0 = fmaf(r, cs, drift);
     g1 = fmaf(r, sn, drift);
 }
@@ -609,27 +595,6 @@ __device__ __forceinline__ bool lane_init(const SingleParams &p, Lane &L, TrialR
 }
 
 // ------------------------------------------------------------------ main kernel
-#ifndef SSM_EXP_COMPACT
-#define SSM_EXP_COMPACT 0
-#endif
-
-// CTA barrier without the .aligned guarantee: warps reach the drain phase's
-// barriers at different times, each when it has seen the queue empty.
-__device__ __forceinline__ void cta_barrier() { asm volatile("barrier.sync 0;" ::: "memory"); }
-
-// Each warp runs three phases.
-//  CLAIM: lanes take trajectories from the global work counter (batched
-//    restarts, see above) until the warp finds the counter past the end.
-//  WAIT: the warp steps its own walks until every warp of the CTA has found
-//    the queue empty (a shared counter); a warp with nothing to step sleeps.
-//  DRAIN (SSM_EXP_COMPACT): block-synchronous over the CTA.  Before each
-//    block the CTA counts its surviving walks and, when they occupy more
-//    warps than needed, re-deals them through shared memory -- round-robin
-//    over the first four warps (one per SM sub-partition) while they fit,
-//    densely otherwise -- so the last long walks share a few warps instead of
-//    crawling along in many sparse ones.
-// Without SSM_EXP_COMPACT a warp leaves as soon as the queue is empty and its
-// own walks have ended.
 template <int MODEL, int BOUND, bool NOISE>
 __global__ void __launch_bounds__(256, MinCtas<MODEL>::value) k_single(const __grid_constant__ SingleParams p) {
     const unsigned FULL = 0xffffffffu;
@@ -637,17 +602,6 @@ __global__ void __launch_bounds__(256, MinCtas<MODEL>::value) k_single(const __g
     const unsigned lt_mask = (1u << lane) - 1u;
     const int64_t total = (p.total >= 0) ? p.total : __ldg(p.offsets + p.n_trials) - __ldg(p.offsets);
     const int64_t chunk = warp_chunk(p.chunk, total);
-#if SSM_EXP_COMPACT
-    const int warp = threadIdx.x >> 5;
-    const int nwarps = blockDim.x >> 5;
-    __shared__ int s_exhausted;  // warps of this CTA that found the queue empty
-    __shared__ int s_count[8];   // live walks per warp (drain phase)
-    __shared__ Lane s_walk[256]; // walks being re-dealt (drain phase)
-    if (threadIdx.x == 0) s_exhausted = 0;
-    __syncthreads();
-    int phase = 0;  // 0 claim, 1 wait, 2 drain (warp-uniform)
-    unsigned naps = 0;
-#endif
 
     Lane L;
     TrialRow r;
@@ -658,107 +612,41 @@ __global__ void __launch_bounds__(256, MinCtas<MODEL>::value) k_single(const __g
     int64_t q_next = 0, q_end = 0, hint = 0;
 
     for (;;) {
-#if SSM_EXP_COMPACT
-        if (phase == 2) {
-            cta_barrier();
-            if (pending) {
-                finalize<MODEL, BOUND, NOISE>(p, L);
-                pending = false;
-            }
-            const unsigned live = __ballot_sync(FULL, active);
-            if (lane == 0) s_count[warp] = __popc(live);
-            cta_barrier();
-            int T = 0, before = 0, busy = 0;
-            for (int i = 0; i < nwarps; ++i) {
-                const int c = s_count[i];
-                before += (i < warp) ? c : 0;
-                T += c;
-                busy += (c > 0) ? 1 : 0;
-            }
-            if (T == 0) break;  // CTA-uniform
-            const int spread = nwarps < 4 ? nwarps : 4;
-            const int want = (T <= 32 * spread) ? spread : (T + 31) >> 5;
-            if (busy > want) {  // CTA-uniform: re-deal walk j to warp j % want, lane j / want
-                if (active) s_walk[before + __popc(live & lt_mask)] = L;
-                cta_barrier();
-                const int j = lane * want + warp;
-                active = (warp < want) && (j < T);
-                if (active) {
-                    L = s_walk[j];
-                    const float4 *src = reinterpret_cast<const float4 *>(p.rows + L.k);
-                    float4 *dst = reinterpret_cast<float4 *>(&r);
-#pragma unroll
-                    for (int i = 0; i < 4; ++i) dst[i] = __ldg(src + i);
-                }
-            }
-        } else
-#endif
-        {
-            // Lanes whose walk ended wait (predicated off) until refill_min of
-            // them have: finishing and restarting lanes runs divergently, with the
-            // rest of the warp idle, so it is done for several lanes in one pass.
-            // Once the queue is empty, pending results are written at once.
-            const unsigned need = __ballot_sync(FULL, !active);
-            const bool pass = exhausted ? (__ballot_sync(FULL, pending) != 0u) : (__popc(need) >= p.refill_min);
-            if (pass && pending) {
-                finalize<MODEL, BOUND, NOISE>(p, L);
-                pending = false;
-            }
-            if (pass && !exhausted) {
-                const int cnt = __popc(need);
-                const int64_t avail = q_end - q_next;
-                int64_t base = 0;
-                if (avail < cnt) {
-                    unsigned long long b = 0ull;
-                    if (lane == 0) b = atomicAdd(&p.hdr->counter, (unsigned long long)chunk);
-                    base = (int64_t)__shfl_sync(FULL, b, 0);
-                    if (base >= total) exhausted = true;
-                }
-                if (!active) {
-                    const int rank = __popc(need & lt_mask);
-                    const int64_t w = (rank < avail) ? q_next + rank : base + (rank - avail);
-                    if (w < total) active = lane_init<MODEL, NOISE>(p, L, r, w, hint);
-                }
-                if (avail >= cnt) {
-                    q_next += cnt;
-                } else {
-                    q_next = base + (cnt - avail);
-                    q_end = base + chunk;
-                }
-                if (q_next >= total) exhausted = true;  // nothing left for this warp to hand out
-            }
-#if SSM_EXP_COMPACT
-            if (phase == 0 && exhausted) {
-                phase = 1;
-                if (lane == 0) atomicAdd(&s_exhausted, 1);
-            }
-            if (phase == 1 && *(volatile int *)&s_exhausted >= nwarps) {
-                phase = 2;
-                continue;
-            }
-            if (__ballot_sync(FULL, active) == 0u) {
-                if (phase == 1) {
-                    // nothing to step until the CTA's other warps find the queue
-                    // empty (their walks are bounded by the step cap); the wait is
-                    // bounded too, after which the drain phase is entered anyway
-                    __nanosleep(200);
-                    if (++naps > (1u << 24)) {
-                        if (lane == 0) raise_error(p.hdr, SSM_ERR_DEVICE, -1);
-                        phase = 2;
-                    }
-                }
-                continue;
-            }
-#else
-            if (__ballot_sync(FULL, active) == 0u) break;
-#endif
+        // Lanes whose walk ended wait (predicated off) until refill_min of
+        // them have: finishing and restarting lanes runs divergently, with the
+        // rest of the warp idle, so it is done for several lanes in one pass.
+        // Once the queue is empty, pending results are written at once.
+        const unsigned need = __ballot_sync(FULL, !active);
+        const bool pass = exhausted ? (__ballot_sync(FULL, pending) != 0u) : (__popc(need) >= p.refill_min);
+        if (pass && pending) {
+            finalize<MODEL, BOUND, NOISE>(p, L);
+            pending = false;
         }
-#if SSM_EXP_TBLOCK
+        if (pass && !exhausted) {
+            const int cnt = __popc(need);
+            const int64_t avail = q_end - q_next;
+            int64_t base = 0;
+            if (avail < cnt) {
+                unsigned long long b = 0ull;
+                if (lane == 0) b = atomicAdd(&p.hdr->counter, (unsigned long long)chunk);
+                base = (int64_t)__shfl_sync(FULL, b, 0);
+                if (base >= total) exhausted = true;
+            }
+            if (!active) {
+                const int rank = __popc(need & lt_mask);
+                const int64_t w = (rank < avail) ? q_next + rank : base + (rank - avail);
+                if (w < total) active = lane_init<MODEL, NOISE>(p, L, r, w, hint);
+            }
+            if (avail >= cnt) {
+                q_next += cnt;
+            } else {
+                q_next = base + (cnt - avail);
+                q_end = base + chunk;
+            }
+        }
+        if (__ballot_sync(FULL, active) == 0u) break;
         // warp-uniform: skip the per-step time test when no active lane can reach its limit in this block
         const bool skip_time = __all_sync(FULL, !active || block_in_time<MODEL, BOUND, NOISE>(p, L, r));
-#else
-        const bool skip_time = false;
-#endif
         if (active) {
             float g[Blk<MODEL>::value];
             draw_block<MODEL, NOISE>(p, L, r, g);
