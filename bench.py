@@ -44,34 +44,41 @@ WORKLOAD = ("ddm_flexbound angle boundary, 4096 theta ~ U(v[-3,3], a[0.3,3], z[0
             "t[0.001,2], theta[-0.1,1.3]), n_samples ~ U{1000..20000} per theta, dt=1e-3, max_t=20, "
             "one persistent graph-captured launch")
 # Issue-slot roofline of the Euler step: the minimum lane-instruction count per
-# accumulator-step of the algorithm, with no block, queue or per-walk overhead.
-# Philox4x32-10: 10 rounds x (2 wide multiplies + 2 three-input XORs) + the
-# counter = 42 instructions per 4 normals -> 10.5; Box-Muller: 12 per pair
-# (two bit-to-float conversions, log2, scale, sqrt, sin, cos, range scale,
-# two fused multiply-adds) -> 6; the step: bound, two compares, predicate,
-# position and time updates -> 5.5.  Total 22 lane-instructions.
-INSTR_PER_STEP = 22.0
+# accumulator-step of the algorithm as implemented, with no block, queue or
+# per-walk overhead.  Philox4x32-10: 10 rounds x (2 wide multiplies + 2
+# three-input XORs) + the counter = 42 instructions per call, six increments
+# per call -> 7; Box-Muller: 14 per pair (radius: bits to float, shift,
+# log2, scale, sqrt = 5; phase: bit assembly 3 on average, range scale, the
+# SFU's argument scaling, sin, cos = 7; two fused multiply-adds) -> 7; the
+# step with the per-block time test passing: moving bound, compare folded
+# with the walk's predicate, position and time updates -> 4.  Total 18.
+# (The four-per-call layout this kernel replaced needed 22: 10.5 + 6 + 5.5.)
+INSTR_PER_STEP = 18.0
 
 # The same accounting for the other benchmarked families, per accumulator-step
-# (lane-instructions, no block, queue or per-walk overhead).  A Gaussian
-# increment costs 16.5 (Philox 10.5 + Box-Muller 6, folded scale and drift);
-# the step of one accumulator against a constant bound costs 4.5 (two
-# compares, predicate, position and time updates), 5.5 against a moving bound.
+# (lane-instructions, no block, queue or per-walk overhead).  The
+# single-accumulator Gaussian models draw six increments per Philox call
+# (7 + 7 = 14 per increment, folded scale and drift) and test the time once per
+# block (constant-bound step 3: compare with predicate, position and time
+# updates); ddm_flex and the race family draw four per call (Philox 10.5 +
+# Box-Muller 6 = 16.5) and test the time every step (constant-bound step 4.5,
+# 5.5 against a moving bound).
 GAUSS_INCREMENT = 16.5
 INSTR_MIN = {
     # constant bound: 16.5 + 4.5
-    "plain_ddm": (21.0, "Gaussian increment 16.5 + constant-bound step 4.5"),
-    "full_ddm": (21.0, "Gaussian increment 16.5 + constant-bound step 4.5 (per-walk draws amortised)"),
+    "plain_ddm": (17.0, "Gaussian increment 14 (six per Philox call) + constant-bound step 3"),
+    "full_ddm": (17.0, "Gaussian increment 14 + constant-bound step 3 (per-walk draws amortised)"),
     # the leaky update y (1 - g dt) + increment is one FFMA, like the plain add
-    "ornstein": (21.0, "Gaussian increment 16.5 + constant-bound step 4.5 (leak folded into one FFMA)"),
+    "ornstein": (17.0, "Gaussian increment 14 + constant-bound step 3 (leak folded into one FFMA)"),
     # drift table: one FFMA v(t) dt + increment, a 16-byte load per four steps
     "conflict_ds": (22.25, "Gaussian increment 16.5 + constant-bound step 4.5 + drift-table FFMA 1 "
                            "+ vector load 0.25"),
     # two Philox words per stable variate (21), Chambers-Mallows-Stuck with
     # reduced-angle polynomials: uniform and fold 5, W = -ln u 5, three
     # polynomial sin/cos 23, three log2 + exponent + ex2 7, product, sign,
-    # clamp and NaN guard 6, scale FFMA 1 = 47; constant-bound step 4.5
-    "levy": (72.5, "Philox 21 (two words per variate) + CMS 47 + constant-bound step 4.5"),
+    # clamp and NaN guard 6, scale FFMA 1 = 47; constant-bound step 3 (time
+    # tested once per block)
+    "levy": (71.0, "Philox 21 (two words per variate) + CMS 47 + constant-bound step 3"),
     # per accumulator: increment 16.5, add + clamp at 0 + threshold compare 3;
     # per step over 4 accumulators: moving bound, time update and test,
     # predicate 3.5 / 4

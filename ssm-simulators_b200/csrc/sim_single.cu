@@ -12,10 +12,11 @@
 //    hands them the next trajectories of its chunk (popc rank) in one
 //    divergent pass, so that pass is paid once per several trajectories and
 //    an ended lane idles for a few blocks at most.
-//  * Steps run in blocks of 32 (16 for ddm_flex, 8 for Levy): eight independent
-//    Philox4x32-10 calls yield 32 words = 16 Box-Muller pairs = the block's
+//  * Steps run in blocks of 36 (16 for ddm_flex, 8 for Levy): six independent
+//    Philox4x32-10 calls yield 24 words = 18 Box-Muller pairs = the block's
 //    increments, already scaled to drift + s sqrt(dt) N(0,1); the steps
-//    themselves are predicated (no per-step branch).
+//    themselves are predicated (no per-step branch), and a warp whose walks
+//    cannot reach their time limit within the block skips the time test.
 //  * Boundaries are evaluated in registers (constant / linear collapse /
 //    Weibull) or read from a caller-evaluated table for arbitrary shapes.
 //  * Noise injection replaces the generator by caller rows and switches every
@@ -27,15 +28,6 @@
 
 #include "common.cuh"
 
-#ifndef SSM_EXP_SIX
-#define SSM_EXP_SIX 0
-#endif
-#ifndef SSM_EXP_SIX_BLK
-#define SSM_EXP_SIX_BLK 48
-#endif
-#ifndef SSM_EXP_MINCTAS
-#define SSM_EXP_MINCTAS 3
-#endif
 
 
 
@@ -268,23 +260,25 @@ __device__ __forceinline__ float cms_stable(uint32_t bu, uint32_t bw, const Tria
     return fminf(fmaxf(X, -1e10f), 1e10f);
 }
 
-// Euler steps per block.  One Philox4x32-10 call gives four words = two
-// Box-Muller pairs = four increments, so a 32-step block makes eight
-// independent Philox calls whose latencies overlap.  Measured on the 4096-set
-// angle batch (ms per launch): 8 steps 37.9, 16 steps 34.5 (64 registers, 4
-// CTAs per SM), 32 steps 32.9 (80 registers, 3 CTAs per SM), 40 steps 32.9,
-// 64 steps 33.5 (128 registers, 2 CTAs).  ddm_flex uses 16-step blocks (its
-// per-block drift values take registers too; 20.4 -> 18.4 ms against 8-step
-// blocks on the conflict_ds sets), and the Levy model 8-step blocks (its
-// stable draws already give each block enough independent work; 16-step
-// blocks measured 8 % slower there).  The Gaussian counter of call h of block
-// b is (BLK/4) b + h, so those streams do not depend on the block size.
+// Euler steps per block.  The Gaussian models draw six increments per
+// Philox4x32-10 call (three Box-Muller pairs, see bm6_increment), so a
+// 36-step block makes six independent Philox calls whose latencies overlap.
+// Measured on the 4096-set angle batch on one B200 (ms per launch): six per
+// call with 24-step blocks 27.8, 36 steps 26.8, 48 steps 27.0 (all 80
+// registers, 3 CTAs per SM; 4 CTAs per SM at 64 registers 27.3 for 24 and 36
+// steps); four per call with 32-step blocks 31.2.  ddm_flex keeps four per
+// call and 16-step blocks (its per-block drift values take registers too;
+// 20.4 -> 18.4 ms against 8-step blocks on the conflict_ds sets), and the Levy
+// model 8-step blocks (its stable draws already give each block enough
+// independent work; 16-step blocks measured 8 % slower there).  Call h of
+// block b uses counter (BLK/6) b + h (ddm_flex: (BLK/4) b + h), so a stream
+// does not depend on the block length.
 template <int MODEL> struct Blk {
-    static constexpr int value = (MODEL == M_LEVY) ? 8 : (MODEL == M_DFLEX ? 16 : (SSM_EXP_SIX ? SSM_EXP_SIX_BLK : 32));
+    static constexpr int value = (MODEL == M_LEVY) ? 8 : (MODEL == M_DFLEX ? 16 : 36);
 };
 // Resident 256-thread CTAs per SM the compiler must fit (register cap
 // 65536 / (256 n)): 3 (80 registers) for blocks longer than 8 steps, 4 otherwise.
-template <int MODEL> struct MinCtas { static constexpr int value = Blk<MODEL>::value > 8 ? SSM_EXP_MINCTAS : 4; };
+template <int MODEL> struct MinCtas { static constexpr int value = Blk<MODEL>::value > 8 ? 3 : 4; };
 
 struct Lane {
     int64_t w;
@@ -313,11 +307,14 @@ __device__ __forceinline__ void bm_increment(uint32_t a, uint32_t b, float c2, f
     g1 = fmaf(r, sn, drift);
 }
 
-#if SSM_EXP_SIX
 // Six increments from one Philox call (128 bits): three Box-Muller pairs whose
 // radii take 23-bit uniforms from the low bits of x, y and z, and whose phases
 // take the low 23 bits of w, and 18 bits each from the top nine bits of (w, x)
-// and of (y, z).
+// and of (y, z).  The radius resolution is that of the four-per-call layout
+// (uniforms on a 2^-23 grid, so |N| <= 5.6); an 18-bit phase puts the pair on
+// one of 262 144 rays, far below what a one-dimensional increment can show.
+// Compared with two pairs per call this takes a third less Philox work per
+// increment.
 __device__ __forceinline__ void bm6_increment(uint4 b, float c2, float drift, float *g) {
     const uint32_t rad[3] = {b.x, b.y, b.z};
     const uint32_t ph[3] = {b.w & 0x007fffffu, ((b.w >> 9) & 0x7fc000u) | ((b.x >> 18) & 0x3fe0u),
@@ -335,7 +332,6 @@ __device__ __forceinline__ void bm6_increment(uint4 b, float c2, float drift, fl
         g[2 * i + 1] = fmaf(r, sn, drift);
     }
 }
-#endif
 
 // The block's increments.  Noise injection returns the raw caller draws (the
 // step applies drift and scale with explicit rounding); the device RNG returns
@@ -360,8 +356,7 @@ __device__ __forceinline__ void draw_block(const SingleParams &p, const Lane &L,
             g[2 * h + 2] = fmaf(r.scale, cms_stable(c.x, c.y, r), r.drift);
             g[2 * h + 3] = fmaf(r.scale, cms_stable(c.z, c.w, r), r.drift);
         }
-    } else if (SSM_EXP_SIX && MODEL != M_DFLEX) {
-#if SSM_EXP_SIX
+    } else if (MODEL != M_DFLEX) {
         const float drift = DrawnDrift<MODEL>::value ? L.dinc : r.drift;
         static_assert(MODEL == M_LEVY || MODEL == M_DFLEX || BLK % 6 == 0, "six increments per Philox call");
 #pragma unroll
@@ -370,9 +365,9 @@ __device__ __forceinline__ void draw_block(const SingleParams &p, const Lane &L,
                                      p.key);
             bm6_increment(b, r.c2, drift, g + 6 * h);
         }
-#endif
     } else {
-        const float drift = DrawnDrift<MODEL>::value ? L.dinc : (MODEL == M_DFLEX ? 0.f : r.drift);
+        // ddm_flex: two pairs per call; the drift comes from the table in the step
+        const float drift = 0.f;
 #pragma unroll
         for (int h = 0; h < BLK / 4; ++h) {
             const uint4 b = philox10(make_uint4((uint32_t)(BLK / 4) * L.blk + (uint32_t)h, L.n, L.k + p.k_base, 0u),
