@@ -648,6 +648,7 @@ def run_other_workloads(args, f_max: float = 1965e6) -> dict:
         sb = SetBatch(name, prep["theta"], prep["boundary"], n, max_t=20.0, delta_t=0.001, drift=prep["drift"])
         o = sb.run(SEED, want_steps=True)
         steps = int(o.steps.to(torch.int64).sum().item())
+        longest = int(o.steps.max().item()) if sb.total else 0
         for w in range(args.warmup):
             sb.run(SEED + 1 + w)
         ms = []
@@ -675,6 +676,8 @@ def run_other_workloads(args, f_max: float = 1965e6) -> dict:
             "ms_per_launch": dev_ms, "trajectories_per_s": sb.total / (dev_ms / 1e3),
             "accumulator_steps_per_s": acc_rate,
             "e2e_trajectories_per_s": sb.total * len(e2e) / sum(e2e),
+            # the launch cannot end before its longest walk: ns per step along that walk
+            "longest_walk_steps": longest, "ns_per_step_of_longest_walk": dev_ms * 1e6 / max(longest, 1),
         }
         if label in INSTR_MIN:
             imin, basis = INSTR_MIN[label]
