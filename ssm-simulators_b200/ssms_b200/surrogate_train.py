@@ -2,7 +2,7 @@
 against simulation + KDE.
 
     python -m ssms_b200.surrogate_train --model angle --train-sets 100000 \\
-        --n-samples 100000 --epochs 20 --out angle_surrogate.pt --report report.json
+        --n-samples 100000 --epochs 60 --lr-decay 0.95 --out angle_surrogate.pt --report report.json
 
 Records come from ``BatchedKdePipeline`` with the reference's LAN-KDE
 generator config (ssms/config/data_generator_config.py) and 1000 rows per
@@ -132,10 +132,10 @@ def main(argv=None) -> dict:
     ap.add_argument("--model", default="angle")
     ap.add_argument("--train-sets", type=int, default=100_000)
     ap.add_argument("--n-samples", type=int, default=100_000)
-    ap.add_argument("--epochs", type=int, default=20)
+    ap.add_argument("--epochs", type=int, default=60)
     ap.add_argument("--batch", type=int, default=8192)
     ap.add_argument("--lr", type=float, default=1e-3)
-    ap.add_argument("--lr-decay", type=float, default=1.0)
+    ap.add_argument("--lr-decay", type=float, default=0.95)
     ap.add_argument("--loss", default="huber")
     ap.add_argument("--judge-sets", type=int, default=1000)
     ap.add_argument("--judge-per-set", type=int, default=1000)
