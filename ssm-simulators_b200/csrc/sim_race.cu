@@ -131,6 +131,14 @@ __device__ __forceinline__ float2 std_normal_pair(uint32_t a, uint32_t b) {
 // launch on 1024 sets x 10000: 2 ahead 65.5, 4 ahead 56.3, 8 ahead 52.1.
 constexpr int RACE_PRE = 8;
 
+#ifndef SSM_RACE_SIX
+#define SSM_RACE_SIX 0
+#endif
+// With six normals per Philox call a lane draws a window of WIN steps at once,
+// WIN * NP a multiple of six: 2 accumulators 12 steps, 3 accumulators 8, 4
+// accumulators 6 (four independent calls per window).
+template <int NP> struct RaceWin { static constexpr int value = NP == 2 ? 12 : (NP == 3 ? 8 : 6); };
+
 template <int NP>
 struct RaceLane {
     int64_t w;
@@ -433,6 +441,25 @@ __global__ void __launch_bounds__(256) k_race(const __grid_constant__ RaceParams
                 sr[j] = (j < np) ? __ldg(sq + j) : 0.f;
             }
             bool live = true;
+#if SSM_RACE_SIX
+            if (!NOISE && NP <= 4) {
+                // the next WIN steps' normals first, six per Philox call (calls
+                // ctr .. ctr + CALLS - 1), then the steps; ctr advances per window
+                constexpr int WIN = RaceWin<NP>::value;
+                constexpr int CALLS = WIN * NP / 6;
+                float nrm[WIN * NP];
+#pragma unroll
+                for (int c = 0; c < CALLS; ++c) {
+                    const uint4 r = philox10(make_uint4(ctr + (uint32_t)c, L.n, L.k + p.k_base, 0u), p.key);
+                    bm6_increment(r, -1.3862944f, 0.f, nrm + 6 * c);
+                }
+                ctr += CALLS;
+                uint32_t unused = 0;
+#pragma unroll
+                for (int s = 0; s < WIN; ++s)
+                    if (live) live = race_step<NP, FAM, BOUND, NOISE, false, true>(p, L, h, vr, sr, np, unused, nrm + s * NP);
+            } else
+#endif
             if (!NOISE && NP <= 4) {
                 // the next RACE_PRE steps' normals first: independent Philox
                 // calls whose latencies overlap (counters ctr .. ctr + RACE_PRE - 1,

@@ -307,32 +307,6 @@ __device__ __forceinline__ void bm_increment(uint32_t a, uint32_t b, float c2, f
     g1 = fmaf(r, sn, drift);
 }
 
-// Six increments from one Philox call (128 bits): three Box-Muller pairs whose
-// radii take 23-bit uniforms from the low bits of x, y and z, and whose phases
-// take the low 23 bits of w, and 18 bits each from the top nine bits of (w, x)
-// and of (y, z).  The radius resolution is that of the four-per-call layout
-// (uniforms on a 2^-23 grid, so |N| <= 5.6); an 18-bit phase puts the pair on
-// one of 262 144 rays, far below what a one-dimensional increment can show.
-// Compared with two pairs per call this takes a third less Philox work per
-// increment.
-__device__ __forceinline__ void bm6_increment(uint4 b, float c2, float drift, float *g) {
-    const uint32_t rad[3] = {b.x, b.y, b.z};
-    const uint32_t ph[3] = {b.w & 0x007fffffu, ((b.w >> 9) & 0x7fc000u) | ((b.x >> 18) & 0x3fe0u),
-                            ((b.y >> 9) & 0x7fc000u) | ((b.z >> 18) & 0x3fe0u)};
-#pragma unroll
-    for (int i = 0; i < 3; ++i) {
-        const float u1 = __uint_as_float(0x3f800000u | (rad[i] & 0x007fffffu)) - 0.99999994f;  // (0, 1)
-        const float ang = fmaf(__uint_as_float(0x3f800000u | ph[i]), 6.2831853f, -6.2831853f);
-        const float e = c2 * lg2_ftz(u1);
-        float r;
-        asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(e));
-        float sn, cs;
-        sincos_ftz(ang, sn, cs);
-        g[2 * i] = fmaf(r, cs, drift);
-        g[2 * i + 1] = fmaf(r, sn, drift);
-    }
-}
-
 // The block's increments.  Noise injection returns the raw caller draws (the
 // step applies drift and scale with explicit rounding); the device RNG returns
 // finished increments drift + scale * X.
