@@ -126,17 +126,13 @@ __device__ __forceinline__ float2 std_normal_pair(uint32_t a, uint32_t b) {
     return box_muller(a, b);
 }
 
-// Steps whose normals a lane draws ahead (models with at most 4 accumulators):
-// that many independent Philox calls overlap.  LCA (4 accumulators), ms per
-// launch on 1024 sets x 10000: 2 ahead 65.5, 4 ahead 56.3, 8 ahead 52.1.
-constexpr int RACE_PRE = 8;
-
-#ifndef SSM_RACE_SIX
-#define SSM_RACE_SIX 0
-#endif
-// With six normals per Philox call a lane draws a window of WIN steps at once,
-// WIN * NP a multiple of six: 2 accumulators 12 steps, 3 accumulators 8, 4
-// accumulators 6 (four independent calls per window).
+// Models with at most 4 accumulators draw a window of WIN steps' normals at
+// once, six per Philox4x32-10 call (bm6_increment), WIN * NP a multiple of six:
+// 2 accumulators 12 steps, 3 accumulators 8, 4 accumulators 6 -- four
+// independent calls per window, whose latencies overlap.  Measured on the
+// 1024-set workloads (ms per launch): LCA 50.3 -> 44.8 and race 19.2 -> 17.0
+// against one call (four normals) per step drawn eight steps ahead, which
+// itself had taken LCA from 66.0 (2 ahead 65.5, 4 ahead 56.3, 8 ahead 52.1).
 template <int NP> struct RaceWin { static constexpr int value = NP == 2 ? 12 : (NP == 3 ? 8 : 6); };
 
 template <int NP>
@@ -441,7 +437,6 @@ __global__ void __launch_bounds__(256) k_race(const __grid_constant__ RaceParams
                 sr[j] = (j < np) ? __ldg(sq + j) : 0.f;
             }
             bool live = true;
-#if SSM_RACE_SIX
             if (!NOISE && NP <= 4) {
                 // the next WIN steps' normals first, six per Philox call (calls
                 // ctr .. ctr + CALLS - 1), then the steps; ctr advances per window
@@ -458,25 +453,6 @@ __global__ void __launch_bounds__(256) k_race(const __grid_constant__ RaceParams
 #pragma unroll
                 for (int s = 0; s < WIN; ++s)
                     if (live) live = race_step<NP, FAM, BOUND, NOISE, false, true>(p, L, h, vr, sr, np, unused, nrm + s * NP);
-            } else
-#endif
-            if (!NOISE && NP <= 4) {
-                // the next RACE_PRE steps' normals first: independent Philox
-                // calls whose latencies overlap (counters ctr .. ctr + RACE_PRE - 1,
-                // one call per step, as the steps themselves would draw them)
-                float pre[RACE_PRE][NP];
-#pragma unroll
-                for (int s = 0; s < RACE_PRE; ++s) {
-                    const uint4 r = philox10(make_uint4(ctr + (uint32_t)s, L.n, L.k + p.k_base, 0u), p.key);
-                    const float2 a = std_normal_pair(r.x, r.y);
-                    const float2 b = std_normal_pair(r.z, r.w);
-                    const float four[4] = {a.x, a.y, b.x, b.y};
-#pragma unroll
-                    for (int j = 0; j < NP; ++j) pre[s][j] = four[j];
-                }
-#pragma unroll
-                for (int s = 0; s < RACE_PRE; ++s)
-                    if (live) live = race_step<NP, FAM, BOUND, NOISE, false, true>(p, L, h, vr, sr, np, ctr, pre[s]);
             } else {
 #pragma unroll 1
                 for (int s = 0; s < 4 && live; ++s)
@@ -508,7 +484,25 @@ __global__ void k_race_record(const __grid_constant__ RaceParams p) {
         sr[j] = (j < np) ? row[16 + np + j] : 0.f;
     }
     uint32_t ctr = 0;
-    while (race_step<NP, FAM, BOUND, NOISE, true>(p, L, h, vr, sr, np, ctr)) {
+    if (!NOISE && NP <= 4) {
+        // the main kernel's windows: the same normals in the same order
+        constexpr int WIN = RaceWin<NP>::value;
+        constexpr int CALLS = WIN * NP / 6;
+        bool live = true;
+        while (live) {
+            float nrm[WIN * NP];
+            for (int c = 0; c < CALLS; ++c) {
+                const uint4 r = philox10(make_uint4(ctr + (uint32_t)c, L.n, L.k + p.k_base, 0u), p.key);
+                bm6_increment(r, -1.3862944f, 0.f, nrm + 6 * c);
+            }
+            ctr += CALLS;
+            uint32_t unused = 0;
+            for (int s = 0; s < WIN && live; ++s)
+                live = race_step<NP, FAM, BOUND, NOISE, true, true>(p, L, h, vr, sr, np, unused, nrm + s * NP);
+        }
+    } else {
+        while (race_step<NP, FAM, BOUND, NOISE, true>(p, L, h, vr, sr, np, ctr)) {
+        }
     }
 }
 

@@ -52,7 +52,8 @@ def test_batched_queries_match_oracle_kde(cuda):
             g = 2 * s + ci
             sl = slice(qoff[g], qoff[g + 1])
             o = ok.kde_eval(qh[sl], np.full(qoff[g + 1] - qoff[g], c))
-            np.testing.assert_allclose(ll[sl], o, rtol=1e-6, atol=1e-5)
+            # float32 kernel terms and sample points against float64 sums (tests/test_gpu_kde.py)
+            np.testing.assert_allclose(ll[sl], o, rtol=2e-6, atol=1e-5)
             assert np.all(qh[sl][60:] >= 0.0001) and np.all(qh[sl][60:] <= 20.0)
 
 

@@ -4,9 +4,14 @@ oracle (oracle/kde_oracle.py) and the reference's scikit-learn values
 
 Tolerance: the GPU evaluates each kernel term in float32 (query split into
 hi + lo parts, SFU exp2) and accumulates in float64; log-likelihoods must
-agree with the exact float64 sums to 1e-5 absolute plus 1e-6 relative.  The
-relative part covers the tails: the exponent (q - x)^2 / 2h^2 is held in
-float32, so its ~1.2e-7 relative rounding is ~1e-5 once the exponent is ~80.
+agree with the exact float64 sums to 1e-5 absolute plus 2e-6 relative.  The
+relative part covers the tails, where two float32 roundings grow with the
+distance z = |q - x| / h of the dominant sample points: the exponent z^2 / 2
+(~1.2e-7 relative, ~1e-5 once it is ~80), and the sample points themselves,
+stored as float32 log-rts (|dx| <= 1.8e-7 for rt <= 20), which move the
+exponent by z |dx| / h -- 4e-5 for a query 10 bandwidths of 0.05 out, where
+the log-likelihood is about -48.  Both stay under 2e-6 |ll| down to the
+floor (-66.8).
 """
 
 import numpy as np
@@ -23,7 +28,7 @@ pytestmark = pytest.mark.gpu
 
 G = dict(np.load(GOLDEN / "kde_golden.npz"))
 TOL = 1e-5
-RTOL = 1e-6
+RTOL = 2e-6
 
 
 def _data(tag):

@@ -71,6 +71,29 @@ def test_race_lca_noise_injection_bit_exact(cuda, oracle, model, npart, bname):
     np.testing.assert_array_equal(_bits(out.traj.cpu().numpy()), _bits(o_tr))
 
 
+@pytest.mark.parametrize("model,npart", [("race_model", 2), ("race_model", 3), ("race_model", 4), ("lca", 3),
+                                         ("lca", 4)])
+def test_device_rng_trajectory_is_sample_zero_walk(cuda, model, npart):
+    """Device RNG: the recorded trajectory (trial 0, sample 0, re-simulated by
+    the recorder kernel) is the walk the main kernel simulated -- one row per
+    step plus the start, and the last row's first maximum is the choice."""
+    rng = np.random.default_rng(40 + npart + (10 if model == "lca" else 0))
+    K, N = 3, 64
+    th = _race_theta(rng, K, npart)
+    lca = model == "lca"
+    spec = bf.kernel_spec(bf.constant, {"a": th["a"]}, K, bf.make_t_s(20.0, 0.001))
+    for seed in range(4):
+        out = dev.simulate_race(model, v=th["v"], z=th["z"], t=th["t"], s=th["s"], deadline=f32([999] * K),
+                                n_trials=K, n_samples=N, g=th["g"] if lca else None, b=th["b"] if lca else None,
+                                max_t=20.0, bound_kind=spec["kind"], a=spec["a"], seed=seed, want_steps=True,
+                                traj_len=20001 * npart)
+        traj = out.traj.cpu().numpy().reshape(-1, npart)
+        rows = int(np.sum(np.all(traj != -999.0, axis=1)))
+        steps0, ch0 = int(out.steps[0].item()), int(out.choices[0].item())
+        assert rows == steps0 + 1, (rows, steps0)
+        assert int(np.argmax(traj[rows - 1])) == ch0
+
+
 def test_lba_noise_injection_bit_exact(cuda, oracle):
     rng = np.random.default_rng(31)
     K, N, nact = 4, 500, 3
