@@ -123,9 +123,14 @@ def test_theta_gradient_against_finite_differences(trained):
     difference of large terms -- d/dt against d/drt is the worst case, at
     about 6 % -- so the bound is 10 %.
     (2) A least-squares slope through six symmetric finite differences of the
-    kernel's own forward pass (steps of 0.5-1.5 % of the range), which averages
-    out the bf16 quantisation of that forward pass; a looser bound, because the
-    quantised forward is a fine staircase in each input.
+    kernel's own forward pass (steps of 1-3 % of the range), which averages out
+    the bf16 quantisation of that forward pass; a looser bound, because the
+    quantised forward is a fine staircase in each input.  The staircase's
+    effect on the slope falls as the steps grow, and the symmetric stencil
+    cancels the even-order curvature terms, so the steps are as wide as the
+    network's smoothness allows: with 0.5-1.5 % steps the parameter with the
+    weakest gradient (theta) measured 0.22 from staircase noise alone while its
+    float64 check gave 0.03.
     Points where the network sits at its label floor (a kink) are left out."""
     net, _ = trained
     rng = np.random.default_rng(3)
@@ -149,7 +154,7 @@ def test_theta_gradient_against_finite_differences(trained):
         den = np.zeros(xq.shape[0])
         for m in (-3, -2, -1, 1, 2, 3):
             xs = xq.copy()
-            xs[:, j] += m * 0.005 * (hi[j] - lo[j])
+            xs[:, j] += m * 0.01 * (hi[j] - lo[j])
             step = xs[:, j].astype(np.float64) - xq[:, j]
             num += step * (f(xs) - f0)
             den += step * step
