@@ -113,36 +113,32 @@ def test_theta_gradient_against_analytic_gradient(trained):
 
 
 def test_theta_gradient_against_finite_differences(trained):
-    """d out / d theta from the backward kernel against finite differences of
-    the same trained network.
+    """d out / d theta from the backward kernel on the trained network.
 
-    (1) Central differences of the network evaluated in float64 (the oracle's
-    unquantised forward on the trained weights; steps of 0.1 % of each
-    parameter's range): the kernel's backward GEMMs take bf16 operands, whose
-    rounding (about 0.4 % per stage) is amplified where a gradient is a small
-    difference of large terms -- d/dt against d/drt is the worst case, at
-    about 6 % -- so the bound is 10 %.
-    (2) A least-squares slope through six symmetric finite differences of the
-    kernel's own forward pass (steps of 1-3 % of the range), which averages out
-    the bf16 quantisation of that forward pass; a looser bound, because the
-    quantised forward is a fine staircase in each input.  The staircase's
-    effect on the slope falls as the steps grow, and the symmetric stencil
-    cancels the even-order curvature terms, so the steps are as wide as the
-    network's smoothness allows: with 0.5-1.5 % steps the parameter with the
-    weakest gradient (theta) measured 0.22 from staircase noise alone while its
-    float64 check gave 0.03.
+    (1) Against central differences of the network evaluated in float64 (the
+    oracle's unquantised forward on the trained weights; steps of 0.1 % of
+    each parameter's range): the kernel's backward GEMMs take bf16 operands,
+    whose rounding (about 0.4 % per stage) is amplified where a gradient is a
+    small difference of large terms -- d/dt against d/drt is the worst case,
+    at about 6 % -- so the bound is 10 %.
+    (2) Against the float64 oracle's input gradient with the kernel's bf16
+    rounding points (oracle/mlp_oracle.py forward(..., want_dx=True)), at the
+    tolerance of the random-weight test in tests/test_gpu_mlp.py: the same
+    check on the weights training produced.
+    (Finite differences of the kernel's own bf16 forward are no yardstick: the
+    quantised forward is a staircase, and over 0.5-1.5 % or 1-3 % steps its
+    slope differs from the network's by 0.05-0.29, depending on how strongly
+    the parameter moves the output -- staircase noise against curvature.)
     Points where the network sits at its label floor (a kink) are left out."""
     net, _ = trained
     rng = np.random.default_rng(3)
     th, xq = T.uniform_queries("angle", 500, 4, seed=13)
     xq[:, 5] = xq[:, 3] + rng.uniform(0.2, 3.0, xq.shape[0])  # rts in the bulk after t
-    _, dx = net.forward(torch.from_numpy(xq), want_dx=True)
-    dx = dx.double().cpu().numpy()
-    f = lambda x: net.forward(torch.from_numpy(x)).double().cpu().numpy()  # noqa: E731
+    out, dx = net.forward(torch.from_numpy(xq), want_dx=True)
+    out, dx = out.double().cpu().numpy(), dx.double().cpu().numpy()
     p64 = net.params.detach().double().cpu().numpy()
     f64 = lambda x: MO.forward(p64, x, net.norm_c, net.norm_s, quantize=False)  # noqa: E731
-    f0 = f(xq)
-    keep = f0 > -10.0
+    keep = out > -10.0
     lo, hi = (np.asarray(b, np.float64) for b in S._model_config["angle"]["param_bounds"])
     for j in range(5):
         xp, xm = xq.copy(), xq.copy()
@@ -150,16 +146,9 @@ def test_theta_gradient_against_finite_differences(trained):
         xm[:, j] -= 0.001 * (hi[j] - lo[j])
         fd64 = (f64(xp) - f64(xm)) / (xp[:, j].astype(np.float64) - xm[:, j])
         rel64 = np.linalg.norm(dx[keep, j] - fd64[keep]) / np.linalg.norm(fd64[keep])
-        num = np.zeros(xq.shape[0])
-        den = np.zeros(xq.shape[0])
-        for m in (-3, -2, -1, 1, 2, 3):
-            xs = xq.copy()
-            xs[:, j] += m * 0.01 * (hi[j] - lo[j])
-            step = xs[:, j].astype(np.float64) - xq[:, j]
-            num += step * (f(xs) - f0)
-            den += step * step
-        fd = num / den
-        rel = np.linalg.norm(dx[keep, j] - fd[keep]) / np.linalg.norm(fd[keep])
-        print("fd", j, "float64 network", rel64, "kernel forward slope", rel)
+        print("fd", j, "float64 network", rel64)
         assert rel64 < 0.1, (j, rel64)
-        assert rel < 0.2, (j, rel)
+    ref_out, ref_dx = MO.forward(net.params.detach().cpu().numpy(), xq, net.norm_c, net.norm_s, want_dx=True)
+    np.testing.assert_allclose(out, ref_out, atol=6e-3, rtol=3e-3)
+    scale = np.abs(ref_dx).max(axis=0)
+    np.testing.assert_allclose(dx, ref_dx, atol=2e-2 * scale.max(), rtol=2e-2)
