@@ -59,16 +59,14 @@ def make_data_generator_configs(model="ddm", generator_approach="lan", data_gene
 
 
 def parse_dict_as_namedtuple(d: dict, to_lowercase: bool = True):
-    """Nested dict -> nested namedtuples (keys lower-cased by default)."""
-
-    def convert(v):
-        if isinstance(v, dict):
-            v = {(k.lower() if to_lowercase else k): convert(val) for k, val in v.items()}
-            return namedtuple("Config", v.keys())(**v)
-        return v
-
-    d = {(k.lower() if to_lowercase else k): convert(v) for k, v in d.items()}
-    return namedtuple("Config", d.keys())(**d)
+    """A YAML mapping as attribute-access records: every mapping (nested ones
+    too) becomes a namedtuple with the keys as fields, lower-cased unless
+    ``to_lowercase`` is false, so ``cfg.simulator.n_samples`` reads the
+    SIMULATOR section's n_samples; other values are kept as they are."""
+    if not isinstance(d, dict):
+        return d
+    fields = {(k.lower() if to_lowercase else k): parse_dict_as_namedtuple(v, to_lowercase) for k, v in d.items()}
+    return namedtuple("Config", list(fields))(*fields.values())
 
 
 def _make_data_folder_path(base_path, basic_config) -> Path:

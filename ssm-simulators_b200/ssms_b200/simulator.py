@@ -45,22 +45,24 @@ def _validate_random_state_for_c_rng(random_state) -> None:
 
 
 def _make_valid_dict(dict_in: dict) -> dict:
-    lengths = []
+    """Every parameter as a float32 vector of one common length: lists,
+    numbers and arrays are converted and squeezed; scalar (or length-1)
+    values are repeated to the length the vector-valued parameters share,
+    or become length-1 vectors when there are none.  Raises ValueError for
+    more than one dimension or for vectors of different lengths.  Updates
+    dict_in in place, as the reference does (simulator.py:80), and returns it."""
+    flat = {}
     for key, value in dict_in.items():
-        if isinstance(value, list):
-            dict_in[key] = np.array(value).astype(np.float32)
-        elif isinstance(value, int | float):
-            dict_in[key] = np.array([value]).astype(np.float32)
-        dict_in[key] = np.squeeze(dict_in[key]).astype(np.float32)
-        if dict_in[key].ndim > 1:
+        arr = np.squeeze(np.asarray(value, dtype=np.float32))
+        if arr.ndim > 1:
             raise ValueError(f"Dimension of {key} is greater than 1")
-        if dict_in[key].ndim > 0:
-            lengths.append(dict_in[key].shape[0])
-    if len(set(lengths)) > 1:
+        flat[key] = arr
+    lengths = {arr.shape[0] for arr in flat.values() if arr.ndim == 1}
+    if len(lengths) > 1:
         raise ValueError("thetas have to be either scalars or same length for all thetas which are not scalars")
-    for key, value in dict_in.items():
-        if value.ndim == 0:
-            dict_in[key] = np.tile(value, lengths[0]) if lengths else np.expand_dims(value, axis=0)
+    n = lengths.pop() if lengths else 1
+    for key, arr in flat.items():
+        dict_in[key] = arr if arr.ndim == 1 else np.full(n, arr, dtype=np.float32)
     return dict_in
 
 
@@ -145,23 +147,22 @@ def validate_ssm_parameters(model: str, theta: dict) -> None:
 
 def bin_simulator_output(out: dict, bin_dt: float = 0.04, nbins: int = 0, max_t: float = -1,
                          freq_cnt: bool = False) -> np.ndarray:
-    """Histogram of rts per choice (simulator.py:435-497): last bin open to +inf."""
+    """Per-choice histogram of a simulator output's rts, [nbins, n_choices]
+    (simulator.py:435-497): nbins edges evenly spaced over [0, max_t] (by
+    default max_t from the metadata and nbins = max_t / bin_dt) plus an edge
+    at +inf, so the last bin collects every later rt; divided by n_samples
+    unless freq_cnt is True."""
     if out is None:
         raise ValueError("out is not supplied")
-    if max_t == -1:
-        max_t = out["metadata"]["max_t"]
-    if nbins == 0:
-        nbins = int(max_t / bin_dt)
-    bins = np.zeros(nbins + 1)
-    bins[:nbins] = np.linspace(0, max_t, nbins)
-    bins[nbins] = np.inf
-    choices = out["metadata"]["possible_choices"]
-    counts = np.zeros((nbins, len(choices)))
-    for i, c in enumerate(choices):
-        counts[:, i] = np.histogram(out["rts"][out["choices"] == c], bins=bins)[0]
-    if freq_cnt is False:
-        counts = counts / out["metadata"]["n_samples"]
-    return counts
+    meta = out["metadata"]
+    max_t = meta["max_t"] if max_t == -1 else max_t
+    nbins = int(max_t / bin_dt) if nbins == 0 else nbins
+    edges = np.append(np.linspace(0, max_t, nbins), np.inf)
+    rts = np.asarray(out["rts"]).reshape(-1)
+    chs = np.asarray(out["choices"]).reshape(-1)
+    table = np.stack([np.histogram(rts[chs == c], bins=edges)[0] for c in meta["possible_choices"]],
+                     axis=1).astype(np.float64)
+    return table / meta["n_samples"] if freq_cnt is False else table
 
 
 def _noise(theta, model_name, no_noise, sigma_noise):
