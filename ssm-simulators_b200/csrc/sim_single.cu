@@ -266,7 +266,9 @@ __device__ __forceinline__ float cms_stable(uint32_t bu, uint32_t bw, const Tria
 // Measured on the 4096-set angle batch on one B200 (ms per launch): six per
 // call with 24-step blocks 27.8, 36 steps 26.8, 48 steps 27.0 (all 80
 // registers, 3 CTAs per SM; 4 CTAs per SM at 64 registers 27.3 for 24 and 36
-// steps); four per call with 32-step blocks 31.2.  ddm_flex keeps four per
+// steps); four per call with 32-step blocks 31.2.  With the re-tuned launch
+// (128 threads, claims of 256): 30 steps 26.95, 36 steps 26.54, 42 steps
+// 26.39, but on 1024 sets 42 steps is the slower (8.02 against 7.92 ms).  ddm_flex keeps four per
 // call and 16-step blocks (its per-block drift values take registers too;
 // 20.4 -> 18.4 ms against 8-step blocks on the conflict_ds sets), and the Levy
 // model 8-step blocks (its stable draws already give each block enough
