@@ -146,14 +146,30 @@ struct RaceLane {
     float x[NP];
 };
 
+// True when none of the lane's next `win` steps can reach the step cap or the
+// time limit: the float32 accumulator after (win - 1) more additions of dt is
+// at most t + (win - 1) dt plus their roundings (under dt/4 below 65536 dt),
+// so t + (win + 1) dt <= dl_tmp leaves margin; LCA's float64 accumulator
+// rounds far less.
+template <int NP, int FAM>
+__device__ __forceinline__ bool window_clear(const RaceParams &p, const RaceLane<NP> &L, const RaceHead &h,
+                                             int win) {
+    if (L.ixf + (float)win > h.capf) return false;
+    const float span = (float)(win + 1);
+    if (FAM == FAM_LCA) return L.tpd + (double)span * (double)p.dt <= (double)h.dl_tmp;
+    return (L.tp < p.dt * 65536.f) && (fmaf(span, p.dt, L.tp) <= h.dl_tmp);
+}
+
 // One Euler step of every accumulator.  Returns false when the loop condition
 // failed before the step (the walk is over).  With PRE the step's normals come
 // from `pre` (drawn ahead from the same counters); ctr still counts the steps.
-template <int NP, int FAM, int BOUND, bool NOISE, bool RECORD, bool PRE = false>
+// CHECKED false skips the step-cap check and the time test, for a window the
+// caller has shown both to pass for (window_clear).
+template <int NP, int FAM, int BOUND, bool NOISE, bool RECORD, bool PRE = false, bool CHECKED = true>
 __device__ __forceinline__ bool race_step(const RaceParams &p, RaceLane<NP> &L, const RaceHead &h,
                                           const float *v, const float *sq, int np, uint32_t &ctr,
                                           const float *pre = nullptr) {
-    if (L.ixf >= h.capf) {
+    if (CHECKED && L.ixf >= h.capf) {
         raise_error(p.hdr, SSM_ERR_DEVICE, (int)L.w);
         return false;
     }
@@ -165,7 +181,7 @@ __device__ __forceinline__ bool race_step(const RaceParams &p, RaceLane<NP> &L, 
             if (j < np) finished |= (L.x[j] > bnd);
     }
     constexpr bool LCA = (FAM == FAM_LCA);
-    const bool in_time = LCA ? (L.tpd <= (double)h.dl_tmp) : (L.tp <= h.dl_tmp);
+    const bool in_time = !CHECKED || (LCA ? (L.tpd <= (double)h.dl_tmp) : (L.tp <= h.dl_tmp));
     if (finished || !in_time) return false;
     float gsn[NP];
     if (NOISE) {
@@ -426,6 +442,10 @@ __global__ void __launch_bounds__(256) k_race(const __grid_constant__ RaceParams
             }
         }
         if (__ballot_sync(FULL, active) == 0u) break;
+        // warp-uniform: skip the per-step cap and time tests when no active
+        // lane can reach either within its next window
+        const bool clear = (!NOISE && NP <= 4) &&
+                           __all_sync(FULL, !active || window_clear<NP, FAM>(p, L, h, RaceWin<NP>::value));
         if (active) {
             const float *row = p.rows + (int64_t)L.k * p.row_floats;
             const float *v = row + 16;
@@ -450,9 +470,17 @@ __global__ void __launch_bounds__(256) k_race(const __grid_constant__ RaceParams
                 }
                 ctr += CALLS;
                 uint32_t unused = 0;
+                if (clear) {
 #pragma unroll
-                for (int s = 0; s < WIN; ++s)
-                    if (live) live = race_step<NP, FAM, BOUND, NOISE, false, true>(p, L, h, vr, sr, np, unused, nrm + s * NP);
+                    for (int s = 0; s < WIN; ++s)
+                        if (live)
+                            live = race_step<NP, FAM, BOUND, NOISE, false, true, false>(p, L, h, vr, sr, np, unused,
+                                                                                        nrm + s * NP);
+                } else {
+#pragma unroll
+                    for (int s = 0; s < WIN; ++s)
+                        if (live) live = race_step<NP, FAM, BOUND, NOISE, false, true>(p, L, h, vr, sr, np, unused, nrm + s * NP);
+                }
             } else {
 #pragma unroll 1
                 for (int s = 0; s < 4 && live; ++s)
