@@ -728,7 +728,9 @@ def run_reference(args):
     workload instead of re-timing one block."""
     theta, n_samples = workload(SEED)
     pool = CpuPool()
-    per_core = 8
+    # 24 rows per core, as cpu_baseline: the rows' sizes differ 20-fold, and
+    # fewer rows per core leave cores idle at the end of each step
+    per_core = 24
     block = per_core * pool.cores
     step = 0
     for _ in range(args.warmup):
