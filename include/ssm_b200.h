@@ -72,6 +72,14 @@ typedef struct ssm_launch {
      * trajectories are skipped. */
     const int32_t *trial_order;
     const int64_t *order_offsets;
+    /* Lanes per trajectory of the single-accumulator simulators (device RNG,
+     * constant / linear / Weibull boundary): 1, 2, 4 or 8; 0 = automatic,
+     * which is 1 for the ragged layout and otherwise chosen from the number
+     * of trajectories against the grid's lanes (ssm_auto_lanes_per_walk).
+     * With W > 1 the W lanes of a group draw a walk's increments in parallel
+     * and step it together: results are bit-identical to W = 1, and a launch
+     * with fewer trajectories than lanes ends sooner; chunk is 32 / W. */
+    int lanes_per_walk;
 } ssm_launch;
 
 /* Version / diagnostics -------------------------------------------------- */
@@ -86,6 +94,12 @@ int ssm_check_status(const void *workspace, void *stream);
 
 /* Bytes of scratch the DDM-family entry points need for n_trials trials. */
 size_t ssm_ddm_workspace_bytes(int64_t n_trials);
+/* Lanes per walk (ssm_launch.lanes_per_walk) the library picks for a
+ * single-accumulator launch of n_walks trajectories on the current device
+ * when the option is 0 and the layout is not ragged; callers of the ragged
+ * layout, which know their total, pass it explicitly.  No reference
+ * counterpart: a launch-shape choice of this library. */
+int ssm_auto_lanes_per_walk(int64_t n_walks);
 
 /*
  * ssm_ddm_flexbound -- replaces cssm.ddm_flexbound

@@ -29,12 +29,13 @@ int sm_count();
     } while (0)
 
 // Trajectories a persistent simulator warp claims per queue access: the
-// caller's chunk, cut (to a multiple of 32, at least 32) so that every warp of
-// the grid gets work when the launch is small.
-__device__ __forceinline__ int64_t warp_chunk(int chunk, int64_t total) {
+// caller's chunk, cut (to a multiple of the warp's walk slots -- 32, or 32 / W
+// with W lanes per walk -- and at least one slot per walk) so that every warp
+// of the grid gets work when the launch is small.
+__device__ __forceinline__ int64_t warp_chunk(int chunk, int64_t total, int slots = 32) {
     const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
-    const int64_t fair = ((total + warps - 1) / warps + 31) & ~(int64_t)31;
-    return max((int64_t)32, min((int64_t)chunk, fair));
+    const int64_t fair = ((total + warps - 1) / warps + slots - 1) / slots * slots;
+    return max((int64_t)slots, min((int64_t)chunk, fair));
 }
 
 // Ended walks a persistent simulator warp collects before it writes their

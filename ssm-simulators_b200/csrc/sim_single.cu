@@ -278,9 +278,22 @@ __device__ __forceinline__ float cms_stable(uint32_t bu, uint32_t bw, const Tria
 template <int MODEL> struct Blk {
     static constexpr int value = (MODEL == M_LEVY) ? 8 : (MODEL == M_DFLEX ? 16 : 36);
 };
+// Lanes per walk W (see wide_block): 1 is the throughput mode above; W = 2,
+// 4, 8 give each trajectory an aligned group of W lanes and blocks of 18 W
+// steps, three Philox calls per lane.
+template <int MODEL, int W> struct BlkW {
+    static constexpr int value = (W == 1) ? Blk<MODEL>::value : 18 * W;
+};
+template <int MODEL, bool NOISE, int BOUND> struct WideOk {
+    static constexpr bool value =
+        !NOISE && MODEL != M_LEVY && MODEL != M_DFLEX && BOUND != SSM_BOUND_TABLE;
+};
 // Resident 256-thread CTAs per SM the compiler must fit (register cap
-// 65536 / (256 n)): 3 (80 registers) for blocks longer than 8 steps, 4 otherwise.
-template <int MODEL> struct MinCtas { static constexpr int value = Blk<MODEL>::value > 8 ? 3 : 4; };
+// 65536 / (256 n)): 3 (80 registers) for blocks longer than 8 steps, 4 otherwise
+// (and 4 for the lanes-per-walk mode, whose lanes hold 18 increments).
+template <int MODEL, int W = 1> struct MinCtas {
+    static constexpr int value = (W == 1 && Blk<MODEL>::value > 8) ? 3 : 4;
+};
 
 struct Lane {
     int64_t w;
@@ -452,20 +465,21 @@ __device__ __forceinline__ bool step_block(const SingleParams &p, Lane &L, const
 // additions' rounding; below 65536 dt an ulp of t is at most dt/64, so that
 // rounding stays under dt/4, and t + (BLK+1) dt <= dl_tmp, evaluated in float,
 // leaves more than that margin.
-template <int MODEL, int BOUND, bool NOISE>
+template <int MODEL, int BOUND, bool NOISE, int BLK = Blk<MODEL>::value>
 __device__ __forceinline__ bool block_in_time(const SingleParams &p, const Lane &L, const TrialRow &r) {
     constexpr bool INT_IX = NOISE || BOUND == SSM_BOUND_TABLE || MODEL == M_DFLEX;
     if (INT_IX) return false;
-    constexpr float SPAN = (float)(Blk<MODEL>::value + 1);
+    // longer blocks (lanes-per-walk mode, 36-144 steps) keep a margin of
+    // 2 dt per 64 steps: past 65536 dt an addition rounds by up to dt/64
+    constexpr float SPAN = (float)(BLK + 1 + 2 * (BLK / 64));
     return (L.tp < p.dt * 65536.f) && (fmaf(SPAN, p.dt, L.tp) <= r.dl_tmp);
 }
 
 // Steps taken by a walk that has ended.  Without an integer index L.ixf
 // counts whole blocks; the steps of the last block are those that took the
 // time accumulator from L.tpb to L.tp (the same float additions replayed).
-template <int MODEL, int BOUND, bool NOISE>
+template <int MODEL, int BOUND, bool NOISE, int BLK = Blk<MODEL>::value>
 __device__ __forceinline__ int steps_taken(const SingleParams &p, const Lane &L) {
-    constexpr int BLK = Blk<MODEL>::value;
     constexpr bool INT_IX = NOISE || BOUND == SSM_BOUND_TABLE || MODEL == M_DFLEX;
     if (INT_IX) return (int)L.ixf;
     float tt = L.tpb;
@@ -477,8 +491,8 @@ __device__ __forceinline__ int steps_taken(const SingleParams &p, const Lane &L)
     return (int)L.ixf - BLK + c;
 }
 
-template <int MODEL, int BOUND, bool NOISE>
-__device__ __forceinline__ void finalize(const SingleParams &p, const Lane &L) {
+template <int MODEL, int BOUND, bool NOISE, int BLK = Blk<MODEL>::value>
+__device__ __forceinline__ void finalize(const SingleParams &p, const Lane &L, bool writer = true) {
     // fields needed only here are re-read instead of being held across the walk
     const TrialRow *row = p.rows + L.k;
     const float t = __ldg(&row->t), deadline = __ldg(&row->deadline), dl = __ldg(&row->dl_tmp);
@@ -502,9 +516,10 @@ __device__ __forceinline__ void finalize(const SingleParams &p, const Lane &L) {
     float rt = __fadd_rn(__fadd_rn(L.tp, tt), sm);
     if (rt >= deadline || deadline <= 0.f) rt = -999.f;  // enforce_deadline
     const int choice = (L.y > 0.f) - (L.y < 0.f);         // sign(y)
+    if (!writer) return;
     p.rts[L.w] = rt;
     p.choices[L.w] = choice;
-    if (p.steps) p.steps[L.w] = steps_taken<MODEL, BOUND, NOISE>(p, L);
+    if (p.steps) p.steps[L.w] = steps_taken<MODEL, BOUND, NOISE, BLK>(p, L);
 }
 
 // Start lane L on the trajectory with queue index w; false (and the error
@@ -565,17 +580,93 @@ __device__ __forceinline__ bool lane_init(const SingleParams &p, Lane &L, TrialR
     return true;
 }
 
+// One block of the lanes-per-walk mode (W = 2, 4, 8; device RNG, in-register
+// boundaries).  The W lanes of an aligned group carry one trajectory and
+// hold identical state.  A block is 18 W steps: lane s of the group makes
+// Philox calls 3 W b + 3 s + m (m = 0, 1, 2) of block b -- the counters the
+// one-lane mode uses for the same steps -- and every lane of the group then
+// runs the block's steps in order, each increment broadcast by a shuffle from
+// the lane that drew it.  The warp issues about 8 instructions per step of
+// 32 / W walks instead of about 21 per step of 32: throughput traded for the
+// latency of one walk, which is what bounds a launch with fewer
+// trajectories than resident lanes.  18 W is a multiple of 36, so the linear
+// boundary comes from the same 36-step bases as in the one-lane mode and the
+// results are bit-identical to it.  Every lane of the warp takes part (the
+// shuffles need the whole warp); a lane without a running walk (`active`
+// false, possibly still holding an ended walk's state for finalize) changes
+// nothing.
+template <int MODEL, int BOUND, bool TCHK, int W>
+__device__ __forceinline__ bool wide_block(const SingleParams &p, Lane &L, const TrialRow &r, bool active,
+                                           int src0, int sub) {
+    static_assert(W == 2 || W == 4 || W == 8, "lanes per walk");
+    constexpr int BLK = 18 * W;
+    constexpr unsigned FULL = 0xffffffffu;
+    const bool capped = active && L.ixf >= r.capf;
+    if (capped) raise_error(p.hdr, SSM_ERR_DEVICE, (int)L.w);
+    bool live = active && !capped;
+    const float drift = DrawnDrift<MODEL>::value ? L.dinc : r.drift;
+    float g[18];
+#pragma unroll
+    for (int m = 0; m < 3; ++m) {
+        const uint4 b = philox10(
+            make_uint4((uint32_t)(3 * W) * L.blk + (uint32_t)(3 * sub + m), L.n, L.k + p.k_base, 0u), p.key);
+        bm6_increment(b, r.c2, drift, g + 6 * m);
+    }
+    const float ixf0 = L.ixf;
+    float b36[W / 2];  // linear boundary at the block's 36-step bases
+#pragma unroll
+    for (int u = 0; u < W / 2; ++u)
+        b36[u] = (BOUND == SSM_BOUND_LINEAR) ? fmaf(ixf0 + (float)(36 * u), r.dtp1, r.a) : 0.f;
+    if (live) L.tpb = L.tp;
+#pragma unroll
+    for (int s = 0; s < W; ++s) {
+#pragma unroll
+        for (int j = 0; j < 18; ++j) {
+            const float gq = __shfl_sync(FULL, g[j], src0 + s);
+            const int q = 18 * s + j;
+            const bool in_time = !TCHK || (L.tp <= r.dl_tmp);
+            bool inside;
+            if (MODEL == M_LEGACY) {
+                inside = live && (L.y <= r.a) && (L.y >= 0.f) && in_time;
+            } else {
+                float bq;
+                if (BOUND == SSM_BOUND_LINEAR)
+                    bq = (q % 36 == 0) ? b36[q / 36] : fmaf((float)(q % 36), r.dtp1, b36[q / 36]);
+                else
+                    bq = bound_at<BOUND, false>(r, ixf0 + (float)q, 0, p, L.k);
+                inside = live && (fabsf(L.y) <= bq) && in_time;
+            }
+            if (inside) {
+                if (MODEL == M_OU) L.y = fmaf(L.y, r.expo, gq);
+                else L.y += gq;
+                L.tp += p.dt;
+            }
+            live = inside;
+        }
+    }
+    if (active && !capped) L.ixf = ixf0 + (float)BLK;
+    return live;
+}
+
 // ------------------------------------------------------------------ main kernel
-template <int MODEL, int BOUND, bool NOISE>
-__global__ void __launch_bounds__(256, MinCtas<MODEL>::value) k_single(const __grid_constant__ SingleParams p) {
+// W lanes per walk (1 = one lane per trajectory; 2, 4, 8 = wide_block).  The
+// queue logic counts walks: a group's lanes share `active`, so a ballot of
+// free lanes holds W bits per free walk.
+template <int MODEL, int BOUND, bool NOISE, int W>
+__global__ void __launch_bounds__(256, (MinCtas<MODEL, W>::value))
+    k_single(const __grid_constant__ SingleParams p) {
+    static_assert(W == 1 || WideOk<MODEL, NOISE, BOUND>::value, "lanes per walk > 1: device RNG, in-register bound");
+    constexpr int BLK = BlkW<MODEL, W>::value;
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
-    const unsigned lt_mask = (1u << lane) - 1u;
+    const int sub = lane & (W - 1);              // place in the group
+    const int src0 = lane - sub;                 // the group's first lane
+    const unsigned lt_mask = (1u << src0) - 1u;  // lanes of the groups before this one
     const int64_t total = (p.total >= 0) ? p.total : __ldg(p.offsets + p.n_trials) - __ldg(p.offsets);
-    const int64_t chunk = warp_chunk(p.chunk, total);
+    const int64_t chunk = warp_chunk(p.chunk, total, 32 / W);
 
     Lane L;
-    TrialRow r;
+    TrialRow r = {};
     L.w = 0; L.k = L.n = L.blk = 0; L.ix = 0; L.y = L.tp = L.ixf = L.dinc = L.tpb = 0.f;
     bool active = false;
     bool pending = false;  // walk ended, result not yet written
@@ -588,13 +679,14 @@ __global__ void __launch_bounds__(256, MinCtas<MODEL>::value) k_single(const __g
         // rest of the warp idle, so it is done for several lanes in one pass.
         // Once the queue is empty, pending results are written at once.
         const unsigned need = __ballot_sync(FULL, !active);
-        const bool pass = exhausted ? (__ballot_sync(FULL, pending) != 0u) : (__popc(need) >= p.refill_min);
+        const int free_walks = __popc(need) / W;
+        const bool pass = exhausted ? (__ballot_sync(FULL, pending) != 0u) : (free_walks >= p.refill_min);
         if (pass && pending) {
-            finalize<MODEL, BOUND, NOISE>(p, L);
+            finalize<MODEL, BOUND, NOISE, BLK>(p, L, sub == 0);
             pending = false;
         }
         if (pass && !exhausted) {
-            const int cnt = __popc(need);
+            const int cnt = free_walks;
             const int64_t avail = q_end - q_next;
             int64_t base = 0;
             if (avail < cnt) {
@@ -604,7 +696,7 @@ __global__ void __launch_bounds__(256, MinCtas<MODEL>::value) k_single(const __g
                 if (base >= total) exhausted = true;
             }
             if (!active) {
-                const int rank = __popc(need & lt_mask);
+                const int rank = __popc(need & lt_mask) / W;
                 const int64_t w = (rank < avail) ? q_next + rank : base + (rank - avail);
                 if (w < total) active = lane_init<MODEL, NOISE>(p, L, r, w, hint);
             }
@@ -617,12 +709,20 @@ __global__ void __launch_bounds__(256, MinCtas<MODEL>::value) k_single(const __g
         }
         if (__ballot_sync(FULL, active) == 0u) break;
         // warp-uniform: skip the per-step time test when no active lane can reach its limit in this block
-        const bool skip_time = __all_sync(FULL, !active || block_in_time<MODEL, BOUND, NOISE>(p, L, r));
+        const bool skip_time = __all_sync(FULL, !active || block_in_time<MODEL, BOUND, NOISE, BLK>(p, L, r));
+        bool live = false;
+        if constexpr (W == 1) {
+            if (active) {
+                float g[Blk<MODEL>::value];
+                draw_block<MODEL, NOISE>(p, L, r, g);
+                live = skip_time ? step_block<MODEL, BOUND, NOISE, false, false>(p, L, r, g)
+                                 : step_block<MODEL, BOUND, NOISE, false, true>(p, L, r, g);
+            }
+        } else {
+            live = skip_time ? wide_block<MODEL, BOUND, false, W>(p, L, r, active, src0, sub)
+                             : wide_block<MODEL, BOUND, true, W>(p, L, r, active, src0, sub);
+        }
         if (active) {
-            float g[Blk<MODEL>::value];
-            draw_block<MODEL, NOISE>(p, L, r, g);
-            const bool live = skip_time ? step_block<MODEL, BOUND, NOISE, false, false>(p, L, r, g)
-                                        : step_block<MODEL, BOUND, NOISE, false, true>(p, L, r, g);
             L.blk += 1;
             if (!live) {
                 active = false;
@@ -654,22 +754,64 @@ __global__ void k_record(const __grid_constant__ SingleParams p) {
 }
 
 // ------------------------------------------------------------------ host side
+// Lanes per walk chosen when the caller leaves it at 0: the wide modes pay
+// where a launch holds about as many trajectories as the grid has lanes
+// (the walks' latency sets the time) and cost throughput beyond.
+int auto_lanes_per_walk(int64_t n_walks) {
+    if (n_walks <= 0) return 1;
+    const double per_lane = (double)n_walks / ((double)sm_count() * 768.0);  // 24 resident warps per SM
+    if (per_lane <= 0.25) return 8;
+    if (per_lane <= 1.5) return 4;
+    if (per_lane <= 4.0) return 2;
+    return 1;
+}
+
 struct Launcher {
+    template <int MODEL, int BOUND, bool NOISE, int W>
+    static int launch(const SingleParams &p, int threads, const ssm_launch *opt, cudaStream_t st) {
+        auto kern = k_single<MODEL, BOUND, NOISE, W>;
+        int per_sm = 0;
+        SSM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, 0));
+        if (opt && opt->blocks_per_sm > 0 && opt->blocks_per_sm < per_sm) per_sm = opt->blocks_per_sm;
+        if (per_sm < 1) per_sm = 1;
+        kern<<<sm_count() * per_sm, threads, 0, st>>>(p);
+        SSM_CUDA(cudaGetLastError());
+        return SSM_OK;
+    }
+
     template <int MODEL, int BOUND, bool NOISE>
     static int run(const SingleParams &p, const ssm_launch *opt, cudaStream_t st) {
-        auto kern = k_single<MODEL, BOUND, NOISE>;
         int threads = (opt && opt->block_threads > 0) ? opt->block_threads : 256;
         if (threads > 256 || threads % 32) {
             set_error("block_threads must be a multiple of 32 and at most 256");
             return SSM_ERR_ARG;
         }
-        int per_sm = 0;
-        SSM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, 0));
-        if (opt && opt->blocks_per_sm > 0 && opt->blocks_per_sm < per_sm) per_sm = opt->blocks_per_sm;
-        if (per_sm < 1) per_sm = 1;
-        const int grid = sm_count() * per_sm;
-        kern<<<grid, threads, 0, st>>>(p);
-        SSM_CUDA(cudaGetLastError());
+        constexpr bool WIDE = WideOk<MODEL, NOISE, BOUND>::value;
+        const int W = (opt && opt->lanes_per_walk > 0) ? opt->lanes_per_walk
+                                                        : (WIDE && p.total >= 0 ? auto_lanes_per_walk(p.total) : 1);
+        if (W != 1 && W != 2 && W != 4 && W != 8) {
+            set_error("lanes_per_walk must be 0 (automatic), 1, 2, 4 or 8");
+            return SSM_ERR_ARG;
+        }
+        if (W > 1 && !WIDE) {
+            set_error("lanes_per_walk > 1 needs the device RNG and a constant, linear or Weibull boundary");
+            return SSM_ERR_ARG;
+        }
+        int rc = SSM_OK;
+        if (W == 1) {
+            rc = launch<MODEL, BOUND, NOISE, 1>(p, threads, opt, st);
+        } else if constexpr (WIDE) {
+            // a warp holds 32 / W walks: it claims that many at a time and
+            // restarts a group as soon as its walk ends (unless told otherwise)
+            SingleParams q = p;
+            const int slots = 32 / W;
+            q.chunk = slots;
+            q.refill_min = (opt && opt->refill_min > 0) ? min(opt->refill_min, slots) : 1;
+            rc = (W == 2)   ? launch<MODEL, BOUND, NOISE, 2>(q, threads, opt, st)
+                 : (W == 4) ? launch<MODEL, BOUND, NOISE, 4>(q, threads, opt, st)
+                            : launch<MODEL, BOUND, NOISE, 8>(q, threads, opt, st);
+        }
+        if (rc != SSM_OK) return rc;
         if (p.traj && p.traj_len > 0) {
             SingleParams pr = p;  // trial 0 / sample 0, whatever the processing order
             pr.order = nullptr;
@@ -833,6 +975,7 @@ static int run_single(const SingleCall &c) {
 extern "C" {
 
 size_t ssm_ddm_workspace_bytes(int64_t n_trials) { return ssm::single_ws_bytes(n_trials); }
+int ssm_auto_lanes_per_walk(int64_t n_walks) { return ssm::auto_lanes_per_walk(n_walks); }
 
 int ssm_ddm_flexbound(const float *v, const float *a, const float *z, const float *t,
                       const float *deadline, const float *s, int64_t n_trials, int64_t n_samples,

@@ -73,6 +73,7 @@ def workspace(nbytes: int, tag: int = 0, stream: torch.cuda.Stream | None = None
 
 
 def launch_opts(block_threads: int = 0, blocks_per_sm: int = 0, chunk: int = 0,
-                first_trial: int = 0, refill_min: int = 0) -> _lib.SsmLaunch:
+                first_trial: int = 0, refill_min: int = 0, lanes_per_walk: int = 0) -> _lib.SsmLaunch:
     return _lib.SsmLaunch(block_threads=int(block_threads), blocks_per_sm=int(blocks_per_sm), chunk=int(chunk),
-                          refill_min=int(refill_min), first_trial=int(first_trial))
+                          refill_min=int(refill_min), first_trial=int(first_trial),
+                          lanes_per_walk=int(lanes_per_walk))

@@ -29,11 +29,20 @@ BOUND_WEIBULL = 3
 class SsmLaunch(C.Structure):
     """Mirror of ``ssm_launch`` (block size, CTAs per SM, warp chunk, ended walks a warp
     collects before restarting lanes, random-stream index of the call's first trial, device
-    pointers of an optional trial processing order and its sample-count prefix sums)."""
+    pointers of an optional trial processing order and its sample-count prefix sums, lanes
+    per trajectory of the single-accumulator simulators)."""
 
     _fields_ = [("block_threads", C.c_int), ("blocks_per_sm", C.c_int), ("chunk", C.c_int),
                 ("refill_min", C.c_int), ("first_trial", C.c_int64), ("trial_order", C.c_void_p),
-                ("order_offsets", C.c_void_p)]
+                ("order_offsets", C.c_void_p), ("lanes_per_walk", C.c_int)]
+
+
+def launch_replace(base: SsmLaunch, **fields) -> SsmLaunch:
+    """A copy of ``base`` with the given fields changed."""
+    out = SsmLaunch.from_buffer_copy(base)
+    for k, v in fields.items():
+        setattr(out, k, v)
+    return out
 
 
 class SsmError(RuntimeError):
@@ -56,6 +65,7 @@ _SIGNATURES: dict[str, tuple] = {
     "ssm_last_error": (C.c_char_p, []),
     "ssm_check_status": (_I, [_P, _P]),
     "ssm_ddm_workspace_bytes": (C.c_size_t, [_I64]),
+    "ssm_auto_lanes_per_walk": (C.c_int, [_I64]),
     "ssm_ddm_flexbound": (_I, [_P, _P, _P, _P, _P, _P, _I64, _I64, _P, _F, _P, _F, _I, _P, _P, _P,
                                _I64, _I64, _U64, _I, _P, _I64, _P, _P, _P, _P, _P, _I64, _P, _P,
                                C.c_size_t, _P]),

@@ -108,11 +108,9 @@ def longest_first(expected_time, n_samples) -> tuple[np.ndarray, np.ndarray]:
 def with_order(base, order_t=None, qoff_t=None, first_trial: int | None = None) -> _lib.SsmLaunch:
     """A copy of the launch options with the given trial order (device tensors
     the caller keeps alive while the launch runs)."""
-    return _lib.SsmLaunch(block_threads=base.block_threads, blocks_per_sm=base.blocks_per_sm, chunk=base.chunk,
-                          refill_min=base.refill_min,
-                          first_trial=base.first_trial if first_trial is None else int(first_trial),
-                          trial_order=None if order_t is None else order_t.data_ptr(),
-                          order_offsets=None if qoff_t is None else qoff_t.data_ptr())
+    return _lib.launch_replace(base, first_trial=base.first_trial if first_trial is None else int(first_trial),
+                               trial_order=None if order_t is None else order_t.data_ptr(),
+                               order_offsets=None if qoff_t is None else qoff_t.data_ptr())
 
 
 class BatchedSimulator:

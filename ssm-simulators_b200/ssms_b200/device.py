@@ -131,6 +131,12 @@ def simulate_single(model: str, *, v, z, t, deadline, s, a=None, alpha=None, sv=
             traj.fill_(-999.0)
         return SimOutput(rts=rts, choices=chs, steps=steps, traj=traj, workspace=ws)
     lopt = launch if launch is not None else launch_for(model)
+    if (offs is not None and lopt.lanes_per_walk == 0 and noise_rows is None
+            and model not in (MODEL_LEVY, MODEL_DFLEX)
+            and (model == MODEL_LEGACY or int(bound_kind) != _lib.BOUND_TABLE)):
+        # the library picks lanes per walk itself only where it knows the
+        # total (reference layout); a ragged call passes the same rule's choice
+        lopt = _lib.launch_replace(lopt, lanes_per_walk=L.ssm_auto_lanes_per_walk(total))
     sp = D.stream_ptr(stream)
     common_tail = (
         _lib.U64_cast(seed), int(bool(smooth_unif)), D.ptr(nrows), nlen, D.ptr(nunif),

@@ -81,4 +81,6 @@ def test_launch_struct_layout_matches_the_header(tmp_path):
     assert got[0] == ctypes.sizeof(_lib.SsmLaunch)
     assert got[1:] == [getattr(_lib.SsmLaunch, f).offset for f in fields]
     assert getattr(_lib.SsmLaunch, "first_trial").offset == 16  # unchanged by refill_min (padding slot)
-    assert ctypes.sizeof(_lib.SsmLaunch) == 40
+    # lanes_per_walk was appended: every earlier field keeps its offset
+    assert getattr(_lib.SsmLaunch, "lanes_per_walk").offset == 40
+    assert ctypes.sizeof(_lib.SsmLaunch) == 48
