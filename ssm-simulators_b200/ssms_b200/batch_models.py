@@ -18,7 +18,9 @@ from . import _device as D
 from . import boundary_functions as bf
 from . import device as dev
 from . import drift_functions as dfn
-from .batch import expected_race_time, expected_walk_time, longest_first, with_order
+from . import _lib
+from .batch import (expected_race_time, expected_walk_time, lanes_per_walk_for, longest_first, wide_family,
+                    with_order)
 from .tuning import launch_for
 
 SINGLE = ("ddm_flexbound", "levy_flexbound", "ddm", "full_ddm", "ddm_sdv", "ornstein_uhlenbeck", "ddm_flex")
@@ -140,6 +142,15 @@ class SetBatch:
             self.t, self.deadline = _dev(_col(kwargs["t"], K), K), _dev(_col(kwargs["deadline"], K), K)
         else:
             raise ValueError(f"no batched device path for simulator {sim_name!r}")
+        self.lanes_per_walk = 0
+        if sim_name in SINGLE and wide_family(sim_name, self.kind):
+            cap = np.minimum(float(max_t), np.maximum(np.asarray(_col(kwargs["deadline"], K), np.float64)
+                                                      - np.asarray(_col(kwargs["t"], K), np.float64), 0.0))
+            e, walk_cap = expected_walk_time(
+                _col(kwargs["v"], K), spec["a"], _col(kwargs["z"], K), _col(kwargs["s"], K),
+                legacy=sim_name == "ddm", bound_kind=self.kind, p1=spec["p1"], p2=spec["p2"], t_cap=cap,
+                return_cap=True)
+            self.lanes_per_walk = lanes_per_walk_for(e, walk_cap, ns, delta_t)
         est = expected_set_time(sim_name, kwargs, spec, K, max_t) if K > 1 else None
         if est is not None:  # sets longest-first (outputs do not depend on the order)
             o, q = longest_first(est, ns)
@@ -150,6 +161,8 @@ class SetBatch:
         if self.sim_name != "lba_vanilla":
             if launch is None:
                 launch = launch_for(self.sim_name)
+            if self.lanes_per_walk and launch.lanes_per_walk == 0:
+                launch = _lib.launch_replace(launch, lanes_per_walk=self.lanes_per_walk)
             if self.order_t is not None and not launch.trial_order:
                 launch = with_order(launch, self.order_t, self.qoff_t)
         if self.sim_name in SINGLE:
