@@ -17,6 +17,10 @@
 //    increments, already scaled to drift + s sqrt(dt) N(0,1); the steps
 //    themselves are predicated (no per-step branch), and a warp whose walks
 //    cannot reach their time limit within the block skips the time test.
+//  * A launch with about as many trajectories as the grid has lanes lasts as
+//    long as its longest walk.  There W = 2, 4 or 8 lanes share a walk
+//    (ssm_launch.lanes_per_walk, wide_block): each draws a third of the
+//    block's increments and all step it, bit-identical to one lane per walk.
 //  * Boundaries are evaluated in registers (constant / linear collapse /
 //    Weibull) or read from a caller-evaluated table for arbitrary shapes.
 //  * Noise injection replaces the generator by caller rows and switches every
