@@ -52,6 +52,37 @@ def to_dev_f32(x, n: int | None = None, name: str = "array") -> torch.Tensor:
     return t
 
 
+def to_dev_f32_rows(xs: dict, n: int) -> dict:
+    """Several per-trial inputs as float32 CUDA tensors of n entries, the host
+    ones uploaded together: one page-locked staging buffer, one copy (each
+    separate pageable upload blocks the host for a round trip).  Entries that
+    are None stay None; device tensors and other lengths go through
+    ``to_dev_f32``.  The staging block is recycled by torch's caching host
+    allocator only after the copy has completed."""
+    out, host = {}, []
+    for name, x in xs.items():
+        if x is None:
+            out[name] = None
+        elif isinstance(x, torch.Tensor):
+            out[name] = to_dev_f32(x, n, name)
+        else:
+            arr = np.asarray(x, dtype=np.float32).reshape(-1)
+            if arr.size != n:
+                out[name] = to_dev_f32(arr, n, name)
+            else:
+                host.append((name, arr))
+    if host:
+        dev = require_cuda()
+        stage = torch.empty((len(host), n), dtype=torch.float32, pin_memory=True)
+        sv = stage.numpy()
+        for i, (_, arr) in enumerate(host):
+            sv[i] = arr
+        d = stage.to(dev, non_blocking=True)
+        for i, (name, _) in enumerate(host):
+            out[name] = d[i]
+    return out
+
+
 def workspace(nbytes: int, tag: int = 0, stream: torch.cuda.Stream | None = None) -> torch.Tensor:
     """A cached, 256-byte aligned device scratch buffer of at least ``nbytes``.
 

@@ -51,27 +51,34 @@ def _minimal_meta(name, choices, n_samples, n_trials, boundary_name=None):
     return meta
 
 
-def _host(x) -> np.ndarray:
-    """A device result as a numpy array, copied through page-locked memory:
-    the copy runs at the link's speed instead of through the driver's
-    pageable staging (about 2-3 GB/s, which made the copy of a 1e7-trajectory
-    result the larger part of a call).  torch's caching host allocator hands
-    the buffer out again once the returned array is released."""
+def _hosts(*xs) -> list:
+    """Several device results as numpy arrays: every copy is queued into its
+    own page-locked buffer and the stream is synchronised once (None stays
+    None).  Page-locked copies run at the link's speed; the driver's pageable
+    staging (about 2-3 GB/s) made the copy of a 1e7-trajectory result the
+    larger part of a call.  torch's caching host allocator hands a buffer out
+    again once its returned array is released."""
     import torch
 
-    if not x.is_cuda:
-        return x.numpy()
-    h = torch.empty(x.shape, dtype=x.dtype, pin_memory=True)
-    h.copy_(x, non_blocking=True)
-    torch.cuda.current_stream(x.device).synchronize()
-    return h.numpy()
+    bufs = []
+    for x in xs:
+        if x is None or not x.is_cuda:
+            bufs.append(x)
+            continue
+        h = torch.empty(x.shape, dtype=x.dtype, pin_memory=True)
+        h.copy_(x, non_blocking=True)
+        bufs.append(h)
+    if any(x is not None and x.is_cuda for x in xs):
+        torch.cuda.current_stream().synchronize()
+    return [None if b is None else b.numpy() for b in bufs]
 
 
-def _traj_host(traj_t, n):
-    traj = np.full((n, 1), -999, dtype=DTYPE)
-    if traj_t is not None:
-        traj[:, 0] = traj_t.cpu().numpy()[:n]
-    return traj
+def _traj_host(traj, n):
+    """The recorded path (host array or None) as the reference's [n, 1] column, -999 padded."""
+    out = np.full((n, 1), -999, dtype=DTYPE)
+    if traj is not None:
+        out[:, 0] = np.asarray(traj)[:n]
+    return out
 
 
 def _run_flex(model, v, a, z, t, deadline, s, levy_alpha, max_t, delta_t, n_samples, n_trials,
@@ -102,11 +109,13 @@ def _run_flex(model, v, a, z, t, deadline, s, levy_alpha, max_t, delta_t, n_samp
         bound_p1=spec["p1"], bound_p2=spec["p2"], bound_table=spec["table"],
         seed=_seed(random_state), smooth_unif=smooth_unif,
         traj_len=nd if (full and n_trials > 0 and n_samples > 0) else 0)
-    rts = _host(out.rts).reshape(n_samples, n_trials, 1)
-    choices = _host(out.choices).reshape(n_samples, n_trials, 1)
+    # the metadata is built on the host while the launch runs; the results
+    # are then copied with one synchronisation
     minimal = _minimal_meta(model, [-1, 1], n_samples, n_trials, boundary_fun.__name__)
     if not full:
-        return {"rts": rts, "choices": choices, "metadata": minimal}
+        rts, choices = _hosts(out.rts, out.choices)
+        return {"rts": rts.reshape(n_samples, n_trials, 1), "choices": choices.reshape(n_samples, n_trials, 1),
+                "metadata": minimal}
     meta = dict(minimal)
     if meta_params is not None:
         meta.update(meta_params)
@@ -122,10 +131,12 @@ def _run_flex(model, v, a, z, t, deadline, s, levy_alpha, max_t, delta_t, n_samp
         bp0 = {key: np.asarray(val)[0] for key, val in boundary_params.items()}
         boundary[:] = np.asarray(boundary_fun(t=t_s, **bp0)).astype(DTYPE)
     meta["boundary"] = boundary
-    meta["trajectory"] = _traj_host(out.traj, nd)
     if boundary_params:
         meta.update(boundary_params)
-    return {"rts": rts, "choices": choices, "metadata": meta}
+    rts, choices, traj = _hosts(out.rts, out.choices, out.traj)
+    meta["trajectory"] = _traj_host(traj, nd)
+    return {"rts": rts.reshape(n_samples, n_trials, 1), "choices": choices.reshape(n_samples, n_trials, 1),
+            "metadata": meta}
 
 
 def ddm_flexbound(v, a, z, t, deadline, s, max_t=20, delta_t=0.001, n_samples=20000,
@@ -230,15 +241,15 @@ def ddm(v, a, z, t, deadline, s, max_t=20, delta_t=0.001, n_samples=20000, n_tri
         "ddm", v=v, z=z, t=t, deadline=deadline, s=s, a=a, n_trials=n_trials,
         n_samples=n_samples, max_t=max_t, delta_t=delta_t, seed=_seed(random_state),
         smooth_unif=smooth_unif, traj_len=nd if (full and n_trials > 0 and n_samples > 0) else 0)
-    rts = _host(out.rts).reshape(n_samples, n_trials, 1)
-    choices = _host(out.choices).reshape(n_samples, n_trials, 1)
     minimal = _minimal_meta("ddm", [-1, 1], n_samples, n_trials, "constant")
+    rts, choices, traj = _hosts(out.rts, out.choices, out.traj if full else None)
+    rts, choices = rts.reshape(n_samples, n_trials, 1), choices.reshape(n_samples, n_trials, 1)
     if not full:
         return {"rts": rts, "choices": choices, "metadata": minimal}
     meta = dict(minimal)
     meta.update({"v": v, "a": a, "z": z, "t": t, "deadline": deadline, "s": s})
     meta.update({"delta_t": float(np.float32(delta_t)), "max_t": max_t, "n_threads": 1})
-    meta["trajectory"] = _traj_host(out.traj, nd)
+    meta["trajectory"] = _traj_host(traj, nd)
     return {"rts": rts, "choices": choices, "metadata": meta}
 
 
@@ -269,8 +280,7 @@ def _run_race(model, v, z, t, s, deadline, g, b, delta_t, max_t, n_samples, n_tr
         max_t=max_t, delta_t=delta_t, bound_kind=spec["kind"], a=spec["a"], bound_p1=spec["p1"],
         bound_p2=spec["p2"], bound_table=spec["table"], seed=_seed(random_state),
         smooth_unif=smooth_unif, traj_len=n_rows * n_part if (full and n_trials and n_samples) else 0)
-    rts = _host(out.rts).reshape(n_samples, n_trials, 1)
-    choices = _host(out.choices).reshape(n_samples, n_trials, 1)
+    rts, choices = (x.reshape(n_samples, n_trials, 1) for x in _hosts(out.rts, out.choices))
     # the reference reports [-1, 1] in minimal metadata and 0..n-1 in full metadata
     minimal = _minimal_meta(model, [-1, 1], n_samples, n_trials, boundary_fun.__name__)
     if not full:
@@ -336,8 +346,7 @@ def racing_diffusion_model(v, b, A, t, s, deadline, delta_t=0.001, max_t=20, n_s
                            n_samples=n_samples, max_t=max_t, delta_t=delta_t, seed=_seed(random_state),
                            smooth_unif=smooth_unif,
                            traj_len=n_rows * n_part if (full and n_trials and n_samples) else 0)
-    rts = _host(out.rts).reshape(n_samples, n_trials, 1)
-    choices = _host(out.choices).reshape(n_samples, n_trials, 1)
+    rts, choices = (x.reshape(n_samples, n_trials, 1) for x in _hosts(out.rts, out.choices))
     minimal = _minimal_meta("rdm_simulator", list(np.arange(0, n_part, 1)), n_samples, n_trials)
     if not full:
         return {"rts": rts, "choices": choices, "metadata": minimal}
@@ -367,8 +376,7 @@ def lba_vanilla(v, a, z, deadline, sd, t, nact=3, n_samples=2000, n_trials=1, ma
     out = dev.simulate_lba(v=v, a=a[:, 0], z=z[:, 0], deadline=deadline, sd=sd, t=t,
                            n_trials=n_trials, n_samples=n_samples,
                            seed=_seed(kwargs.get("random_state")))
-    rts = _host(out.rts).reshape(n_samples, n_trials, 1)
-    choices = _host(out.choices).reshape(n_samples, n_trials, 1)
+    rts, choices = (x.reshape(n_samples, n_trials, 1) for x in _hosts(out.rts, out.choices))
     meta = _minimal_meta("lba_vanilla", list(np.arange(0, nact, 1)), n_samples, n_trials)
     meta.update({"a": a, "z": z, "deadline": deadline, "sd": sd, "t": t})
     meta.update({"max_t": max_t, "n_threads": 1})

@@ -80,17 +80,13 @@ def simulate_single(model: str, *, v, z, t, deadline, s, a=None, alpha=None, sv=
     """
     dev = D.require_cuda()
     K = int(n_trials)
-    vt = D.to_dev_f32(v, K, "v")
-    zt = D.to_dev_f32(z, K, "z")
-    tt = D.to_dev_f32(t, K, "t")
-    dlt = D.to_dev_f32(deadline, K, "deadline")
-    s_t = D.to_dev_f32(s, K, "s")
-    at = D.to_dev_f32(a if a is not None else np.ones(K, np.float32), K, "a")
-    alt = _opt_f32(alpha, K, "alpha")
-    svt, szt, stt, gt = (_opt_f32(x, K, nm) for x, nm in ((sv, "sv"), (sz, "sz"), (st, "st"), (g, "g")))
-    p1t = _opt_f32(bound_p1, K, "bound_p1")
-    p2t = _opt_f32(bound_p2, K, "bound_p2")
-    mtk = _opt_f32(max_t_per_trial, K, "max_t_per_trial")
+    up = D.to_dev_f32_rows({
+        "v": v, "z": z, "t": t, "deadline": deadline, "s": s,
+        "a": a if a is not None else np.ones(K, np.float32), "alpha": alpha, "sv": sv, "sz": sz, "st": st,
+        "g": g, "bound_p1": bound_p1, "bound_p2": bound_p2, "max_t_per_trial": max_t_per_trial}, K)
+    vt, zt, tt, dlt, s_t, at = (up[k] for k in ("v", "z", "t", "deadline", "s", "a"))
+    alt, svt, szt, stt, gt = (up[k] for k in ("alpha", "sv", "sz", "st", "g"))
+    p1t, p2t, mtk = up["bound_p1"], up["bound_p2"], up["max_t_per_trial"]
     tab = None
     tstride = tlen = 0
     if bound_table is not None:
