@@ -8,12 +8,14 @@ ssms/dataset_generators/lan_mlp.py:66-133), so this oracle restates the model
 the device kernels define:
 
     x~  = (x - c) * s                 split x~ = hi + lo, both rounded to bf16
-    h1  = bf(tanh(bf(W1) (hi + lo) + b1))
-    h2  = bf(tanh(bf(W2) h1 + b2))
-    h3  = tanh(bf(W3) h2 + b3)
+    h1  = bf(tanh(bf(W1) (hi + lo) + bb(b1)))
+    h2  = bf(tanh(bf(W2) h1 + bb(b2)))
+    h3  = tanh(bf(W3) h2 + bb(b3))
     out = w4 . h3 + b4                (fp32 output layer)
 
-bf(.) is round-to-nearest-even to bfloat16.  The backward mirrors the kernels
+bf(.) is round-to-nearest-even to bfloat16; bb(b) = bf(b) + bf(b - bf(b)), the
+bias as the two bf16 weight columns the kernels multiply by their two ones
+columns.  The backward mirrors the kernels
 too: every operand of a tensor-core GEMM is rounded to bf16 (G3, G2, G1, the
 output gradient, the stored activations) and derivatives of tanh use the bf16
 activations that the kernels read back, except G3 of d out / d x, which the
@@ -95,13 +97,18 @@ def pack_image(p):
     """The packed weight image (uint8 [IMAGE_BYTES]) the device kernels read."""
     W1, b1, W2, b2, W3, b3, w4, b4 = unpack(np.asarray(p, np.float32))
     img = np.zeros(IMAGE_BYTES, np.uint8)
-    for (off, R, W, dup) in ((OFF_W1, N1, W1, True), (OFF_W2, N2, W2, False), (OFF_W3, N3, W3, False)):
+    for (off, R, W, b, ones, dup) in ((OFF_W1, N1, W1, b1, 2 * DIN, True), (OFF_W2, N2, W2, b2, H1, False),
+                                      (OFF_W3, N3, W3, b3, H2, False)):
         t = img[off:].view(np.uint16)
         rows, cols = np.meshgrid(np.arange(W.shape[0]), np.arange(W.shape[1]), indexing="ij")
         bits = _bf16_bits(W.astype(np.float32))
         t[_tile_index(R, rows, cols)] = bits
         if dup:
             t[_tile_index(R, rows, cols + DIN)] = bits
+        hi, lo = bias_split(b)
+        r = np.arange(W.shape[0])
+        t[_tile_index(R, r, ones)] = _bf16_bits(hi.astype(np.float32))
+        t[_tile_index(R, r, ones + 1)] = _bf16_bits(lo.astype(np.float32))
     f = img.view(np.float32)
     f[OFF_B1 // 4:OFF_B1 // 4 + H1] = b1
     f[OFF_B2 // 4:OFF_B2 // 4 + H2] = b2
@@ -113,6 +120,20 @@ def pack_image(p):
 
 def _q(x, quantize):
     return bf16(x) if quantize else np.asarray(x, np.float64)
+
+
+def bias_split(b):
+    """(hi, lo): the bias's two bf16 weight columns, hi = bf(b), lo = bf(b - hi)."""
+    b = np.asarray(b, np.float32)
+    hi = bf16(b)
+    return hi, bf16((b - hi.astype(np.float32)).astype(np.float32))
+
+
+def _qb(b, quantize):
+    if not quantize:
+        return np.asarray(b, np.float64)
+    hi, lo = bias_split(b)
+    return hi + lo
 
 
 def _hidden(pre, quantize):
@@ -134,9 +155,9 @@ def forward(p, x, norm_c, norm_s, *, quantize=True, want_dx=False):
         xin = hi + lo
     else:
         xin = xt.astype(np.float64)
-    h1q = _hidden(xin @ W1q.T + b1, quantize)
-    h2q = _hidden(h1q @ W2q.T + b2, quantize)
-    h3 = np.tanh(h2q @ W3q.T + b3)
+    h1q = _hidden(xin @ W1q.T + _qb(b1, quantize), quantize)
+    h2q = _hidden(h1q @ W2q.T + _qb(b2, quantize), quantize)
+    h3 = np.tanh(h2q @ W3q.T + _qb(b3, quantize))
     out = h3 @ w4 + b4
     if not want_dx:
         return out
@@ -164,9 +185,9 @@ def train_grad(p, rec, norm_c, norm_s, *, loss="huber", inv_batch=None, quantize
         xin = hi + lo
     else:
         xin = xt.astype(np.float64)
-    h1q = _hidden(xin @ W1q.T + b1, quantize)
-    h2q = _hidden(h1q @ W2q.T + b2, quantize)
-    h3 = np.tanh(h2q @ W3q.T + b3)
+    h1q = _hidden(xin @ W1q.T + _qb(b1, quantize), quantize)
+    h2q = _hidden(h1q @ W2q.T + _qb(b2, quantize), quantize)
+    h3 = np.tanh(h2q @ W3q.T + _qb(b3, quantize))
     h3q = _q(h3, quantize)
     out = h3 @ w4 + b4
     e = out - rec[:, DIN].astype(np.float64)

@@ -13,7 +13,12 @@
 //   layer 3  [128 x 112] x W3^T [112 x 128]  -> acc 128 cols
 //   output   h3 . w4 + b4 on the FP32 pipe (120 terms, fp32 weights)
 // Inputs are normalised x~ = (x - c) * s and split x~ = hi + lo into two bf16
-// columns each, so the first layer sees ~16 significant bits of rt.
+// columns each, so the first layer sees ~16 significant bits of rt.  The
+// hidden layers' biases ride in the GEMMs the same way: every layer input
+// carries two ones columns (14 and 15 of the input tile, 100 and 101 of the
+// hidden tiles) against weight columns holding bf16(b) and bf16(b - bf16(b)),
+// so the fp32 accumulator starts from b to ~16 bits and the epilogues, whose
+// shared-memory and SFU queue is the forward pass's bottleneck, add nothing.
 //
 // Shared-memory operand layout ("chunk-major", no swizzle): an R x C bf16 tile
 // stores element (r, c) at byte (c / 8) * (R * 16) + r * 16 + (c % 8) * 2, i.e.
@@ -38,13 +43,14 @@ namespace mlp {
 
 constexpr int DIN = 7, H1 = 100, H2 = 100, H3 = 120;
 constexpr int K0 = 16, N1 = 112, N2 = 112, N3 = 128;
-constexpr int ONES1 = 100, ONES3 = 120, ONES0 = 14;  // ones columns (bias gradients)
+constexpr int ONES1 = 100, ONES3 = 120, ONES0 = 14;  // ones columns (bias terms and bias gradients)
 
 // bf16 weight image (device global and shared memory), byte offsets
 constexpr int OFF_W1 = 0;                       // 112 rows x 16 cols
 constexpr int OFF_W2 = OFF_W1 + N1 * K0 * 2;    // 112 x 112
 constexpr int OFF_W3 = OFF_W2 + N2 * N1 * 2;    // 128 x 112
-constexpr int OFF_B1 = OFF_W3 + N3 * N2 * 2;    // fp32 [112]
+constexpr int OFF_B1 = OFF_W3 + N3 * N2 * 2;    // fp32 [112] (the biases in fp32; the kernels use the
+                                                // bf16 hi/lo columns of W1-W3)
 constexpr int OFF_B2 = OFF_B1 + N1 * 4;         // fp32 [112]
 constexpr int OFF_B3 = OFF_B2 + N2 * 4;         // fp32 [128]
 constexpr int OFF_W4 = OFF_B3 + N3 * 4;         // fp32 [128]
@@ -248,7 +254,7 @@ __device__ __forceinline__ uint4 ld_row(const uint8_t *tile, int chunk, int r) {
 }
 
 // ------------------------------------------------------------ epilogue pieces
-// x row -> normalised, split hi/lo -> X tile (cols 0-6 hi, 7-13 lo, 14 = 1).
+// x row -> normalised, split hi/lo -> X tile (cols 0-6 hi, 7-13 lo, 14 = 15 = 1).
 __device__ __forceinline__ void stage_x(uint8_t *X, int r, const float *xr, bool valid, const Norm &nm) {
     float hi[7], lo[7];
 #pragma unroll
@@ -258,19 +264,19 @@ __device__ __forceinline__ void stage_x(uint8_t *X, int r, const float *xr, bool
         lo[j] = v - hi[j];
     }
     uint4 c0 = {pack2(hi[0], hi[1]), pack2(hi[2], hi[3]), pack2(hi[4], hi[5]), pack2(hi[6], lo[0])};
-    uint4 c1 = {pack2(lo[1], lo[2]), pack2(lo[3], lo[4]), pack2(lo[5], lo[6]), pack2(1.f, 0.f)};
+    uint4 c1 = {pack2(lo[1], lo[2]), pack2(lo[3], lo[4]), pack2(lo[5], lo[6]), pack2(1.f, 1.f)};
     st_row(X, 0, r, c0);
     st_row(X, 1, r, c1);
 }
 
-// Hidden layers 1 and 2: tanh(acc + bias) in fp32 (tanh.approx.f32), rounded
-// to bf16 pairs -> bf16 tile.  Columns from H (the real width) on are padding:
-// written as zeros without a tanh, except the ones column.  Optionally the
-// packed pairs are also stashed in TMEM at ts.  (tanh.approx.bf16x2 was
-// measured: it costs the XU pipe as much as two fp32 tanh, so it buys nothing.)
+// Hidden layers 1 and 2: tanh(acc) in fp32 (tanh.approx.f32; the bias is in
+// acc already), rounded to bf16 pairs -> bf16 tile.  Columns from H (the real
+// width) on are padding: written as zeros without a tanh, except the two ones
+// columns.  Optionally the packed pairs are also stashed in TMEM at ts.
+// (tanh.approx.bf16x2 was measured: it costs the XU pipe as much as two fp32
+// tanh, so it buys nothing.)
 template <bool EDGE, int H, int ONES, bool STASH>
-__device__ __forceinline__ void hidden_chunk(int c, uint32_t ta, const float4 *b4v, uint8_t *dst, int r,
-                                             uint32_t ts) {
+__device__ __forceinline__ void hidden_chunk(int c, uint32_t ta, uint8_t *dst, int r, uint32_t ts) {
     float v[16];
     tmem_ld16(ta + 16 * c, v);
     uint32_t p[8];
@@ -280,14 +286,13 @@ __device__ __forceinline__ void hidden_chunk(int c, uint32_t ta, const float4 *b
         if (EDGE && col >= H) {
             p[2 * q] = p[2 * q + 1] = 0u;
         } else {
-            const float4 b = b4v[col / 4];
-            p[2 * q] = pack2(tanh_fast(v[4 * q] + b.x), tanh_fast(v[4 * q + 1] + b.y));
-            p[2 * q + 1] = pack2(tanh_fast(v[4 * q + 2] + b.z), tanh_fast(v[4 * q + 3] + b.w));
+            p[2 * q] = pack2(tanh_fast(v[4 * q]), tanh_fast(v[4 * q + 1]));
+            p[2 * q + 1] = pack2(tanh_fast(v[4 * q + 2]), tanh_fast(v[4 * q + 3]));
         }
         if (EDGE) {
 #pragma unroll
             for (int e = 0; e < 4; ++e)
-                if (col + e == ONES) {
+                if (col + e == ONES || col + e == ONES + 1) {
                     uint32_t &w = p[2 * q + e / 2];
                     w = (e & 1) ? ((w & 0x0000FFFFu) | (BF16_ONE << 16)) : ((w & 0xFFFF0000u) | BF16_ONE);
                 }
@@ -299,12 +304,11 @@ __device__ __forceinline__ void hidden_chunk(int c, uint32_t ta, const float4 *b
 }
 
 template <int NC, int H, int ONES, bool STASH>
-__device__ __forceinline__ void epi_hidden(uint32_t ta, const float *bias, uint8_t *dst, int r, uint32_t ts) {
-    static_assert(H > NC - 16 && ONES >= NC - 16 && ONES < NC, "padding and ones column lie in the last chunk");
-    const float4 *b4v = reinterpret_cast<const float4 *>(bias);
+__device__ __forceinline__ void epi_hidden(uint32_t ta, uint8_t *dst, int r, uint32_t ts) {
+    static_assert(H > NC - 16 && ONES >= NC - 16 && ONES + 1 < NC, "padding and ones columns lie in the last chunk");
 #pragma unroll 1
-    for (int c = 0; c < NC / 16 - 1; ++c) hidden_chunk<false, H, ONES, STASH>(c, ta, b4v, dst, r, ts);
-    hidden_chunk<true, H, ONES, STASH>(NC / 16 - 1, ta, b4v, dst, r, ts);
+    for (int c = 0; c < NC / 16 - 1; ++c) hidden_chunk<false, H, ONES, STASH>(c, ta, dst, r, ts);
+    hidden_chunk<true, H, ONES, STASH>(NC / 16 - 1, ta, dst, r, ts);
 }
 
 // G = D (TMEM, NC cols) * (1 - h^2) with h read from this row of H; G -> dst
@@ -349,12 +353,11 @@ __device__ __forceinline__ void epi_dtanh_stash(uint32_t ta, uint32_t ts, uint8_
     }
 }
 
-// Layer-3 epilogue: h3 = tanh(acc + b3) in fp32, out = b4 + h3 . w4 (fp32),
+// Layer-3 epilogue: h3 = tanh(acc) in fp32 (b3 is in acc), out = b4 + h3 . w4 (fp32),
 // and per KIND: 0 nothing else, 1 G3 = w4 (1 - h3^2) -> dst (d out / d acc3),
 // 2 bf16 h3 with the ones column -> dst (training operand).
 template <int KIND, bool EDGE>
-__device__ __forceinline__ void out_chunk(int c, uint32_t ta, const float4 *b3v, const float4 *w4v, float &o,
-                                          uint8_t *dst, int r) {
+__device__ __forceinline__ void out_chunk(int c, uint32_t ta, const float4 *w4v, float &o, uint8_t *dst, int r) {
     float v[16];
     tmem_ld16(ta + 16 * c, v);
     uint32_t p[8];
@@ -363,11 +366,11 @@ __device__ __forceinline__ void out_chunk(int c, uint32_t ta, const float4 *b3v,
         const int col = 16 * c + 4 * q;
         float h[4] = {0.f, 0.f, 0.f, 0.f}, w[4] = {0.f, 0.f, 0.f, 0.f};
         if (!EDGE || col < H3) {
-            const float4 b = b3v[col / 4], ww = w4v[col / 4];
-            h[0] = tanh_fast(v[4 * q] + b.x);
-            h[1] = tanh_fast(v[4 * q + 1] + b.y);
-            h[2] = tanh_fast(v[4 * q + 2] + b.z);
-            h[3] = tanh_fast(v[4 * q + 3] + b.w);
+            const float4 ww = w4v[col / 4];
+            h[0] = tanh_fast(v[4 * q]);
+            h[1] = tanh_fast(v[4 * q + 1]);
+            h[2] = tanh_fast(v[4 * q + 2]);
+            h[3] = tanh_fast(v[4 * q + 3]);
             w[0] = ww.x; w[1] = ww.y; w[2] = ww.z; w[3] = ww.w;
 #pragma unroll
             for (int e = 0; e < 4; ++e) o = fmaf(w[e], h[e], o);
@@ -389,15 +392,13 @@ __device__ __forceinline__ void out_chunk(int c, uint32_t ta, const float4 *b3v,
 }
 
 template <int KIND>
-__device__ __forceinline__ float epi_out(uint32_t ta, const float *b3, const float *w4, float b4, uint8_t *dst,
-                                         int r) {
+__device__ __forceinline__ float epi_out(uint32_t ta, const float *w4, float b4, uint8_t *dst, int r) {
     static_assert(H3 > N3 - 16 && ONES3 >= N3 - 16, "padding and ones column lie in the last chunk");
-    const float4 *b3v = reinterpret_cast<const float4 *>(b3);
     const float4 *w4v = reinterpret_cast<const float4 *>(w4);
     float o = b4;
 #pragma unroll 1
-    for (int c = 0; c < N3 / 16 - 1; ++c) out_chunk<KIND, false>(c, ta, b3v, w4v, o, dst, r);
-    out_chunk<KIND, true>(N3 / 16 - 1, ta, b3v, w4v, o, dst, r);
+    for (int c = 0; c < N3 / 16 - 1; ++c) out_chunk<KIND, false>(c, ta, w4v, o, dst, r);
+    out_chunk<KIND, true>(N3 / 16 - 1, ta, w4v, o, dst, r);
     return o;
 }
 
@@ -418,9 +419,6 @@ k_mlp(const uint8_t *__restrict__ image, const float *__restrict__ x, int64_t n,
     const uint32_t s0 = su32(sm);
     const uint32_t wbar = s0 + SM_BAR, mbar = s0 + SM_BAR + 8 * (1 + wg);
     uint32_t *tslot = reinterpret_cast<uint32_t *>(sm + SM_BAR + 64);
-    const float *b1 = reinterpret_cast<const float *>(sm + OFF_B1);
-    const float *b2 = reinterpret_cast<const float *>(sm + OFF_B2);
-    const float *b3 = reinterpret_cast<const float *>(sm + OFF_B3);
     const float *w4 = reinterpret_cast<const float *>(sm + OFF_W4);
 
     if (tid == 0) {
@@ -494,7 +492,7 @@ k_mlp(const uint8_t *__restrict__ image, const float *__restrict__ x, int64_t n,
                 }
                 late |= !mbar_wait(mbar, phase); phase ^= 1;
                 tc_after();
-                epi_hidden<N1, H1, ONES1, MODE == FWD_DX>(tw, b1, B0, r, tstash);
+                epi_hidden<N1, H1, ONES1, MODE == FWD_DX>(tw, B0, r, tstash);
                 if (MODE == FWD_DX) tmem_wait_st();
                 tc_before();
                 fence_async_smem();
@@ -507,7 +505,7 @@ k_mlp(const uint8_t *__restrict__ image, const float *__restrict__ x, int64_t n,
                 }
                 late |= !mbar_wait(mbar, phase); phase ^= 1;
                 tc_after();
-                epi_hidden<N2, H2, ONES1, false>(tw, b2, Hb, r, 0);
+                epi_hidden<N2, H2, ONES1, false>(tw, Hb, r, 0);
                 tc_before();
                 fence_async_smem();
                 bar_sync(bid, 128);
@@ -520,7 +518,7 @@ k_mlp(const uint8_t *__restrict__ image, const float *__restrict__ x, int64_t n,
                 late |= !mbar_wait(mbar, phase); phase ^= 1;
                 tc_after();
                 // layer 3 epilogue: h3, output, and (FWD_DX) G3 = w4 (1 - h3^2) -> B0
-                const float o = epi_out<MODE == FWD_DX ? 1 : 0>(tw, b3, w4, bias4, B0, r);
+                const float o = epi_out<MODE == FWD_DX ? 1 : 0>(tw, w4, bias4, B0, r);
                 if (valid) out[row] = o;
                 tc_before();
                 if (MODE == FWD_DX) {
@@ -582,7 +580,7 @@ k_mlp(const uint8_t *__restrict__ image, const float *__restrict__ x, int64_t n,
                 }
                 late |= !mbar_wait(mbar, phase); phase ^= 1;
                 tc_after();
-                epi_hidden<N1, H1, ONES1, false>(tw, b1, H1t, r, 0);
+                epi_hidden<N1, H1, ONES1, false>(tw, H1t, r, 0);
                 tc_before();
                 fence_async_smem();
                 bar_sync(bid, 128);
@@ -594,7 +592,7 @@ k_mlp(const uint8_t *__restrict__ image, const float *__restrict__ x, int64_t n,
                 }
                 late |= !mbar_wait(mbar, phase); phase ^= 1;
                 tc_after();
-                epi_hidden<N2, H2, ONES1, false>(tw, b2, H2t, r, 0);
+                epi_hidden<N2, H2, ONES1, false>(tw, H2t, r, 0);
                 tc_before();
                 fence_async_smem();
                 bar_sync(bid, 128);
@@ -606,7 +604,7 @@ k_mlp(const uint8_t *__restrict__ image, const float *__restrict__ x, int64_t n,
                 }
                 late |= !mbar_wait(mbar, phase); phase ^= 1;
                 tc_after();
-                const float o = epi_out<2>(tw, b3, w4, bias4, H3t, r);
+                const float o = epi_out<2>(tw, w4, bias4, H3t, r);
                 const float y = valid ? xr[DIN] : 0.f;
                 const float e = o - y;
                 float g, l;
@@ -749,6 +747,12 @@ __device__ __forceinline__ int img_index(int R, int row, int col) {  // bf16 ele
     return (col >> 3) * (R * 8) + row * 8 + (col & 7);
 }
 
+// bias b as the bf16 pair (hi, lo) of its two weight columns: hi + lo = b to ~16 bits
+__device__ __forceinline__ float bias_part(float b, bool lo) {
+    const float hi = __bfloat162float(__float2bfloat16_rn(b));
+    return lo ? b - hi : hi;
+}
+
 // full image from the master parameters (pads are zero)
 __global__ void k_mlp_pack(const float *__restrict__ p, uint8_t *__restrict__ image) {
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
@@ -764,10 +768,13 @@ __global__ void k_mlp_pack(const float *__restrict__ p, uint8_t *__restrict__ im
         if (off == OFF_W1) {
             if (row < H1 && col < DIN) v = p[P_W1 + row * DIN + col];
             else if (row < H1 && col >= DIN && col < 2 * DIN) v = p[P_W1 + row * DIN + col - DIN];
+            else if (row < H1 && (col == ONES0 || col == ONES0 + 1)) v = bias_part(p[P_B1 + row], col != ONES0);
         } else if (off == OFF_W2) {
             if (row < H2 && col < H1) v = p[P_W2 + row * H1 + col];
+            else if (row < H2 && (col == ONES1 || col == ONES1 + 1)) v = bias_part(p[P_B2 + row], col != ONES1);
         } else {
             if (row < H3 && col < H2) v = p[P_W3 + row * H2 + col];
+            else if (row < H3 && (col == ONES1 || col == ONES1 + 1)) v = bias_part(p[P_B3 + row], col != ONES1);
         }
         reinterpret_cast<__nv_bfloat16 *>(image + off)[le] = __float2bfloat16_rn(v);
     } else if (e < NB + NF) {
@@ -807,11 +814,24 @@ __global__ void k_mlp_adam(float *__restrict__ p, float *__restrict__ m, float *
         const int o = i / DIN, j = i % DIN;
         w1[img_index(N1, o, j)] = wb;
         w1[img_index(N1, o, j + DIN)] = wb;
-    } else if (i < P_W2) f[OFF_B1 / 4 + (i - P_B1)] = w;
-    else if (i < P_B2) { const int o = (i - P_W2) / H1, c = (i - P_W2) % H1; w2[img_index(N2, o, c)] = wb; }
-    else if (i < P_W3) f[OFF_B2 / 4 + (i - P_B2)] = w;
-    else if (i < P_B3) { const int o = (i - P_W3) / H2, c = (i - P_W3) % H2; w3[img_index(N3, o, c)] = wb; }
-    else if (i < P_W4) f[OFF_B3 / 4 + (i - P_B3)] = w;
+    } else if (i < P_W2) {
+        const int o = i - P_B1;
+        f[OFF_B1 / 4 + o] = w;
+        w1[img_index(N1, o, ONES0)] = __float2bfloat16_rn(bias_part(w, false));
+        w1[img_index(N1, o, ONES0 + 1)] = __float2bfloat16_rn(bias_part(w, true));
+    } else if (i < P_B2) { const int o = (i - P_W2) / H1, c = (i - P_W2) % H1; w2[img_index(N2, o, c)] = wb; }
+    else if (i < P_W3) {
+        const int o = i - P_B2;
+        f[OFF_B2 / 4 + o] = w;
+        w2[img_index(N2, o, ONES1)] = __float2bfloat16_rn(bias_part(w, false));
+        w2[img_index(N2, o, ONES1 + 1)] = __float2bfloat16_rn(bias_part(w, true));
+    } else if (i < P_B3) { const int o = (i - P_W3) / H2, c = (i - P_W3) % H2; w3[img_index(N3, o, c)] = wb; }
+    else if (i < P_W4) {
+        const int o = i - P_B3;
+        f[OFF_B3 / 4 + o] = w;
+        w3[img_index(N3, o, ONES1)] = __float2bfloat16_rn(bias_part(w, false));
+        w3[img_index(N3, o, ONES1 + 1)] = __float2bfloat16_rn(bias_part(w, true));
+    }
     else if (i < P_B4) f[OFF_W4 / 4 + (i - P_W4)] = w;
     else f[OFF_B4 / 4] = w;
 }

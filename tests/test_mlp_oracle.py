@@ -39,18 +39,23 @@ def test_pack_image_layout():
     t2 = img[M.OFF_W2:M.OFF_W3].view(np.uint16)
     t3 = img[M.OFF_W3:M.OFF_B1].view(np.uint16)
     as_f = lambda bits: (bits.astype(np.uint32) << 16).view(np.float32).astype(np.float64)  # noqa: E731
-    for (t, R, C, W, dup) in ((t1, 112, 16, W1, True), (t2, 112, 112, W2, False), (t3, 128, 112, W3, False)):
+    for (t, R, C, W, b, dup) in ((t1, 112, 16, W1, b1, True), (t2, 112, 112, W2, b2, False),
+                                 (t3, 128, 112, W3, b3, False)):
         full = np.zeros((R, C))
         for r in range(R):
             for c in range(C):
                 full[r, c] = as_f(t[M._tile_index(R, r, c):M._tile_index(R, r, c) + 1])[0]
         h, w = W.shape
         np.testing.assert_array_equal(full[:h, :w], M.bf16(W))
+        ones = 2 * w if dup else w  # the bias's two columns, against the input's two ones columns
         if dup:
             np.testing.assert_array_equal(full[:h, w:2 * w], M.bf16(W))
-            assert not full[:, 2 * w:].any()
-        else:
-            assert not full[:, w:].any()
+        hi, lo = M.bias_split(b)
+        np.testing.assert_array_equal(full[:h, ones], hi)
+        np.testing.assert_array_equal(full[:h, ones + 1], lo)
+        # hi + lo carries the float32 bias to about 16 significant bits
+        assert np.all(np.abs(hi + lo - b.astype(np.float32)) <= 2.0 ** -16 * np.abs(b) + 1e-30)
+        assert not full[:, ones + 2:].any()
         assert not full[h:, :].any()
     f = img.view(np.float32)
     np.testing.assert_array_equal(f[M.OFF_B1 // 4:M.OFF_B1 // 4 + 100], b1.astype(np.float32))
