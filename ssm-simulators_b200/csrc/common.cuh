@@ -149,8 +149,10 @@ __device__ __forceinline__ float2 box_muller(uint32_t a, uint32_t b) {
 // one of 262 144 rays, far below what a one-dimensional increment can show.
 // Compared with two pairs per call this takes a third less Philox work per
 // increment.  c2 = -2 ln(2) scale^2 scales the radius, so each output is
-// drift + scale * N(0,1) (scale 1, drift 0: standard normals).
-__device__ __forceinline__ void bm6_increment(uint4 b, float c2, float drift, float *g) {
+// drift + scale * N(0,1) (scale 1, drift 0: standard normals).  Pair i (outputs
+// 2i, 2i+1) takes its own c2[i] and drift[i] (bm6_increment: the same for all).
+__device__ __forceinline__ void bm6_increment_pairs(uint4 b, const float (&c2)[3], const float (&drift)[3],
+                                                    float *g) {
     const uint32_t rad[3] = {b.x, b.y, b.z};
     const uint32_t ph[3] = {b.w & 0x007fffffu, ((b.w >> 9) & 0x7fc000u) | ((b.x >> 18) & 0x3fe0u),
                             ((b.y >> 9) & 0x7fc000u) | ((b.z >> 18) & 0x3fe0u)};
@@ -158,14 +160,18 @@ __device__ __forceinline__ void bm6_increment(uint4 b, float c2, float drift, fl
     for (int i = 0; i < 3; ++i) {
         const float u1 = __uint_as_float(0x3f800000u | (rad[i] & 0x007fffffu)) - 0.99999994f;  // (0, 1)
         const float ang = fmaf(__uint_as_float(0x3f800000u | ph[i]), 6.2831853f, -6.2831853f);
-        const float e = c2 * lg2_ftz(u1);
+        const float e = c2[i] * lg2_ftz(u1);
         float r;
         asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(e));
         float sn, cs;
         sincos_ftz(ang, sn, cs);
-        g[2 * i] = fmaf(r, cs, drift);
-        g[2 * i + 1] = fmaf(r, sn, drift);
+        g[2 * i] = fmaf(r, cs, drift[i]);
+        g[2 * i + 1] = fmaf(r, sn, drift[i]);
     }
+}
+__device__ __forceinline__ void bm6_increment(uint4 b, float c2, float drift, float *g) {
+    const float c[3] = {c2, c2, c2}, d[3] = {drift, drift, drift};
+    bm6_increment_pairs(b, c, d, g);
 }
 
 __device__ __forceinline__ void raise_error(WorkspaceHeader *h, int code, int detail) {

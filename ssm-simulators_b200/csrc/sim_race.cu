@@ -146,6 +146,34 @@ struct RaceLane {
     float x[NP];
 };
 
+// The next window's increments, drawn ahead six per Philox call (calls ctr ..
+// ctr + CALLS - 1) and stored accumulator-major: pre[j * WIN + s] is
+// accumulator j's increment v_j dt + sq_j N(0,1) at step s of the window.
+// WIN is even, so every Box-Muller pair belongs to one accumulator and that
+// accumulator's scale and drift fold into the pair (radius constant
+// c2 = -2 ln(2) sq_j^2, drift v_j dt): a step adds one increment instead of
+// scaling a standard normal and adding the drift.
+template <int NP>
+__device__ __forceinline__ void draw_window(const RaceParams &p, const RaceLane<NP> &L, const float *vr,
+                                            const float *sr, uint32_t ctr, float *pre) {
+    constexpr int WIN = RaceWin<NP>::value;
+    constexpr int CALLS = WIN * NP / 6;
+    static_assert(WIN % 2 == 0 && (WIN * NP) % 6 == 0, "pairs within one accumulator, whole calls");
+    float c2a[NP], dta[NP];
+#pragma unroll
+    for (int j = 0; j < NP; ++j) {
+        c2a[j] = -1.3862944f * sr[j] * sr[j];
+        dta[j] = vr[j] * p.dt;
+    }
+#pragma unroll
+    for (int c = 0; c < CALLS; ++c) {
+        const uint4 r = philox10(make_uint4(ctr + (uint32_t)c, L.n, L.k + p.k_base, 0u), p.key);
+        const float c2[3] = {c2a[(6 * c) / WIN], c2a[(6 * c + 2) / WIN], c2a[(6 * c + 4) / WIN]};
+        const float d[3] = {dta[(6 * c) / WIN], dta[(6 * c + 2) / WIN], dta[(6 * c + 4) / WIN]};
+        bm6_increment_pairs(r, c2, d, pre + 6 * c);
+    }
+}
+
 // True when none of the lane's next `win` steps can reach the step cap or the
 // time limit: the float32 accumulator after (win - 1) more additions of dt is
 // at most t + (win - 1) dt plus their roundings (under dt/4 below 65536 dt),
@@ -161,11 +189,13 @@ __device__ __forceinline__ bool window_clear(const RaceParams &p, const RaceLane
 }
 
 // One Euler step of every accumulator.  Returns false when the loop condition
-// failed before the step (the walk is over).  With PRE the step's normals come
-// from `pre` (drawn ahead from the same counters); ctr still counts the steps.
+// failed before the step (the walk is over).  With PRE the step's increments
+// v_j dt + sq_j N(0,1) come from pre[j * PSTRIDE] (draw_window); ctr still
+// counts the steps.
 // CHECKED false skips the step-cap check and the time test, for a window the
 // caller has shown both to pass for (window_clear).
-template <int NP, int FAM, int BOUND, bool NOISE, bool RECORD, bool PRE = false, bool CHECKED = true>
+template <int NP, int FAM, int BOUND, bool NOISE, bool RECORD, bool PRE = false, bool CHECKED = true,
+          int PSTRIDE = 1>
 __device__ __forceinline__ bool race_step(const RaceParams &p, RaceLane<NP> &L, const RaceHead &h,
                                           const float *v, const float *sq, int np, uint32_t &ctr,
                                           const float *pre = nullptr) {
@@ -195,7 +225,7 @@ __device__ __forceinline__ bool race_step(const RaceParams &p, RaceLane<NP> &L, 
         for (int j = 0; j < NP; ++j) gsn[j] = (j < np) ? __ldg(row + j) : 0.f;
     } else if (PRE) {
 #pragma unroll
-        for (int j = 0; j < NP; ++j) gsn[j] = pre[j];
+        for (int j = 0; j < NP; ++j) gsn[j] = pre[j * PSTRIDE];
         ctr += 1;
     } else {
 #pragma unroll
@@ -217,11 +247,15 @@ __device__ __forceinline__ bool race_step(const RaceParams &p, RaceLane<NP> &L, 
 #pragma unroll
         for (int j = 0; j < NP; ++j)
             if (j < np) sum = NOISE ? __fadd_rn(sum, L.x[j]) : sum + L.x[j];
+        // with PRE the increments carry v dt + sq N: x (1 - g dt + b dt) - b dt sum + increment
+        const float c1 = fmaf(h.b - h.g, p.dt, 1.f), c2 = -h.b * p.dt;
 #pragma unroll
         for (int j = 0; j < NP; ++j) {
             if (j < np) {
                 float xj = L.x[j];
-                if (NOISE) {
+                if (PRE && !NOISE) {
+                    xj = fmaf(xj, c1, fmaf(sum, c2, gsn[j]));
+                } else if (NOISE) {
                     // race_models.pyx:849-857 with the reference build's association
                     const float red = __double2float_rn(__dadd_rn(-(double)xj, (double)sum));
                     const float A = __fsub_rn(__fsub_rn(v[j], __fmul_rn(h.g, xj)), __fmul_rn(h.b, red));
@@ -244,6 +278,7 @@ __device__ __forceinline__ bool race_step(const RaceParams &p, RaceLane<NP> &L, 
             if (j < np) {
                 float xj;
                 if (NOISE) xj = __fadd_rn(__fadd_rn(L.x[j], __fmul_rn(v[j], p.dt)), __fmul_rn(sq[j], gsn[j]));
+                else if (PRE) xj = L.x[j] + gsn[j];
                 else xj = fmaf(sq[j], gsn[j], L.x[j] + v[j] * p.dt);
                 L.x[j] = xj;
                 if (win < 0 && xj >= bnd) win = j;
@@ -260,6 +295,7 @@ __device__ __forceinline__ bool race_step(const RaceParams &p, RaceLane<NP> &L, 
             if (j < np) {
                 float xj;
                 if (NOISE) xj = __fadd_rn(__fadd_rn(L.x[j], __fmul_rn(v[j], p.dt)), __fmul_rn(sq[j], gsn[j]));
+                else if (PRE) xj = L.x[j] + gsn[j];
                 else xj = fmaf(sq[j], gsn[j], L.x[j] + v[j] * p.dt);
                 L.x[j] = fmaxf(0.f, xj);
             }
@@ -458,28 +494,25 @@ __global__ void __launch_bounds__(256) k_race(const __grid_constant__ RaceParams
             }
             bool live = true;
             if (!NOISE && NP <= 4) {
-                // the next WIN steps' normals first, six per Philox call (calls
-                // ctr .. ctr + CALLS - 1), then the steps; ctr advances per window
+                // the next WIN steps' increments first (draw_window), then the
+                // steps; ctr advances per window
                 constexpr int WIN = RaceWin<NP>::value;
-                constexpr int CALLS = WIN * NP / 6;
                 float nrm[WIN * NP];
-#pragma unroll
-                for (int c = 0; c < CALLS; ++c) {
-                    const uint4 r = philox10(make_uint4(ctr + (uint32_t)c, L.n, L.k + p.k_base, 0u), p.key);
-                    bm6_increment(r, -1.3862944f, 0.f, nrm + 6 * c);
-                }
-                ctr += CALLS;
+                draw_window<NP>(p, L, vr, sr, ctr, nrm);
+                ctr += WIN * NP / 6;
                 uint32_t unused = 0;
                 if (clear) {
 #pragma unroll
                     for (int s = 0; s < WIN; ++s)
                         if (live)
-                            live = race_step<NP, FAM, BOUND, NOISE, false, true, false>(p, L, h, vr, sr, np, unused,
-                                                                                        nrm + s * NP);
+                            live = race_step<NP, FAM, BOUND, NOISE, false, true, false, WIN>(p, L, h, vr, sr, np,
+                                                                                             unused, nrm + s);
                 } else {
 #pragma unroll
                     for (int s = 0; s < WIN; ++s)
-                        if (live) live = race_step<NP, FAM, BOUND, NOISE, false, true>(p, L, h, vr, sr, np, unused, nrm + s * NP);
+                        if (live)
+                            live = race_step<NP, FAM, BOUND, NOISE, false, true, true, WIN>(p, L, h, vr, sr, np,
+                                                                                            unused, nrm + s);
                 }
             } else {
 #pragma unroll 1
@@ -515,18 +548,14 @@ __global__ void k_race_record(const __grid_constant__ RaceParams p) {
     if (!NOISE && NP <= 4) {
         // the main kernel's windows: the same normals in the same order
         constexpr int WIN = RaceWin<NP>::value;
-        constexpr int CALLS = WIN * NP / 6;
         bool live = true;
         while (live) {
             float nrm[WIN * NP];
-            for (int c = 0; c < CALLS; ++c) {
-                const uint4 r = philox10(make_uint4(ctr + (uint32_t)c, L.n, L.k + p.k_base, 0u), p.key);
-                bm6_increment(r, -1.3862944f, 0.f, nrm + 6 * c);
-            }
-            ctr += CALLS;
+            draw_window<NP>(p, L, vr, sr, ctr, nrm);
+            ctr += WIN * NP / 6;
             uint32_t unused = 0;
             for (int s = 0; s < WIN && live; ++s)
-                live = race_step<NP, FAM, BOUND, NOISE, true, true>(p, L, h, vr, sr, np, unused, nrm + s * NP);
+                live = race_step<NP, FAM, BOUND, NOISE, true, true, true, WIN>(p, L, h, vr, sr, np, unused, nrm + s);
         }
     } else {
         while (race_step<NP, FAM, BOUND, NOISE, true>(p, L, h, vr, sr, np, ctr)) {
