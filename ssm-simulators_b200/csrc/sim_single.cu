@@ -12,7 +12,7 @@
 //    hands them the next trajectories of its chunk (popc rank) in one
 //    divergent pass, so that pass is paid once per several trajectories and
 //    an ended lane idles for a few blocks at most.
-//  * Steps run in blocks of 36 (16 for ddm_flex, 8 for Levy): six independent
+//  * Steps run in blocks of 36 (24 for ddm_flex, 8 for Levy): six independent
 //    Philox4x32-10 calls yield 24 words = 18 Box-Muller pairs = the block's
 //    increments, already scaled to drift + s sqrt(dt) N(0,1); the steps
 //    themselves are predicated (no per-step branch), and a warp whose walks
@@ -82,7 +82,7 @@ struct SingleParams {
     int64_t tstride, tlen;
     const float *dtable;     // DFLEX: drift v(t_ix) per trial, row stride dstride, dlen entries
     int64_t dstride, dlen;
-    int dvec;                // rows 16-byte aligned: a block's 8 drifts are two float4 loads
+    int dvec;                // rows 16-byte aligned: a block's 24 drifts are six float4 loads
     const float *noise;      // injected increments: row w holds nlen floats
     int64_t nlen;
     const float *nunif;      // injected jitter uniforms, one per trajectory
@@ -272,15 +272,17 @@ __device__ __forceinline__ float cms_stable(uint32_t bu, uint32_t bw, const Tria
 // registers, 3 CTAs per SM; 4 CTAs per SM at 64 registers 27.3 for 24 and 36
 // steps); four per call with 32-step blocks 31.2.  With the re-tuned launch
 // (128 threads, claims of 256): 30 steps 26.95, 36 steps 26.54, 42 steps
-// 26.39, but on 1024 sets 42 steps is the slower (8.02 against 7.92 ms).  ddm_flex keeps four per
-// call and 16-step blocks (its per-block drift values take registers too;
-// 20.4 -> 18.4 ms against 8-step blocks on the conflict_ds sets), and the Levy
-// model 8-step blocks (its stable draws already give each block enough
-// independent work; 16-step blocks measured 8 % slower there).  Call h of
-// block b uses counter (BLK/6) b + h (ddm_flex: (BLK/4) b + h), so a stream
-// does not depend on the block length.
+// 26.39, but on 1024 sets 42 steps is the slower (8.02 against 7.92 ms).
+// ddm_flex holds a block's table drifts in registers as well, so its blocks
+// are shorter: 24 steps (four Philox calls, six float4 drift loads) took
+// 14.46 ms on the 1 024 conflict_ds sets against 15.73 for 12 steps and
+// 16.51 for 16-step blocks of four increments per call (36 steps spill).
+// The Levy model keeps 8-step blocks (its stable draws already give each
+// block enough independent work; 16-step blocks measured 8 % slower there).
+// Call h of block b uses counter (BLK/6) b + h, so a stream does not depend
+// on the block length.
 template <int MODEL> struct Blk {
-    static constexpr int value = (MODEL == M_LEVY) ? 8 : (MODEL == M_DFLEX ? 16 : 36);
+    static constexpr int value = (MODEL == M_LEVY) ? 8 : (MODEL == M_DFLEX ? 24 : 36);
 };
 // Lanes per walk W (see wide_block): 1 is the throughput mode above; W = 2,
 // 4, 8 give each trajectory an aligned group of W lanes and blocks of 18 W
@@ -311,21 +313,6 @@ struct Lane {
 // models whose drift is drawn once per trajectory
 template <int MODEL> struct DrawnDrift { static constexpr bool value = (MODEL == M_SDV || MODEL == M_FULL); };
 
-// Box-Muller pair already scaled into Euler increments: drift + scale * N(0,1).
-// c2 = -2 ln(2) scale^2, so r = sqrt(c2 * log2(u1)) = scale * sqrt(-2 ln u1).
-__device__ __forceinline__ void bm_increment(uint32_t a, uint32_t b, float c2, float drift,
-                                             float &g0, float &g1) {
-    const float u1 = __uint_as_float(0x3f800000u | (a & 0x007fffffu)) - 0.99999994f;  // (0, 1)
-    const float ang = fmaf(__uint_as_float(0x3f800000u | (b & 0x007fffffu)), 6.2831853f, -6.2831853f);
-    const float e = c2 * lg2_ftz(u1);
-    float r;
-    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(e));
-    float sn, cs;
-    sincos_ftz(ang, sn, cs);
-    g0 = fmaf(r, cs, drift);
-    g1 = fmaf(r, sn, drift);
-}
-
 // The block's increments.  Noise injection returns the raw caller draws (the
 // step applies drift and scale with explicit rounding); the device RNG returns
 // finished increments drift + scale * X.
@@ -349,24 +336,15 @@ __device__ __forceinline__ void draw_block(const SingleParams &p, const Lane &L,
             g[2 * h + 2] = fmaf(r.scale, cms_stable(c.x, c.y, r), r.drift);
             g[2 * h + 3] = fmaf(r.scale, cms_stable(c.z, c.w, r), r.drift);
         }
-    } else if (MODEL != M_DFLEX) {
-        const float drift = DrawnDrift<MODEL>::value ? L.dinc : r.drift;
-        static_assert(MODEL == M_LEVY || MODEL == M_DFLEX || BLK % 6 == 0, "six increments per Philox call");
+    } else {
+        // ddm_flex: drift 0 here, v(t_ix) dt from the table in the step
+        const float drift = (MODEL == M_DFLEX) ? 0.f : (DrawnDrift<MODEL>::value ? L.dinc : r.drift);
+        static_assert(MODEL == M_LEVY || BLK % 6 == 0, "six increments per Philox call");
 #pragma unroll
         for (int h = 0; h < BLK / 6; ++h) {
             const uint4 b = philox10(make_uint4((uint32_t)(BLK / 6) * L.blk + (uint32_t)h, L.n, L.k + p.k_base, 0u),
                                      p.key);
             bm6_increment(b, r.c2, drift, g + 6 * h);
-        }
-    } else {
-        // ddm_flex: two pairs per call; the drift comes from the table in the step
-        const float drift = 0.f;
-#pragma unroll
-        for (int h = 0; h < BLK / 4; ++h) {
-            const uint4 b = philox10(make_uint4((uint32_t)(BLK / 4) * L.blk + (uint32_t)h, L.n, L.k + p.k_base, 0u),
-                                     p.key);
-            bm_increment(b.x, b.y, r.c2, drift, g[4 * h], g[4 * h + 1]);
-            bm_increment(b.z, b.w, r.c2, drift, g[4 * h + 2], g[4 * h + 3]);
         }
     }
 }
