@@ -60,11 +60,10 @@ INSTR_PER_STEP = 18.0
 # single-accumulator Gaussian models draw six increments per Philox call
 # (7 + 7 = 14 per increment, folded scale and drift) and test the time once per
 # block (constant-bound step 3: compare with predicate, position and time
-# updates); the race family draws six per call too (14 per normal) and tests
-# the time every step; ddm_flex draws four per call (Philox 10.5 + Box-Muller
-# 6 = 16.5) and tests the time every step (constant-bound step 4.5, 5.5
-# against a moving bound).
-GAUSS_INCREMENT = 16.5
+# updates); the race family draws six per call too (14 per normal, each
+# accumulator's scale and drift folded into its pairs) and tests the time
+# every step; ddm_flex draws six per call as well and tests the time every step
+# (constant-bound step 4.5, 5.5 against a moving bound).
 INSTR_MIN = {
     # constant bound: 16.5 + 4.5
     "plain_ddm": (17.0, "Gaussian increment 14 (six per Philox call) + constant-bound step 3"),
@@ -72,25 +71,26 @@ INSTR_MIN = {
     # the leaky update y (1 - g dt) + increment is one FFMA, like the plain add
     "ornstein": (17.0, "Gaussian increment 14 + constant-bound step 3 (leak folded into one FFMA)"),
     # drift table: one FFMA v(t) dt + increment, a 16-byte load per four steps
-    "conflict_ds": (22.25, "Gaussian increment 16.5 + constant-bound step 4.5 + drift-table FFMA 1 "
-                           "+ vector load 0.25"),
+    "conflict_ds": (19.75, "Gaussian increment 14 (six per Philox call) + constant-bound step 4.5 "
+                           "+ drift-table FFMA 1 + vector load 0.25"),
     # two Philox words per stable variate (21), Chambers-Mallows-Stuck with
     # reduced-angle polynomials: uniform and fold 5, W = -ln u 5, three
     # polynomial sin/cos 23, three log2 + exponent + ex2 7, product, sign,
     # clamp and NaN guard 6, scale FFMA 1 = 47; constant-bound step 3 (time
     # tested once per block)
     "levy": (71.0, "Philox 21 (two words per variate) + CMS 47 + constant-bound step 3"),
-    # per accumulator: normal 14, scale and add + clamp at 0 + threshold
-    # compare 3; per step over 4 accumulators: moving bound, time update and
-    # test, predicate 3.5 / 4
+    # per accumulator: increment 14 (scale and drift folded in), add + clamp at
+    # 0 + threshold compare 3; per step over 4 accumulators: moving bound, time
+    # update and test, predicate 3.5 / 4
     "race_no_bias_angle_4": (17.875, "normal 14 (six per Philox call) + add, clamp, compare 3 "
                                      "+ shared step 3.5/4"),
-    # per accumulator: normal 14, (x + (v - g x - b (S - x)) dt) + noise 5,
-    # clamp 1, compare 1; the sum S 3/4; per step the float64 time update,
-    # test and predicate 3 / 4
-    "lca_no_bias_4": (22.5, "normal 14 + LCA update 5 + clamp, compare 2 + sum 0.75 + shared step 3/4"),
-    # per accumulator: normal 14, add + compare 2; shared step 3.5 / 3
-    "racing_diffusion_3": (17.17, "normal 14 + add, compare 2 + shared step 3.5/3"),
+    # per accumulator: increment 14 (v dt + s sqrt(dt) N), the update
+    # x (1 - g dt + b dt) + S (-b dt) + increment as two FFMA, clamp 1,
+    # compare 1; the sum S 3/4; per step the float64 time update, test and
+    # predicate 3 / 4
+    "lca_no_bias_4": (19.5, "increment 14 + LCA update 2 + clamp, compare 2 + sum 0.75 + shared step 3/4"),
+    # per accumulator: increment 14, add + compare 2; shared step 3.5 / 3
+    "racing_diffusion_3": (17.17, "increment 14 + add, compare 2 + shared step 3.5/3"),
 }
 E2E_WINDOWS = 5
 N_SM = 148
