@@ -41,14 +41,16 @@ __device__ __forceinline__ int64_t warp_chunk(int chunk, int64_t total, int slot
 // Ended walks a persistent simulator warp collects before it writes their
 // results and restarts those lanes (ssm_launch.refill_min = 0).  Batching
 // pays where a step is cheap next to the restart (single accumulator, 4:
-// 10-12 % faster than 1 on the angle and full_ddm batches); a race step over
-// several accumulators costs more than the restart it would save, so the race
-// kernel restarts each lane at once.
+// 10-12 % faster than 1 on the angle and full_ddm batches).  The race kernel,
+// whose steps cost more, restarts two at a time by default: with windows of
+// steps drawn ahead, 1 024-set launches measured 2.4 % (LCA) and 7.9 %
+// (racing diffusion) faster with 2 than with 1, and the race model 8.3 %
+// with 6 (its tuned value, like the others', is in the launch-option store).
 #ifndef SSM_REFILL_MIN
 #define SSM_REFILL_MIN 4
 #endif
 #ifndef SSM_REFILL_MIN_RACE
-#define SSM_REFILL_MIN_RACE 1
+#define SSM_REFILL_MIN_RACE 2
 #endif
 
 // Workspace header shared by every persistent kernel: a work counter and an

@@ -115,15 +115,47 @@ def tune_batched(model: str = "angle", n_theta: int = 4096, seed: int = 0, persi
     return res
 
 
+def tune_sets(model: str, n_theta: int = 1024, n_samples: int = 10_000, seed: int = 0, persist: bool = False,
+              candidates=None, repeats: int = 2) -> dict:
+    """Autotune the simulator of any configured ``model`` (the race and LCA
+    families included) on ``n_theta`` parameter sets drawn uniformly from the
+    model's bounds, ``n_samples`` each, run as one ``SetBatch`` launch; the
+    winner is stored under the model's simulator family."""
+    import numpy as np
+
+    from .batch_models import SetBatch
+    from .config import model_config
+    from .simulator import Simulator
+
+    cfg = model_config[model]
+    lo, hi = (np.asarray(b, np.float64) for b in cfg["param_bounds"])
+    rng = np.random.default_rng(seed)
+    theta = {k: rng.uniform(lo[i], hi[i], n_theta).astype(np.float32) for i, k in enumerate(cfg["params"])}
+    prep = Simulator(model).prepare(theta, n_samples=n_samples, random_state=seed)
+    family = prep["config"]["simulator"].__name__
+    sb = SetBatch(family, prep["theta"], prep["boundary"], n_samples, max_t=20.0, delta_t=0.001,
+                  drift=prep["drift"])
+    res = autotune(family, lambda opt: sb.run(seed, launch=opt), candidates=candidates, repeats=repeats,
+                   persist=persist)
+    res["model"], res["family"], res["trajectories"] = model, family, sb.total
+    return res
+
+
 def main(argv=None) -> dict:
     import argparse
 
     ap = argparse.ArgumentParser(description="autotune the persistent simulators' launch configuration")
     ap.add_argument("--model", default="angle")
-    ap.add_argument("--n-theta", type=int, default=4096)
+    ap.add_argument("--n-theta", type=int, default=None,
+                    help="parameter sets (default 4096; 1024 with --sets)")
+    ap.add_argument("--sets", action="store_true",
+                    help="tune on a SetBatch of n-theta sets x 10000 samples (any simulator family)")
     ap.add_argument("--persist", action="store_true")
     a = ap.parse_args(argv)
-    res = tune_batched(a.model, n_theta=a.n_theta, persist=a.persist)
+    if a.sets:
+        res = tune_sets(a.model, n_theta=a.n_theta or 1024, persist=a.persist)
+    else:
+        res = tune_batched(a.model, n_theta=a.n_theta or 4096, persist=a.persist)
     print(json.dumps(res))
     return res
 
