@@ -361,7 +361,7 @@ __device__ __forceinline__ bool step_block(const SingleParams &p, Lane &L, const
         raise_error(p.hdr, SSM_ERR_DEVICE, (int)L.w);
         return false;
     }
-    constexpr bool INT_IX = NOISE || RECORD || BOUND == SSM_BOUND_TABLE || MODEL == M_DFLEX;
+    constexpr bool INT_IX = NOISE || RECORD || BOUND == SSM_BOUND_TABLE;
     // Without an integer index (device RNG, in-register bounds) step q of the
     // block sits at step ixf0 + q: the step count advances once per block,
     // the linear bound is a + ixf0 slope dt plus q slope dt, and finalize()
@@ -375,8 +375,9 @@ __device__ __forceinline__ bool step_block(const SingleParams &p, Lane &L, const
     // a multiple of BLK steps); past the table's end the last entry repeats
     float dvq[BLK];
     if (MODEL == M_DFLEX && !NOISE) {
-        if (p.dvec && (L.ix & 3) == 0 && L.ix + BLK <= p.dlen) {
-            const float4 *d4 = reinterpret_cast<const float4 *>(drow + L.ix);
+        const int ix0 = INT_IX ? L.ix : (int)ixf0;  // the block's first step
+        if (p.dvec && (ix0 & 3) == 0 && ix0 + BLK <= p.dlen) {
+            const float4 *d4 = reinterpret_cast<const float4 *>(drow + ix0);
 #pragma unroll
             for (int h = 0; h < BLK / 4; ++h) {
                 const float4 a = __ldg(d4 + h);
@@ -384,7 +385,7 @@ __device__ __forceinline__ bool step_block(const SingleParams &p, Lane &L, const
             }
         } else {
 #pragma unroll
-            for (int q = 0; q < BLK; ++q) dvq[q] = __ldg(drow + ((L.ix + q < p.dlen) ? L.ix + q : p.dlen - 1));
+            for (int q = 0; q < BLK; ++q) dvq[q] = __ldg(drow + ((ix0 + q < p.dlen) ? ix0 + q : p.dlen - 1));
         }
     }
     bool live = true;
@@ -449,7 +450,7 @@ __device__ __forceinline__ bool step_block(const SingleParams &p, Lane &L, const
 // leaves more than that margin.
 template <int MODEL, int BOUND, bool NOISE, int BLK = Blk<MODEL>::value>
 __device__ __forceinline__ bool block_in_time(const SingleParams &p, const Lane &L, const TrialRow &r) {
-    constexpr bool INT_IX = NOISE || BOUND == SSM_BOUND_TABLE || MODEL == M_DFLEX;
+    constexpr bool INT_IX = NOISE || BOUND == SSM_BOUND_TABLE;
     if (INT_IX) return false;
     // longer blocks (lanes-per-walk mode, 36-144 steps) keep a margin of
     // 2 dt per 64 steps: past 65536 dt an addition rounds by up to dt/64
@@ -462,7 +463,7 @@ __device__ __forceinline__ bool block_in_time(const SingleParams &p, const Lane 
 // time accumulator from L.tpb to L.tp (the same float additions replayed).
 template <int MODEL, int BOUND, bool NOISE, int BLK = Blk<MODEL>::value>
 __device__ __forceinline__ int steps_taken(const SingleParams &p, const Lane &L) {
-    constexpr bool INT_IX = NOISE || BOUND == SSM_BOUND_TABLE || MODEL == M_DFLEX;
+    constexpr bool INT_IX = NOISE || BOUND == SSM_BOUND_TABLE;
     if (INT_IX) return (int)L.ixf;
     float tt = L.tpb;
     int c = 0;
