@@ -139,8 +139,7 @@ template <int NP>
 struct RaceLane {
     int64_t w;
     uint32_t k, n;
-    int ix;
-    float ixf, tp;  // race: float32 time accumulator
+    float ixf, tp;  // steps taken (as float); race: float32 time accumulator
     double tpd;     // lca: double time accumulator (Cython infers double, race_models.pyx:838)
     int win;        // rdm: index of the winning accumulator (-1 while racing)
     float x[NP];
@@ -203,7 +202,7 @@ __device__ __forceinline__ bool race_step(const RaceParams &p, RaceLane<NP> &L, 
         raise_error(p.hdr, SSM_ERR_DEVICE, (int)L.w);
         return false;
     }
-    const float bnd = race_bound<BOUND, NOISE>(h, L.ixf, L.ix, p, L.k);
+    const float bnd = race_bound<BOUND, NOISE>(h, L.ixf, (int)L.ixf, p, L.k);
     bool finished = false;
     if (FAM != FAM_RDM) {  // race / LCA test the bound before the step; RDM after each update
 #pragma unroll
@@ -215,7 +214,7 @@ __device__ __forceinline__ bool race_step(const RaceParams &p, RaceLane<NP> &L, 
     if (finished || !in_time) return false;
     float gsn[NP];
     if (NOISE) {
-        const int64_t base = (int64_t)L.ix * np;
+        const int64_t base = (int64_t)L.ixf * np;
         if (base + np > p.nlen) {
             raise_error(p.hdr, SSM_ERR_NOISE_RANGE, (int)L.w);
             return false;
@@ -272,7 +271,7 @@ __device__ __forceinline__ bool race_step(const RaceParams &p, RaceLane<NP> &L, 
     } else if (FAM == FAM_RDM) {
         // no lower barrier; the first accumulator (in index order) at or above b
         // wins and its step does not advance the time (race_models.pyx:1227-1244)
-        int win = -1;
+        bool hit = false;
 #pragma unroll
         for (int j = 0; j < NP; ++j) {
             if (j < np) {
@@ -281,10 +280,14 @@ __device__ __forceinline__ bool race_step(const RaceParams &p, RaceLane<NP> &L, 
                 else if (PRE) xj = L.x[j] + gsn[j];
                 else xj = fmaf(sq[j], gsn[j], L.x[j] + v[j] * p.dt);
                 L.x[j] = xj;
-                if (win < 0 && xj >= bnd) win = j;
+                hit |= (xj >= bnd);
             }
         }
-        if (win >= 0) {
+        if (hit) {  // once per walk: the winner is the first accumulator at or above b
+            int win = 0;
+#pragma unroll
+            for (int j = NP - 1; j >= 0; --j)
+                if (j < np && L.x[j] >= bnd) win = j;
             L.win = win;
             return false;
         }
@@ -302,10 +305,11 @@ __device__ __forceinline__ bool race_step(const RaceParams &p, RaceLane<NP> &L, 
         }
         L.tp = NOISE ? __fadd_rn(L.tp, p.dt) : L.tp + p.dt;
     }
-    L.ixf += 1.0f;
-    L.ix += 1;
-    if (RECORD && (int64_t)(L.ix + 1) * np <= p.traj_len) {
-        for (int j = 0; j < np && j < NP; ++j) p.traj[(int64_t)L.ix * np + j] = L.x[j];
+    L.ixf += 1.0f;  // steps taken, exact in float32 below 2^24
+    if (RECORD) {
+        const int64_t ix = (int64_t)L.ixf;
+        if ((ix + 1) * np <= p.traj_len)
+            for (int j = 0; j < np && j < NP; ++j) p.traj[ix * np + j] = L.x[j];
     }
     return true;
 }
@@ -332,7 +336,7 @@ __device__ __forceinline__ void race_finalize(const RaceParams &p, const RaceLan
         const bool omit = (rt == -999.f) || (L.win < 0);
         p.rts[L.w] = omit ? -999.f : rt;
         p.choices[L.w] = omit ? -1 : L.win;
-        if (p.steps) p.steps[L.w] = L.ix;
+        if (p.steps) p.steps[L.w] = (int)L.ixf;
         return;
     }
     int best = 0;
@@ -345,7 +349,7 @@ __device__ __forceinline__ void race_finalize(const RaceParams &p, const RaceLan
         }
     p.rts[L.w] = rt;
     p.choices[L.w] = best;
-    if (p.steps) p.steps[L.w] = L.ix;
+    if (p.steps) p.steps[L.w] = (int)L.ixf;
 }
 
 __device__ __forceinline__ int64_t race_find(const int64_t *off, int64_t K, int64_t w, int64_t hint) {
@@ -419,7 +423,6 @@ __device__ __forceinline__ bool race_init(const RaceParams &p, RaceLane<NP> &L, 
 #pragma unroll
         for (int j = 0; j < NP; ++j) L.x[j] = (j < np) ? __fmul_rn(__ldg(z + j), h.y0scale) : 0.f;
     }
-    L.ix = 0;
     L.ixf = 0.f;
     L.tp = 0.f;
     L.tpd = 0.0;
@@ -436,7 +439,7 @@ __global__ void __launch_bounds__(256) k_race(const __grid_constant__ RaceParams
     const int np = (NP == RACE_MAX_NP) ? p.np : NP;
     RaceLane<NP> L;
     RaceHead h;
-    L.w = 0; L.k = L.n = 0; L.ix = 0; L.ixf = L.tp = 0.f; L.tpd = 0.0; L.win = -1;
+    L.w = 0; L.k = L.n = 0; L.ixf = L.tp = 0.f; L.tpd = 0.0; L.win = -1;
 #pragma unroll
     for (int j = 0; j < NP; ++j) L.x[j] = 0.f;
     uint32_t ctr = 0;
