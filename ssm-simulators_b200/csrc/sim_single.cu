@@ -244,12 +244,11 @@ __device__ __forceinline__ float cms_stable(uint32_t bu, uint32_t bw, const Tria
         X = cos_q(V) / sin_q(V);  // |tan U|
     } else {
         const float cu = sin_q(V);                                             // cos U > 0
-        // cos((1 - alpha) U) = cos(c |U|), c = |1 - alpha| <= 1; past pi/4 as
-        // sin(pi/2 - c |U|) = sin(pi/2 (1 - c) + c V), which does not cancel
+        // cos((1 - alpha) U) = cos(c |U|), c = |1 - alpha| <= 1, evaluated as
+        // sin(pi/2 - c |U|) = sin(pi/2 (1 - c) + c V): two non-negative terms,
+        // so the argument does not cancel, and one polynomial serves every c |U|
         const float c = fabsf(1.0f - r.alpha);
-        const float B = c * aU;
-        const float cua = fmaxf((B > 0.78539816f) ? sin_q(fmaf(c, V, 1.57079633f * (1.0f - c))) : cos_q(B),
-                                1e-10f);
+        const float cua = fmaxf(sin_q(fmaf(c, V, 1.57079633f * (1.0f - c))), 1e-10f);
         // alpha |U| in [0, pi); past pi/2 use pi - alpha |U| = pi (1 - alpha/2) + alpha V,
         // which does not cancel as alpha -> 2
         float A = r.alpha * aU;
