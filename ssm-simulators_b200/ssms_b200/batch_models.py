@@ -60,9 +60,12 @@ def expected_set_time(sim_name: str, kwargs: dict, spec: dict | None, K: int, ma
     v = np.asarray(kwargs["v"], np.float64).reshape(K, -1)
     if sim_name in RACE:  # start z_j b(0), threshold b(t)
         a0 = np.asarray(spec["a"], np.float64).reshape(K, 1)
-        dist = a0 * (1.0 - np.asarray(kwargs["z"], np.float64).reshape(K, -1))
-        return expected_race_time(v, dist, np.asarray(kwargs["s"], np.float64).reshape(K, -1),
-                                  bound_kind=int(spec["kind"]), a=spec["a"], p1=spec["p1"], t_cap=cap)
+        zz = np.asarray(kwargs["z"], np.float64).reshape(K, -1)
+        lca = sim_name == "lca"
+        return expected_race_time(v, a0 * (1.0 - zz), np.asarray(kwargs["s"], np.float64).reshape(K, -1),
+                                  bound_kind=int(spec["kind"]), a=spec["a"], p1=spec["p1"], t_cap=cap,
+                                  start=a0 * zz if lca else None, leak=_col(kwargs["g"], K) if lca else None,
+                                  inhibition=_col(kwargs["b"], K) if lca else None)
     if sim_name == "racing_diffusion_model":  # start U(0, A), threshold b
         dist = np.asarray(_col(kwargs["b"], K), np.float64) - 0.5 * np.asarray(_col(kwargs["A"], K), np.float64)
         return expected_race_time(v, dist.reshape(K, 1), _col(kwargs["s"], K).reshape(K, 1), t_cap=cap)

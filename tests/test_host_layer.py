@@ -172,6 +172,29 @@ def test_expected_race_time_limits():
     np.testing.assert_allclose(e, [0.5])
 
 
+def test_expected_race_time_with_leak_and_inhibition():
+    from ssms_b200.batch import expected_race_time
+
+    v, dist, s = [[1.0, 0.5, 0.2, 0.1]], [[1.5, 1.5, 1.5, 1.5]], 1.0
+    # no leak, no inhibition: the plain drift-plus-diffusion time
+    plain = expected_race_time(v, dist, s, t_cap=1e9)
+    e = expected_race_time(v, dist, s, t_cap=1e9, start=[[0.5] * 4], leak=[0.0], inhibition=[0.0])
+    np.testing.assert_allclose(e, plain, rtol=1e-12)
+    # leak g: the drift route from 0.5 to 2.0 takes ln((v - 0.5 g) / (v - 2 g)) / g
+    g = 0.2
+    e = expected_race_time([[1.0]], [[1.5]], 1.0, t_cap=1e9, start=[[0.5]], leak=[g])
+    t_leak = np.log((1.0 - 0.5 * g) / (1.0 - 2.0 * g)) / g
+    np.testing.assert_allclose(e, [1.0 / (1.0 / t_leak + 1.0 / 1.5 ** 2)])
+    # a leak that holds x below the threshold (v / g < threshold) leaves diffusion alone
+    e = expected_race_time([[1.0]], [[1.5]], 1.0, t_cap=1e9, start=[[0.5]], leak=[1.0])
+    np.testing.assert_allclose(e, [1.5 ** 2])
+    # inhibition slows the race as leak does: g' = g + (n - 2) b for n accumulators
+    e_b = expected_race_time(v, dist, s, t_cap=1e9, start=[[0.5] * 4], leak=[0.1], inhibition=[0.2])
+    e_g = expected_race_time(v, dist, s, t_cap=1e9, start=[[0.5] * 4], leak=[0.1 + 2 * 0.2], inhibition=[0.0])
+    np.testing.assert_allclose(e_b, e_g, rtol=1e-12)
+    assert e_b[0] > plain[0]
+
+
 def test_with_order_copies_the_launch_options():
     import torch
 
