@@ -12,11 +12,13 @@
 //    hands them the next trajectories of its chunk (popc rank) in one
 //    divergent pass, so that pass is paid once per several trajectories and
 //    an ended lane idles for a few blocks at most.
-//  * Steps run in blocks of 36 (24 for ddm_flex, 8 for Levy): six independent
-//    Philox4x32-10 calls yield 24 words = 18 Box-Muller pairs = the block's
-//    increments, already scaled to drift + s sqrt(dt) N(0,1); the steps
-//    themselves are predicated (no per-step branch), and a warp whose walks
-//    cannot reach their time limit within the block skips the time test.
+//  * Steps run in blocks of 36 (24 for ddm_flex with a Weibull or table
+//    bound, 8 for Levy): six independent Philox4x32-10 calls yield 24 words =
+//    18 Box-Muller pairs = the block's increments, already scaled to drift +
+//    s sqrt(dt) N(0,1), each call drawn in the step loop just before the six
+//    steps that use it; the steps themselves are predicated (no per-step
+//    branch), and a warp whose walks cannot reach their time limit within the
+//    block skips the time test.
 //  * A launch with about as many trajectories as the grid has lanes lasts as
 //    long as its longest walk.  There W = 2, 4 or 8 lanes share a walk
 //    (ssm_launch.lanes_per_walk, wide_block): each draws a third of the
@@ -82,7 +84,7 @@ struct SingleParams {
     int64_t tstride, tlen;
     const float *dtable;     // DFLEX: drift v(t_ix) per trial, row stride dstride, dlen entries
     int64_t dstride, dlen;
-    int dvec;                // rows 16-byte aligned: a block's 24 drifts are six float4 loads
+    int dvec;                // rows 16-byte aligned: a block's drifts are float4 loads
     const float *noise;      // injected increments: row w holds nlen floats
     int64_t nlen;
     const float *nunif;      // injected jitter uniforms, one per trajectory
@@ -272,22 +274,35 @@ __device__ __forceinline__ float cms_stable(uint32_t bu, uint32_t bw, const Tria
 // steps); four per call with 32-step blocks 31.2.  With the re-tuned launch
 // (128 threads, claims of 256): 30 steps 26.95, 36 steps 26.54, 42 steps
 // 26.39, but on 1024 sets 42 steps is the slower (8.02 against 7.92 ms).
-// ddm_flex holds a block's table drifts in registers as well, so its blocks
-// are shorter: 24 steps (four Philox calls, six float4 drift loads) took
-// 14.46 ms on the 1 024 conflict_ds sets against 15.73 for 12 steps and
-// 16.51 for 16-step blocks of four increments per call (36 steps spill).
+// ddm_flex holds a block's table drifts in registers as well: with the
+// increments drawn a block at a time, 24 steps (four Philox calls, six float4
+// drift loads) took 14.46 ms on the 1 024 conflict_ds sets against 15.73 for
+// 12 steps and 16.51 for 16-step blocks of four increments per call (36 steps
+// spilled).  With the draws fused into the steps (step_block FUSE) 36 steps
+// fit for the constant and linear bounds (11.42 -> 11.00 ms against 24); the
+// Weibull and table bounds keep 24 (at 36 the Weibull bound spills 294 bytes).
 // The Levy model keeps 8-step blocks (its stable draws already give each
 // block enough independent work; 16-step blocks measured 8 % slower there).
 // Call h of block b uses counter (BLK/6) b + h, so a stream does not depend
 // on the block length.
-template <int MODEL> struct Blk {
-    static constexpr int value = (MODEL == M_LEVY) ? 8 : (MODEL == M_DFLEX ? 24 : 36);
+template <int MODEL, int BOUND = SSM_BOUND_CONSTANT> struct Blk {
+    static constexpr int value =
+        (MODEL == M_LEVY) ? 8
+                          : ((MODEL == M_DFLEX && BOUND != SSM_BOUND_CONSTANT && BOUND != SSM_BOUND_LINEAR) ? 24 : 36);
 };
 // Lanes per walk W (see wide_block): 1 is the throughput mode above; W = 2,
 // 4, 8 give each trajectory an aligned group of W lanes and blocks of 18 W
 // steps, three Philox calls per lane.
-template <int MODEL, int W> struct BlkW {
-    static constexpr int value = (W == 1) ? Blk<MODEL>::value : 18 * W;
+template <int MODEL, int W, int BOUND = SSM_BOUND_CONSTANT> struct BlkW {
+    static constexpr int value = (W == 1) ? Blk<MODEL, BOUND>::value : 18 * W;
+};
+// Device-RNG Gaussian models draw their increments inside the step loop
+// (step_block FUSE).  Outputs are bit-identical to drawing the block first;
+// measured on one B200 (ms per launch): 4 096-set angle batch 26.43 -> 26.33
+// (80 -> 64 registers), 1 024 conflict_ds sets 12.29 -> 11.42 (its 52-62 bytes
+// of spills gone), Ornstein 20.70 -> 20.41.
+template <int MODEL, bool NOISE> struct FuseOk {
+    static constexpr bool value = !NOISE && MODEL != M_LEVY;
 };
 template <int MODEL, bool NOISE, int BOUND> struct WideOk {
     static constexpr bool value =
@@ -312,13 +327,26 @@ struct Lane {
 // models whose drift is drawn once per trajectory
 template <int MODEL> struct DrawnDrift { static constexpr bool value = (MODEL == M_SDV || MODEL == M_FULL); };
 
+// Increments 6h .. 6h+5 of the lane's current block from the device RNG
+// (Gaussian models): Philox call (BLK/6) blk + h of the trajectory's stream.
+template <int MODEL, int BOUND>
+__device__ __forceinline__ void draw_call(const SingleParams &p, const Lane &L, const TrialRow &r, int h,
+                                          float *g6) {
+    constexpr int BLK = Blk<MODEL, BOUND>::value;
+    // ddm_flex: drift 0 here, v(t_ix) dt from the table in the step
+    const float drift = (MODEL == M_DFLEX) ? 0.f : (DrawnDrift<MODEL>::value ? L.dinc : r.drift);
+    const uint4 b = philox10(make_uint4((uint32_t)(BLK / 6) * L.blk + (uint32_t)h, L.n, L.k + p.k_base, 0u),
+                             p.key);
+    bm6_increment(b, r.c2, drift, g6);
+}
+
 // The block's increments.  Noise injection returns the raw caller draws (the
 // step applies drift and scale with explicit rounding); the device RNG returns
 // finished increments drift + scale * X.
-template <int MODEL, bool NOISE>
+template <int MODEL, int BOUND, bool NOISE>
 __device__ __forceinline__ void draw_block(const SingleParams &p, const Lane &L, const TrialRow &r,
-                                           float g[Blk<MODEL>::value]) {
-    constexpr int BLK = Blk<MODEL>::value;
+                                           float g[Blk<MODEL, BOUND>::value]) {
+    constexpr int BLK = Blk<MODEL, BOUND>::value;
     if (NOISE) {
         // SDV/FULL rows start with the trajectory's drift normal
         constexpr int OFF = DrawnDrift<MODEL>::value ? 1 : 0;
@@ -336,26 +364,26 @@ __device__ __forceinline__ void draw_block(const SingleParams &p, const Lane &L,
             g[2 * h + 3] = fmaf(r.scale, cms_stable(c.z, c.w, r), r.drift);
         }
     } else {
-        // ddm_flex: drift 0 here, v(t_ix) dt from the table in the step
-        const float drift = (MODEL == M_DFLEX) ? 0.f : (DrawnDrift<MODEL>::value ? L.dinc : r.drift);
         static_assert(MODEL == M_LEVY || BLK % 6 == 0, "six increments per Philox call");
 #pragma unroll
-        for (int h = 0; h < BLK / 6; ++h) {
-            const uint4 b = philox10(make_uint4((uint32_t)(BLK / 6) * L.blk + (uint32_t)h, L.n, L.k + p.k_base, 0u),
-                                     p.key);
-            bm6_increment(b, r.c2, drift, g + 6 * h);
-        }
+        for (int h = 0; h < BLK / 6; ++h) draw_call<MODEL, BOUND>(p, L, r, h, g + 6 * h);
     }
 }
 
 // Advance one lane by up to BLK Euler steps.  Every step first tests the
 // reference's `while` condition (ddm_models.pyx:719; legacy DDM :451); once it
 // fails the remaining steps of the block are predicated off.  Returns whether
-// the walk is still running.
-template <int MODEL, int BOUND, bool NOISE, bool RECORD, bool TCHK = true>
+// the walk is still running.  With FUSE (device RNG, Gaussian models) the
+// increments are drawn inside the step loop, six per Philox call (g unused):
+// the same values as draw_block, with each call's draws in the same straight-
+// line code as the steps, so their independent work fills the latency of the
+// dependent step chain and only six increments are live at a time.
+template <int MODEL, int BOUND, bool NOISE, bool RECORD, bool TCHK = true, bool FUSE = false>
 __device__ __forceinline__ bool step_block(const SingleParams &p, Lane &L, const TrialRow &r,
-                                           const float g[Blk<MODEL>::value]) {
-    constexpr int BLK = Blk<MODEL>::value;
+                                           const float *g) {
+    constexpr int BLK = Blk<MODEL, BOUND>::value;
+    static_assert(!FUSE || (!NOISE && MODEL != M_LEVY), "fused draws: device RNG, Gaussian models");
+    float g6[6];
     if (L.ixf >= r.capf) {
         raise_error(p.hdr, SSM_ERR_DEVICE, (int)L.w);
         return false;
@@ -390,6 +418,8 @@ __device__ __forceinline__ bool step_block(const SingleParams &p, Lane &L, const
     bool live = true;
 #pragma unroll
     for (int q = 0; q < BLK; ++q) {
+        if (FUSE && q % 6 == 0) draw_call<MODEL, BOUND>(p, L, r, q / 6, g6);
+        const float gq = FUSE ? g6[q % 6] : g[q];
         bool inside;
         // the time test; a block whose every step is known to pass it skips it (TCHK false)
         const bool in_time = !TCHK || (L.tp <= r.dl_tmp);
@@ -411,22 +441,22 @@ __device__ __forceinline__ bool step_block(const SingleParams &p, Lane &L, const
                 if (MODEL == M_OU) {
                     // (y + (v - g y) dt) + scale*g (ornstein_models.pyx:177)
                     const float lk = __fmul_rn(__fsub_rn(r.alpha, __fmul_rn(r.inv_alpha, L.y)), p.dt);
-                    L.y = __fadd_rn(__fadd_rn(L.y, lk), __fmul_rn(r.scale, g[q]));
+                    L.y = __fadd_rn(__fadd_rn(L.y, lk), __fmul_rn(r.scale, gq));
                 } else if (MODEL == M_DFLEX) {
                     // (y + v(t_ix) dt) + scale*g (ddm_models.pyx:1025)
                     const float dv = __ldg(drow + ((L.ix < p.dlen) ? L.ix : p.dlen - 1));
-                    L.y = __fadd_rn(__fadd_rn(L.y, __fmul_rn(dv, p.dt)), __fmul_rn(r.scale, g[q]));
+                    L.y = __fadd_rn(__fadd_rn(L.y, __fmul_rn(dv, p.dt)), __fmul_rn(r.scale, gq));
                 } else {
                     // (y + v*dt) + scale*g: the association the reference build uses
                     const float dr = DrawnDrift<MODEL>::value ? L.dinc : r.drift;
-                    L.y = __fadd_rn(__fadd_rn(L.y, dr), __fmul_rn(r.scale, g[q]));
+                    L.y = __fadd_rn(__fadd_rn(L.y, dr), __fmul_rn(r.scale, gq));
                 }
                 L.tp = __fadd_rn(L.tp, p.dt);
             } else {
-                if (MODEL == M_OU) L.y = fmaf(L.y, r.expo, g[q]);  // y (1 - g dt) + v dt + noise
+                if (MODEL == M_OU) L.y = fmaf(L.y, r.expo, gq);  // y (1 - g dt) + v dt + noise
                 else if (MODEL == M_DFLEX)                          // y + v(t_ix) dt + noise
-                    L.y += fmaf(dvq[q], p.dt, g[q]);
-                else L.y += g[q];
+                    L.y += fmaf(dvq[q], p.dt, gq);
+                else L.y += gq;
                 L.tp += p.dt;
             }
             if (INT_IX) {
@@ -447,7 +477,7 @@ __device__ __forceinline__ bool step_block(const SingleParams &p, Lane &L, const
 // additions' rounding; below 65536 dt an ulp of t is at most dt/64, so that
 // rounding stays under dt/4, and t + (BLK+1) dt <= dl_tmp, evaluated in float,
 // leaves more than that margin.
-template <int MODEL, int BOUND, bool NOISE, int BLK = Blk<MODEL>::value>
+template <int MODEL, int BOUND, bool NOISE, int BLK = Blk<MODEL, BOUND>::value>
 __device__ __forceinline__ bool block_in_time(const SingleParams &p, const Lane &L, const TrialRow &r) {
     constexpr bool INT_IX = NOISE || BOUND == SSM_BOUND_TABLE;
     if (INT_IX) return false;
@@ -460,7 +490,7 @@ __device__ __forceinline__ bool block_in_time(const SingleParams &p, const Lane 
 // Steps taken by a walk that has ended.  Without an integer index L.ixf
 // counts whole blocks; the steps of the last block are those that took the
 // time accumulator from L.tpb to L.tp (the same float additions replayed).
-template <int MODEL, int BOUND, bool NOISE, int BLK = Blk<MODEL>::value>
+template <int MODEL, int BOUND, bool NOISE, int BLK = Blk<MODEL, BOUND>::value>
 __device__ __forceinline__ int steps_taken(const SingleParams &p, const Lane &L) {
     constexpr bool INT_IX = NOISE || BOUND == SSM_BOUND_TABLE;
     if (INT_IX) return (int)L.ixf;
@@ -473,7 +503,7 @@ __device__ __forceinline__ int steps_taken(const SingleParams &p, const Lane &L)
     return (int)L.ixf - BLK + c;
 }
 
-template <int MODEL, int BOUND, bool NOISE, int BLK = Blk<MODEL>::value>
+template <int MODEL, int BOUND, bool NOISE, int BLK = Blk<MODEL, BOUND>::value>
 __device__ __forceinline__ void finalize(const SingleParams &p, const Lane &L, bool writer = true) {
     // fields needed only here are re-read instead of being held across the walk
     const TrialRow *row = p.rows + L.k;
@@ -638,7 +668,7 @@ template <int MODEL, int BOUND, bool NOISE, int W>
 __global__ void __launch_bounds__(256, (MinCtas<MODEL, W>::value))
     k_single(const __grid_constant__ SingleParams p) {
     static_assert(W == 1 || WideOk<MODEL, NOISE, BOUND>::value, "lanes per walk > 1: device RNG, in-register bound");
-    constexpr int BLK = BlkW<MODEL, W>::value;
+    constexpr int BLK = BlkW<MODEL, W, BOUND>::value;
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const int sub = lane & (W - 1);              // place in the group
@@ -695,10 +725,15 @@ __global__ void __launch_bounds__(256, (MinCtas<MODEL, W>::value))
         bool live = false;
         if constexpr (W == 1) {
             if (active) {
-                float g[Blk<MODEL>::value];
-                draw_block<MODEL, NOISE>(p, L, r, g);
-                live = skip_time ? step_block<MODEL, BOUND, NOISE, false, false>(p, L, r, g)
-                                 : step_block<MODEL, BOUND, NOISE, false, true>(p, L, r, g);
+                if constexpr (FuseOk<MODEL, NOISE>::value) {
+                    live = skip_time ? step_block<MODEL, BOUND, NOISE, false, false, true>(p, L, r, nullptr)
+                                     : step_block<MODEL, BOUND, NOISE, false, true, true>(p, L, r, nullptr);
+                } else {
+                    float g[Blk<MODEL, BOUND>::value];
+                    draw_block<MODEL, BOUND, NOISE>(p, L, r, g);
+                    live = skip_time ? step_block<MODEL, BOUND, NOISE, false, false>(p, L, r, g)
+                                     : step_block<MODEL, BOUND, NOISE, false, true>(p, L, r, g);
+                }
             }
         } else {
             live = skip_time ? wide_block<MODEL, BOUND, false, W>(p, L, r, active, src0, sub)
@@ -727,8 +762,8 @@ __global__ void k_record(const __grid_constant__ SingleParams p) {
     lane_init<MODEL, NOISE>(p, L, r, 0, hint);
     if (p.traj_len > 0) p.traj[0] = L.y;
     for (;;) {
-        float g[Blk<MODEL>::value];
-        draw_block<MODEL, NOISE>(p, L, r, g);
+        float g[Blk<MODEL, BOUND>::value];
+        draw_block<MODEL, BOUND, NOISE>(p, L, r, g);
         const bool live = step_block<MODEL, BOUND, NOISE, true>(p, L, r, g);
         L.blk += 1;
         if (!live) break;
