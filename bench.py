@@ -261,11 +261,11 @@ class ClockSampler:
 
 # ------------------------------------------------------------------ GPU side
 # DRAM bytes (read + write) of one k_single launch on the 4096-theta workload,
-# from one ncu capture of that launch (dram__bytes_read.sum 13,818,368 +
-# dram__bytes_write.sum 289,421,568).
+# from one ncu capture of that launch (dram__bytes_read.sum 10,086,144 +
+# dram__bytes_write.sum 287,236,864).
 # The algorithmic output is 8 B per trajectory (338 MB); part of it is still in
 # L2 when the kernel ends, so the measured writes sit slightly below it.
-K_SINGLE_TRAFFIC_BYTES = 13_818_368 + 289_421_568
+K_SINGLE_TRAFFIC_BYTES = 10_086_144 + 287_236_864
 
 
 def hbm_peak() -> tuple[float, str]:

@@ -360,7 +360,7 @@ class BatchedSimulator:
             self._streams = (torch.cuda.Stream(), torch.cuda.Stream(), torch.cuda.Stream())
         cs0, cs1, copy_s = self._streams
         bounds = self.window_bounds(chunks)
-        base = launch_for(self.family) if self.launch is None else self.launch
+        base = launch_for(self.family, windows=True) if self.launch is None else self.launch
         if base.lanes_per_walk == 0:
             base = _lib.launch_replace(base, lanes_per_walk=self.lanes_per_walk)
         orders = self._window_order(bounds) if self.expected_time is not None else None

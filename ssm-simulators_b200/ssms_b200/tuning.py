@@ -45,8 +45,14 @@ DEFAULT_CANDIDATES = [(bt, bps, ch, rm) for bt in (128, 256) for bps in (0, 3) f
                       for rm in (0, 2, 6)]
 
 
-def launch_for(model: str) -> _lib.SsmLaunch:
-    cfg = _load().get(model, {})
+def launch_for(model: str, windows: bool = False) -> _lib.SsmLaunch:
+    """The stored launch configuration of a simulator family.  ``windows``
+    asks for the shape of the windowed end-to-end path
+    (``BatchedSimulator.run_to_host``), whose consecutive trial windows share
+    the GPU on two streams; a family may store it under ``"<family>:windows"``
+    and otherwise uses its single-launch shape."""
+    table = _load()
+    cfg = table.get(f"{model}:windows", table.get(model, {})) if windows else table.get(model, {})
     return _lib.SsmLaunch(block_threads=int(cfg.get("block_threads", 0)),
                           blocks_per_sm=int(cfg.get("blocks_per_sm", 0)), chunk=int(cfg.get("chunk", 0)),
                           refill_min=int(cfg.get("refill_min", 0)))

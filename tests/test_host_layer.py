@@ -239,3 +239,21 @@ def test_set_order_estimates_for_every_configured_model():
         assert est.shape == (K,) and np.all(np.isfinite(est)) and np.all(est >= 0) and np.all(est <= 20.0), name
         done += 1
     assert done >= 40
+
+
+def test_windowed_path_launch_shape_lookup(monkeypatch):
+    from ssms_b200 import tuning
+
+    table = {"fam": {"block_threads": 256, "blocks_per_sm": 3, "chunk": 128, "refill_min": 0},
+             "fam:windows": {"block_threads": 128, "blocks_per_sm": 0, "chunk": 256, "refill_min": 2},
+             "other": {"block_threads": 64, "blocks_per_sm": 2, "chunk": 32, "refill_min": 1}}
+    monkeypatch.setattr(tuning, "_cache", table)
+    one = tuning.launch_for("fam")
+    win = tuning.launch_for("fam", windows=True)
+    assert (one.block_threads, one.blocks_per_sm, one.chunk) == (256, 3, 128)
+    assert (win.block_threads, win.blocks_per_sm, win.chunk, win.refill_min) == (128, 0, 256, 2)
+    # a family without a windowed entry uses its single-launch shape for both
+    o1, o2 = tuning.launch_for("other"), tuning.launch_for("other", windows=True)
+    assert (o1.block_threads, o1.chunk) == (o2.block_threads, o2.chunk) == (64, 32)
+    # unknown families fall back to the library defaults (zeros)
+    assert tuning.launch_for("missing", windows=True).block_threads == 0
