@@ -257,3 +257,22 @@ def test_windowed_path_launch_shape_lookup(monkeypatch):
     assert (o1.block_threads, o1.chunk) == (o2.block_threads, o2.chunk) == (64, 32)
     # unknown families fall back to the library defaults (zeros)
     assert tuning.launch_for("missing", windows=True).block_threads == 0
+
+
+def test_stored_launch_shapes_are_well_formed():
+    import json
+    from pathlib import Path
+
+    import ssms_b200
+
+    families = {"ddm", "ddm_flexbound", "ddm_flex", "full_ddm", "ddm_sdv", "ornstein_uhlenbeck", "levy_flexbound",
+                "race_model", "lca", "racing_diffusion_model"}
+    table = json.loads((Path(ssms_b200.__file__).parent / "_tuned.json").read_text())
+    for key, cfg in table.items():
+        fam = key.split(":")[0]
+        assert fam in families, key
+        assert key == fam or (key == f"{fam}:windows" and fam in table), key
+        assert set(cfg) == {"block_threads", "blocks_per_sm", "chunk", "refill_min"}, key
+        assert all(isinstance(v, int) and v >= 0 for v in cfg.values()), key
+        assert cfg["block_threads"] in (0, 64, 128, 256, 512), key
+        assert cfg["refill_min"] <= 32, key
